@@ -1,0 +1,315 @@
+#!/usr/bin/env python
+"""Induced-velocity (Biot-Savart) benchmark on the large helical wake.
+
+Workload (one step = one full evaluation): 3 blades x 41 cosine-spaced nodes x
+720 wake steps at 1 deg (two revolutions), every shed and trailing filament
+(175,080) onto every wake node and lifting-line point (88,803), Vatistas n=2
+core, FP32-compensated arithmetic with FP64 near-singular terms. Synthetic,
+seeded inputs (no dataset). Metric: Gint/s (1e9 target-filament interactions
+per second), whole job over all ranks.
+
+``python bench.py [--gpus N --steps K --warmup W]`` -- this engine.
+``python bench.py --impl reference``                 -- the reference's CPU
+  formula (the C restatement of core/BiotSavart.m, all host threads) on a
+  bounded sample of the same workload.
+For N > 1 (torchrun) each rank evaluates its own wake (seed + rank): weak
+scaling, no data-path collective; the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+FLOP_PER_INTERACTION = 52  # Vatistas n=2 kernel, FMA = 2
+METRIC = "biot_savart_gint_per_s"
+UNIT = "Gint/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = str(gpu_index)
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.th = threading.Thread(target=self._read, daemon=True)
+        self.th.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9 and parts[0] == self.idx:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------------ workload
+def workload(seed):
+    synth = importlib.import_module("winds-master_b200.synth")
+    w = synth.make_wake(synth.large_case(seed=seed))
+    fams = [synth.shed_filaments(w["dom"]) + (w["gamma_shed"], w["rc_shed"]),
+            synth.trail_filaments(w["dom"]) + (w["gamma_trail"], w["rc_trail"])]
+    pts = np.concatenate([synth.flat_points(w["dom"]), synth.flat_points(w["ll"])])
+    P = np.asfortranarray(pts.reshape(-1, 3, 1, 1))
+    nf = sum(f[0].shape[0] * f[0].shape[2] * f[0].shape[3] for f in fams)
+    return w, fams, P, nf, P.shape[0]
+
+
+def cpu_rate(fams, P, n_targets, seed=0):
+    """C oracle (FP64 restatement of BiotSavart.m, OpenMP on all host threads)
+    over n_targets sampled targets x all filaments; returns (Gint/s, seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    rng = np.random.default_rng(seed)
+    idx = rng.choice(P.shape[0], n_targets, replace=False)
+    Ps = np.asfortranarray(P[idx])
+    nf = sum(f[0].shape[0] * f[0].shape[2] * f[0].shape[3] for f in fams)
+    t0 = time.perf_counter()
+    for F1, F2, g, rc in fams:
+        orc.c_eval(F1, F2, Ps, g, rc, "visc2", 1000.0, nthreads=os.cpu_count())
+    dt = time.perf_counter() - t0
+    return n_targets * nf / dt / 1e9, dt
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    _, fams, P, nf, nt = workload(1)
+    cores = os.cpu_count()
+    # size one step to about 3 s of CPU work
+    rate, _ = cpu_rate(fams, P, 16)
+    n = int(max(16, min(nt, 3.0 * rate * 1e9 / nf)))
+    for i in range(args.warmup):
+        cpu_rate(fams, P, max(16, n // 8), seed=100 + i)
+    total_t, total_int = 0.0, 0
+    for i in range(args.steps):
+        r, dt = cpu_rate(fams, P, n, seed=i)
+        total_t += dt
+        total_int += n * nf
+    value = total_int / total_t / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total_t / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "helical wake 3x41x720 (1 deg), Vatistas n=2, all shed+trailing "
+                   "filaments onto all wake nodes + lifting-line points", "targets": nt, "filaments": nf},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{n} sampled targets x {nf} filaments per step"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "oracle/_ref (the reference MEX host loop) implements only the cut-off core, so "
+                "the Vatistas workload runs on the FP64 C restatement of core/BiotSavart.m",
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ our arm
+def ours(args):
+    import torch
+    import torch.distributed as dist
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    wb = importlib.import_module("winds-master_b200")
+    lib = wb.lib()
+    w, fams, P, nf, nt = workload(1 + rank)
+    interactions = nf * nt
+
+    def dev(a):
+        return torch.from_numpy(np.asarray(a).ravel(order="F").copy()).cuda()
+
+    dfams = [(dev(F1), dev(F2), dev(g), dev(rc), F1.shape) for F1, F2, g, rc in fams]
+    dP = (dev(P), P.shape)
+    out = torch.zeros(P.size, dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    core = wb.bs.CORE_VATISTAS
+
+    # warm-up on the library stream (the first call autotunes the tiling)
+    for _ in range(max(1, args.warmup)):
+        wb.eval_device(dfams, dP, core, 2.0, 1000.0, out, "f32c")
+    wb.sync()
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    peak = C.c_double()
+    lib.winds_bs_fp32_peak(C.byref(peak))
+
+    clocks = ClockSampler(torch.cuda.current_device() if "CUDA_VISIBLE_DEVICES" not in os.environ
+                          else int(os.environ["CUDA_VISIBLE_DEVICES"].split(",")[local]))
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    step_ms, main_ms = [], []
+    launches = 0
+    near_pairs = 0
+    for _ in range(args.steps):
+        flush.zero_()  # L2 flush between timed steps (outside the events)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        wb.eval_device(dfams, dP, core, 2.0, 1000.0, out, "f32c", stream=sp)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        m, n, near = wb.last_stats()
+        main_ms.append(m)
+        launches += n
+        near_pairs = near
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    wb.sync(sp)
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * interactions * args.steps / (total_ms * 1e-3) / 1e9
+    u32 = out.cpu().numpy()
+
+    # plain FP64 GPU direct sum (the comparison path) and the accuracy of FP32c against it
+    fp64 = None
+    rel_err = None
+    if not args.no_fp64:
+        out64 = torch.zeros_like(out)
+        wb.eval_device(dfams, dP, core, 2.0, 1000.0, out64, "f64", stream=sp)
+        torch.cuda.synchronize()
+        t64 = []
+        for _ in range(2):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            wb.eval_device(dfams, dP, core, 2.0, 1000.0, out64, "f64", stream=sp)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            t64.append(e0.elapsed_time(e1))
+        fp64 = interactions / (statistics.median(t64) * 1e-3) / 1e9
+        a = np.stack([u32.reshape(P.shape, order="F")[:, c].ravel(order="F") for c in range(3)], 1)
+        b64 = out64.cpu().numpy().reshape(P.shape, order="F")
+        b = np.stack([b64[:, c].ravel(order="F") for c in range(3)], 1)
+        rel_err = float(np.max(np.linalg.norm(a - b, axis=1) / np.linalg.norm(b, axis=1)))
+
+    # end to end through the public host API: pinned host inputs, H2D + eval + D2H per step
+    pin = lambda a: torch.from_numpy(np.asfortranarray(a)).pin_memory().numpy()
+    hfams = [tuple(pin(x) for x in f) for f in fams]
+    hP = pin(P)
+    h2d = sum(sum(x.nbytes for x in f) for f in hfams) + hP.nbytes
+    d2h = hP.nbytes
+    wb.eval_host(hfams, hP, core, 2.0, 1000.0, "f32c")
+    e2e_t = []
+    for _ in range(max(1, min(args.steps, 5))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        wb.eval_host(hfams, hP, core, 2.0, 1000.0, "f32c")
+        e2e_t.append(time.perf_counter() - t0)
+    e2e = world * interactions / statistics.median(e2e_t) / 1e9
+
+    mean_main = statistics.mean(main_ms)
+    achieved = FLOP_PER_INTERACTION * interactions / (mean_main * 1e-3) / 1e12
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "bs_f32c_traffic.json")
+    if os.path.exists(tf):
+        tj = json.load(open(tf))
+        traffic = tj.get("bytes_per_interaction", 0.0) * interactions
+
+    cpu = None
+    if rank == 0 and world == 1:
+        rate, _ = cpu_rate(fams, P, 16)
+        n = int(max(16, min(nt, 10.0 * rate * 1e9 / nf)))
+        rate, dt = cpu_rate(fams, P, n, seed=1)
+        cpu = {"value": rate, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+               "sample": f"{n} sampled targets x {nf} filaments ({dt:.1f} s), FP64 C restatement "
+                         "of core/BiotSavart.m, OpenMP"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic",
+            "config": {"workload": "helical wake 3x41x720 (1 deg), Vatistas n=2, all shed+trailing "
+                       "filaments onto all wake nodes + lifting-line points", "targets": nt,
+                       "filaments": nf, "interactions_per_step": interactions,
+                       "l2": "256 MB buffer written between timed steps",
+                       "parallelism": f"replicated wakes x{world}" if world > 1 else "single GPU"},
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                         "frac": achieved / peak.value if peak.value else None, "traffic": traffic,
+                         "peak_source": "FFMA probe measured in this run (winds_bs_fp32_peak)",
+                         "kernel": "bs_f32c", "flop_per_interaction": FLOP_PER_INTERACTION,
+                         "kernel_ms": mean_main},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "timing": "wall clock around the synchronous host-API call"},
+            "gpu_launches": launches,
+            "clocks": clk,
+            "plain_fp64_gint_per_s": fp64,
+            "speedup_vs_plain_fp64": (value / world / fp64) if fp64 else None,
+            "rel_err_max_vs_fp64": rel_err,
+            "near_pairs_per_step": near_pairs,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        reference_arm(a)
+    else:
+        ours(a)

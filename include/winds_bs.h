@@ -1,0 +1,144 @@
+/*
+ * winds_bs.h -- C ABI of libwinds_bs, the sm_100a induced-velocity engine that
+ * replaces WInDS's Biot-Savart hot path.
+ *
+ * Every entry point takes plain pointers and sizes. Arrays keep WInDS's MATLAB
+ * layout: column-major doubles shaped [span, component, age, blade].
+ *
+ * What each entry point replaces in the reference (ndevelder/WInDS-Master):
+ *   winds_bs_eval_host    core/BiotSavart.m:1-119 (the [uind,L]=BiotSavart(...)
+ *                         'full' call) and cuda/source/BiotSavartMex.cu:452-685
+ *                         (biot_calc: pack, copy in, kernel, copy out).
+ *   winds_bs_eval_device  the same evaluation on device-resident arrays
+ *                         (cuda/source/BiotSavartMex.cu:131-193, the
+ *                         BiotSavart_naive / BiotSavart_sh kernels).
+ *   winds_bs_length_*     core/FilamentLength.m:27-44 and the 'leng' branch of
+ *                         cuda/source/BiotSavartMex.cu:197-206,582-587.
+ *   mexFunction           cuda/source/BiotSavartMex.cu:688-807, the 11-argument
+ *                         [uind,L]=BiotSavartMex(F1,F2,P,gamma,rc,d,cmod,co,
+ *                         type,gpu,gpuhw) contract.
+ *
+ * All functions return WINDS_BS_OK (0) or a positive WINDS_BS_ERR_* code; the
+ * message of the last failure on the calling thread is available from
+ * winds_bs_last_error(). Nothing prints.
+ */
+#ifndef WINDS_BS_H
+#define WINDS_BS_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WINDS_BS_OK 0
+#define WINDS_BS_ERR_ARG 1      /* bad shape, pointer or option */
+#define WINDS_BS_ERR_CUDA 2     /* a CUDA runtime call failed */
+#define WINDS_BS_ERR_TIMEOUT 3  /* a bounded device wait ran out; context stays usable */
+#define WINDS_BS_ERR_NOMEM 4    /* device or pinned allocation failed */
+#define WINDS_BS_ERR_NODEV 5    /* no CUDA device, or the library was built without one */
+
+/* Core models of core/BiotSavart.m:102-109. */
+#define WINDS_CORE_CUTOFF 0   /* ubar = G/4pi (r1+r2)/(r1r2(r1r2+r1.r2) + d|L|^2)      (:108) */
+#define WINDS_CORE_VATISTAS 1 /* ubar scaled by Cnu = h^2 (rc^n + h^2n)^(-1/n), n = d  (:103-106) */
+
+/* Arithmetic of the direct sum. */
+#define WINDS_PREC_F32C 0 /* FP32 tiles + per-target Kahan, FP64 near-singular terms (default) */
+#define WINDS_PREC_F64 1  /* plain FP64 direct sum (the comparison GPU path) */
+
+/* One filament family, e.g. the shed call F1=dom(1:end-1,:,:,:),
+ * F2=dom(2:end,:,:,:) of WInDS.m:150 or the trailing call of WInDS.m:153. */
+typedef struct {
+  const double *F1;    /* [dims0, 3, dims2, dims3] first endpoints            */
+  const double *F2;    /* [dims0, 3, dims2, dims3] second endpoints           */
+  const double *gamma; /* [dims0, 1, dims2, dims3] circulation                */
+  const double *rc;    /* [dims0, 1, dims2, dims3] squared core radius (rc^2) */
+  long long dims[4];   /* dims[1] must be 3 */
+} winds_bs_family;
+
+/* Flags of winds_bs_params.flags. */
+#define WINDS_BS_FLAG_SEQUENTIAL 1 /* FP64: one pass per target over all filaments in order
+                                      (reproduces the reference's serial host loop,
+                                      BiotSavartMex.cu:268-282, bit for bit, cut-off model) */
+
+typedef struct {
+  int core_model; /* WINDS_CORE_* */
+  double d;       /* cut-off: squared cut-off (user.d); Vatistas: index n */
+  double co;      /* reach cut-off: a term is zero when r1>co and r2>co (BiotSavart.m:111) */
+  int precision;  /* WINDS_PREC_* ; Vatistas n != 2 and non-finite or negative d use FP64 */
+  int flags;      /* WINDS_BS_FLAG_* */
+} winds_bs_params;
+
+/* Library version string. */
+const char *winds_bs_version(void);
+
+/* Message of the last failure on this thread ("" if none). */
+const char *winds_bs_last_error(void);
+
+/* Number of visible CUDA devices (0 on a machine without a GPU). */
+int winds_bs_device_count(int *n);
+
+/* Select the device later calls on this thread use (gpuhw(3) of the MEX). */
+int winds_bs_set_device(int device);
+
+/* Induced velocity at every point of P from every filament of fams[0..nfam).
+ * Device pointers. P is [pdims0, 3, pdims2, pdims3] (a 2-D or 3-D P is passed
+ * with trailing dims 1); uind has P's layout and is overwritten. stream is a
+ * cudaStream_t (NULL: the library's own stream); the call is asynchronous on
+ * it except that it waits for completion when it must report a device error.
+ * Replaces core/BiotSavart.m:80-116 / cuda/source/BiotSavartMex.cu:131-193. */
+int winds_bs_eval_device(const winds_bs_family *fams, int nfam, const double *P,
+                         const long long pdims[4], const winds_bs_params *prm,
+                         double *uind, void *stream);
+
+/* Same evaluation from host arrays: copies in, evaluates, copies uind out and
+ * synchronises. Replaces cuda/source/BiotSavartMex.cu:452-685 (biot_calc). */
+int winds_bs_eval_host(const winds_bs_family *fams, int nfam, const double *P,
+                       const long long pdims[4], const winds_bs_params *prm,
+                       double *uind);
+
+/* Filament lengths sqrt(|F2-F1|^2), MATLAB layout [dims0,1,dims2,dims3].
+ * Replaces core/FilamentLength.m:27-44. Device pointers. */
+int winds_bs_length_device(const double *F1, const double *F2, const long long dims[4],
+                           double *L, void *stream);
+
+/* Wall-free timing hook for benchmarks: device time in ms of the last
+ * winds_bs_eval_* call's main direct-sum kernel(s), measured with CUDA events
+ * on the launch stream; also reports how many kernels that call launched and
+ * how many near-singular pairs were recomputed in FP64 (if counted). */
+int winds_bs_last_stats(double *main_ms, int *launches, long long *near_pairs);
+
+/* Synchronises `stream` (NULL: the library's stream) and reports a device-side
+ * error (WINDS_BS_ERR_TIMEOUT for a bounded wait that ran out) recorded by an
+ * earlier asynchronous call; the error word is cleared. */
+int winds_bs_sync(void *stream);
+
+/* Autotuner control. The first FP32 evaluation of a (core model, log2 targets,
+ * log2 filaments) bucket on the library's own stream times the candidate
+ * tilings (targets per thread T in {2,4,8}, filaments per tile KF in {32,64},
+ * work-queue depth) and caches the fastest; set_tuning / get_tuning read and
+ * write that cache directly (e.g. to restore a saved choice). */
+int winds_bs_set_autotune(int on);
+int winds_bs_set_tuning(int core_model, long long n_targets, long long n_filaments, int T, int KF,
+                        double waves);
+int winds_bs_get_tuning(int core_model, long long n_targets, long long n_filaments, int *T,
+                        int *KF, double *waves);
+
+/* Measured FP32 FMA throughput of this GPU in TFLOP/s (a ~0.1 s probe of
+ * independent FFMA chains): the roofline denominator of the direct sum. */
+int winds_bs_fp32_peak(double *tflops);
+
+/* Failure-detection self-test: launches a kernel whose bounded mbarrier wait
+ * (limit_ns) has no producer, so it must run out. Returns WINDS_BS_ERR_TIMEOUT
+ * when the timeout was detected and reported; the context stays usable. */
+int winds_bs_selftest_wait_timeout(unsigned long long limit_ns);
+
+/* Frees every device buffer, stream and event of every device context
+ * (the mexAtExit hook of the MEX layer). */
+void winds_bs_shutdown(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WINDS_BS_H */

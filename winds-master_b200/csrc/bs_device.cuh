@@ -1,0 +1,180 @@
+// bs_device.cuh -- device helpers shared by the induced-velocity kernels:
+// mbarrier + bulk-copy (TMA) wrappers with bounded waits, fast FP32
+// reciprocal square roots, ordered-float atomics, and the FP64 pair term that
+// restates the reference formulas (used by the plain FP64 kernel and by the
+// near-singular fix-up of the FP32 kernel).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "bs_types.h"
+
+namespace winds {
+
+// ---------------------------------------------------------------- constants
+constexpr double kPi = 3.14159265358979324;  // cuda/source/BiotSavartMex.cu:35
+// (1.000/(4.000*pi)) as the reference's host loop folds it (BiotSavartMex.cu:260)
+constexpr double kInv4PiMex = 1.000 / (4.000 * kPi);
+// 4*pi as MATLAB evaluates it in core/BiotSavart.m:106,108
+constexpr double k4Pi = 4.0 * 3.141592653589793;
+
+
+// ------------------------------------------------------- PTX: barriers + bulk
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Arrive once on the barrier and add `bytes` to its expected transaction count.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t global_timer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Waits for the barrier phase with the given parity for at most `limit_ns`
+// nanoseconds. On timeout it sets kErrWaitTimeout in *err and returns false.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, unsigned *err,
+                                                  uint64_t limit_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_timer_ns();
+  while (true) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (global_timer_ns() - t0 > limit_ns) {
+      atomicOr(err, kErrWaitTimeout);
+      return false;
+    }
+  }
+}
+
+// One non-multicast bulk copy global -> this CTA's shared memory, completing
+// `bytes` transactions on `bar`. Both addresses 16-byte aligned, bytes % 16 == 0.
+__device__ __forceinline__ void bulk_g2s(void *smem_dst, const void *gmem_src, uint32_t bytes,
+                                         uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(smem_dst)),
+      "l"(gmem_src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// ------------------------------------------------------------ fast FP32 math
+__device__ __forceinline__ float rsqrt_approx(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// Ordered mapping float <-> int so that atomicMin/atomicMax on ints order floats.
+__device__ __forceinline__ int float_key(float f) {
+  int i = __float_as_int(f);
+  return i >= 0 ? i : i ^ 0x7fffffff;
+}
+__host__ __device__ inline float key_float(int k) {
+  int i = k >= 0 ? k : k ^ 0x7fffffff;
+  float f;
+  memcpy(&f, &i, sizeof(f));
+  return f;
+}
+
+// ---------------------------------------------------- FP64 reference pair term
+struct RefParams {
+  int model;   // kCoreCutoff / kCoreVatistas
+  double d;    // cut-off squared radius (cut-off model)
+  double n;    // Vatistas index (Vatistas model)
+  double co;   // reach cut-off
+};
+
+// Contribution of filament (A.xyz -> B.xyz, circulation A.w, squared core B.w)
+// at point p, accumulated into u.
+//
+// Cut-off model: the operation sequence of the reference's host loop
+// biot_p2p_nogpu (cuda/source/BiotSavartMex.cu:236-266), which is also the
+// formula of core/BiotSavart.m:108, with no fused multiply-adds, so a
+// sequential sum over filaments reproduces that loop bit for bit.
+// Vatistas model: the sequence of core/BiotSavart.m:103-106.
+// kGeneralN = false compiles only the n = 2 branch (the FP32 kernel's case).
+// Both then apply core/BiotSavart.m:111: a NaN/Inf ubar, or r1>co and r2>co,
+// gives ubar = 0 (the cross product still multiplies it, as in MATLAB).
+template <bool kGeneralN = true>
+__device__ __forceinline__ void ref_pair(const double4 A, const double4 B, double px, double py,
+                                         double pz, const RefParams &rp, double &ux, double &uy,
+                                         double &uz) {
+  const double x1 = A.x, y1 = A.y, z1 = A.z, g = A.w;
+  const double x2 = B.x, y2 = B.y, z2 = B.z, rc = B.w;
+  const double pxx1 = __dsub_rn(px, x1), pxx2 = __dsub_rn(px, x2);
+  const double pyy1 = __dsub_rn(py, y1), pyy2 = __dsub_rn(py, y2);
+  const double pzz1 = __dsub_rn(pz, z1), pzz2 = __dsub_rn(pz, z2);
+  const double r1 = sqrt(
+      __dadd_rn(__dadd_rn(__dmul_rn(pxx1, pxx1), __dmul_rn(pyy1, pyy1)), __dmul_rn(pzz1, pzz1)));
+  const double r2 = sqrt(
+      __dadd_rn(__dadd_rn(__dmul_rn(pxx2, pxx2), __dmul_rn(pyy2, pyy2)), __dmul_rn(pzz2, pzz2)));
+  const double r1dr2 =
+      __dadd_rn(__dadd_rn(__dmul_rn(pxx1, pxx2), __dmul_rn(pyy1, pyy2)), __dmul_rn(pzz1, pzz2));
+  const double r1tr2 = __dmul_rn(r1, r2);
+  double ubar;
+  if (rp.model == kCoreCutoff) {
+    const double ldx = __dsub_rn(x1, x2), ldy = __dsub_rn(y1, y2), ldz = __dsub_rn(z1, z2);
+    const double len =
+        __dadd_rn(__dadd_rn(__dmul_rn(ldx, ldx), __dmul_rn(ldy, ldy)), __dmul_rn(ldz, ldz));
+    const double den = __dadd_rn(__dmul_rn(r1tr2, __dadd_rn(r1tr2, r1dr2)), __dmul_rn(rp.d, len));
+    ubar = __dmul_rn(__dmul_rn(g, __dadd_rn(r1, r2)), kInv4PiMex);
+    ubar = __ddiv_rn(ubar, den);
+  } else {
+    const double x2x1 = __dsub_rn(x2, x1), y2y1 = __dsub_rn(y2, y1), z2z1 = __dsub_rn(z2, z1);
+    const double L = __dadd_rn(__dadd_rn(__dmul_rn(x2x1, x2x1), __dmul_rn(y2y1, y2y1)),
+                               __dmul_rn(z2z1, z2z1));
+    const double ld = __dadd_rn(__dadd_rn(__dmul_rn(x2x1, pxx1), __dmul_rn(y2y1, pyy1)),
+                                __dmul_rn(z2z1, pzz1));
+    const double Ldr12 = __dmul_rn(ld, ld);
+    double Cnu = __dsub_rn(__dmul_rn(r1, r1), __ddiv_rn(Ldr12, L));
+    double base;
+    if (!kGeneralN || rp.n == 2.0) {
+      base = __dadd_rn(__dmul_rn(rc, rc), __dmul_rn(Cnu, Cnu));
+      Cnu = __dmul_rn(Cnu, __ddiv_rn(1.0, sqrt(base)));
+    } else {
+      base = __dadd_rn(pow(rc, rp.n), pow(Cnu, rp.n));
+      Cnu = __dmul_rn(Cnu, pow(base, -1.0 / rp.n));
+    }
+    ubar = __ddiv_rn(__dmul_rn(__ddiv_rn(__dmul_rn(Cnu, g), k4Pi), __dadd_rn(r1, r2)),
+                     __dmul_rn(r1tr2, __dadd_rn(r1tr2, r1dr2)));
+  }
+  if (isnan(ubar) || isinf(ubar) || (r1 > rp.co && r2 > rp.co)) ubar = 0.0;
+  ux = __dadd_rn(ux, __dmul_rn(ubar, __dsub_rn(__dmul_rn(pyy1, pzz2), __dmul_rn(pzz1, pyy2))));
+  uy = __dadd_rn(uy, __dmul_rn(ubar, __dsub_rn(__dmul_rn(pzz1, pxx2), __dmul_rn(pxx1, pzz2))));
+  uz = __dadd_rn(uz, __dmul_rn(ubar, __dsub_rn(__dmul_rn(pxx1, pyy2), __dmul_rn(pyy1, pxx2))));
+}
+
+}  // namespace winds

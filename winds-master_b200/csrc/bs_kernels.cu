@@ -1,0 +1,680 @@
+// bs_kernels.cu -- sm_100a kernels of the induced-velocity (Biot-Savart) direct
+// sum that replaces core/BiotSavart.m:80-116 and the BiotSavart_naive /
+// BiotSavart_sh kernels of cuda/source/BiotSavartMex.cu:131-193.
+//
+// Kernels
+//   bs_pack_filaments  MATLAB-layout F1/F2/gamma/rc -> packed SoA float4 tiles
+//                      (+ FP64 copies), the device-side replacement of the host
+//                      crunch_f / crunch_rg packing (BiotSavartMex.cu:316-357)
+//   bs_pack_targets    MATLAB-layout P -> double4 targets (crunch_p, :361-379)
+//   bs_f32c            persistent FP32 direct sum: filament tiles staged into
+//                      shared memory by bulk copies (cp.async.bulk + mbarrier),
+//                      T register-resident targets per thread, Kahan-compensated
+//                      per-target sums across tiles, FP64 recomputation of the
+//                      near-singular pairs
+//   bs_f64             plain FP64 direct sum (the comparison GPU path)
+//   bs_reduce          deterministic sum of the per-chunk partials, written in
+//                      MATLAB layout (reassem_uind, :383-401)
+//   bs_length          filament lengths (core/FilamentLength.m:27-44)
+#include "bs_device.cuh"
+#include "bs_launch.h"
+#include "bs_types.h"
+
+#include <cfloat>
+
+namespace winds {
+
+// --------------------------------------------------------------- packing
+__global__ void bs_bbox_init(BBox *bb) {
+  if (threadIdx.x == 0) {
+    for (int c = 0; c < 3; ++c) {
+      bb->tmin[c] = bb->fmin[c] = float_key(FLT_MAX);
+      bb->tmax[c] = bb->fmax[c] = float_key(-FLT_MAX);
+    }
+  }
+}
+
+// Block-level min/max of three floats, then one atomic per block and bound.
+__device__ __forceinline__ void bbox_accumulate(const float lo[3], const float hi[3], int *gmin,
+                                                int *gmax) {
+  __shared__ float smin[3][32], smax[3][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  float l[3] = {lo[0], lo[1], lo[2]}, h[3] = {hi[0], hi[1], hi[2]};
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    for (int o = 16; o > 0; o >>= 1) {
+      l[c] = fminf(l[c], __shfl_xor_sync(0xffffffffu, l[c], o));
+      h[c] = fmaxf(h[c], __shfl_xor_sync(0xffffffffu, h[c], o));
+    }
+    if (lane == 0) {
+      smin[c][warp] = l[c];
+      smax[c][warp] = h[c];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    const int c = threadIdx.x;
+    float a = FLT_MAX, b = -FLT_MAX;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      a = fminf(a, smin[c][w]);
+      b = fmaxf(b, smax[c][w]);
+    }
+    atomicMin(&gmin[c], float_key(a));
+    atomicMax(&gmax[c], float_key(b));
+  }
+}
+
+__global__ void bs_pack_filaments(const double *__restrict__ F1, const double *__restrict__ F2,
+                                  const double *__restrict__ gam, const double *__restrict__ rc,
+                                  long long d0, long long nf, long long off, int model, double dcut,
+                                  float4 *fa, float4 *fb, float4 *fc, float *fd, double4 *ra,
+                                  double4 *rb, BBox *bb) {
+  const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+  if (f < nf) {
+    const long long j = f / d0, i = f - j * d0;
+    const long long b = i + d0 * 3 * j;
+    const double x1 = F1[b], y1 = F1[b + d0], z1 = F1[b + 2 * d0];
+    const double x2 = F2[b], y2 = F2[b + d0], z2 = F2[b + 2 * d0];
+    const double g = gam[f], r = rc[f];
+    ra[off + f] = make_double4(x1, y1, z1, g);
+    rb[off + f] = make_double4(x2, y2, z2, r);
+    const double Lx = x2 - x1, Ly = y2 - y1, Lz = z2 - z1;
+    const double L2 = Lx * Lx + Ly * Ly + Lz * Lz;
+    double K = g / k4Pi;
+    // A NaN/Inf ubar is zeroed by the reference (core/BiotSavart.m:111); with
+    // finite endpoints that happens exactly when gamma (or, Vatistas, rc; or,
+    // cut-off, d*|L|^2) is not finite, so such filaments contribute nothing.
+    double D;
+    if (model == kCoreVatistas) {
+      D = (r * L2) * (r * L2);
+      if (!isfinite(r)) K = 0.0;
+      if (!(D >= 1e-30)) D = 1e-30;
+      if (D > 1e30) D = 1e30;
+    } else {
+      D = dcut * L2;
+      if (!isfinite(D)) K = 0.0, D = 0.0;
+    }
+    if (!isfinite(g)) K = 0.0;
+    // Near-singular region: r1.r2 < Rn^2, a ball around the midpoint of radius
+    // sqrt(|L|^2/4 + Rn^2) that contains every point within 3 core radii.
+    double Rn2 = L2;
+    if (isfinite(r) && 9.0 * r > Rn2) Rn2 = 9.0 * r;
+    if (!(Rn2 > 1e-20)) Rn2 = 1e-20;
+    const float hx = (float)x1, hy = (float)y1, hz = (float)z1;
+    fa[off + f] = make_float4(hx, hy, hz, (float)L2);
+    fb[off + f] = make_float4((float)(x1 - (double)hx), (float)(y1 - (double)hy),
+                              (float)(z1 - (double)hz), (float)Rn2);
+    fc[off + f] = make_float4((float)Lx, (float)Ly, (float)Lz, (float)K);
+    fd[off + f] = (float)D;
+    lo[0] = (float)fmin(x1, x2), lo[1] = (float)fmin(y1, y2), lo[2] = (float)fmin(z1, z2);
+    hi[0] = (float)fmax(x1, x2), hi[1] = (float)fmax(y1, y2), hi[2] = (float)fmax(z1, z2);
+  }
+  bbox_accumulate(lo, hi, bb->fmin, bb->fmax);
+}
+
+// Inert filaments filling [from, to): far away, zero length, zero circulation.
+__global__ void bs_pad_filaments(long long from, long long to, float4 *fa, float4 *fb, float4 *fc,
+                                 float *fd, double4 *ra, double4 *rb) {
+  const long long f = from + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= to) return;
+  const double far = 1e18;
+  fa[f] = make_float4((float)far, (float)far, (float)far, 0.f);
+  fb[f] = make_float4(0.f, 0.f, 0.f, 0.f);
+  fc[f] = make_float4(0.f, 0.f, 0.f, 0.f);
+  fd[f] = 1.f;
+  ra[f] = make_double4(far, far, far, 0.0);
+  rb[f] = make_double4(far, far, far, 0.0);
+}
+
+__global__ void bs_pack_targets(const double *__restrict__ P, long long ns, long long np,
+                                long long off, double4 *tp, BBox *bb) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+  if (t < np) {
+    const long long j = t / ns, i = t - j * ns;
+    const long long b = i + ns * 3 * j;
+    const double x = P[b], y = P[b + ns], z = P[b + 2 * ns];
+    tp[off + t] = make_double4(x, y, z, 0.0);
+    lo[0] = hi[0] = (float)x;
+    lo[1] = hi[1] = (float)y;
+    lo[2] = hi[2] = (float)z;
+  }
+  bbox_accumulate(lo, hi, bb->tmin, bb->tmax);
+}
+
+// Largest possible squared target-endpoint distance from the bounds; the
+// reach cut-off can only zero a term when co^2 is below it.
+__device__ __forceinline__ bool co_can_trigger(const BBox *bb, double co) {
+  double d2 = 0.0;
+  for (int c = 0; c < 3; ++c) {
+    const double a = (double)key_float(bb->tmax[c]) - (double)key_float(bb->fmin[c]);
+    const double b = (double)key_float(bb->fmax[c]) - (double)key_float(bb->tmin[c]);
+    const double m = fmax(fabs(a), fabs(b)) * (1.0 + 1e-6) + 1e-3;
+    d2 += m * m;
+  }
+  return co * co < d2;  // false for NaN co: r > NaN is never true
+}
+
+// ------------------------------------------------------- FP32 direct sum
+constexpr int kThreads = 128;
+constexpr int kStages = 4;
+constexpr uint64_t kDefaultWaitNs = 2000000000ull;  // 2 s per tile: far above any real latency
+
+template <int KF>
+struct StageSmem {
+  static constexpr int kBytes = KF * 52;  // fa, fb, fc: 16 B each; fd: 4 B
+};
+
+// Dynamic shared memory: kStages filament stages, then the per-target Kahan
+// state (sum, compensation) x 3 components as floats, then the barriers.
+template <int T, int KF>
+__host__ __device__ constexpr size_t f32c_smem_bytes_t() {
+  return (size_t)kStages * StageSmem<KF>::kBytes + (size_t)6 * kThreads * T * sizeof(float) +
+         kStages * sizeof(uint64_t);
+}
+
+// Kahan step: (sum, comp) += v.
+__device__ __forceinline__ void kahan_add(float &sum, float &comp, float v) {
+  const float y = __fsub_rn(v, comp);
+  const float s = __fadd_rn(sum, y);
+  comp = __fsub_rn(__fsub_rn(s, sum), y);
+  sum = s;
+}
+
+template <int KF>
+__device__ __forceinline__ void issue_stage(const F32cArgs &a, unsigned char *stage, uint64_t *bar,
+                                            int f0) {
+  mbar_arrive_expect_tx(bar, StageSmem<KF>::kBytes);
+  bulk_g2s(stage, a.fa + f0, KF * 16, bar);
+  bulk_g2s(stage + KF * 16, a.fb + f0, KF * 16, bar);
+  bulk_g2s(stage + KF * 32, a.fc + f0, KF * 16, bar);
+  bulk_g2s(stage + KF * 48, a.fd + f0, KF * 4, bar);
+}
+
+// One item: the thread's T targets against filaments [it.f_begin, it.f_end).
+// Returns false when a bounded wait ran out (the item is abandoned).
+template <int T, int KF, int MODEL, bool CO>
+__device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, const Tile &tl,
+                                          unsigned char *smem, uint64_t *full, float *s_k,
+                                          unsigned &gt, float (&px)[T], float (&py)[T],
+                                          float (&pz)[T], float cx, float cy, float cz,
+                                          unsigned &near_cnt) {
+  const int tid = threadIdx.x;
+  const int ntiles = (it.f_end - it.f_begin) / KF;
+  const float co2 = (float)(a.co * a.co);
+  RefParams rp;
+  rp.model = a.model;
+  rp.d = a.d;
+  rp.n = a.n;
+  rp.co = a.co;
+  if (tid == 0) {
+    for (int s = 0; s < kStages && s < ntiles; ++s) {
+      const int st = (gt + s) % kStages;
+      issue_stage<KF>(a, smem + st * StageSmem<KF>::kBytes, &full[st], it.f_begin + s * KF);
+    }
+  }
+  float ax[T], ay[T], az[T];
+#pragma unroll
+  for (int t = 0; t < T; ++t) ax[t] = ay[t] = az[t] = 0.f;
+
+  bool ok = true;
+  int i = 0;
+  for (; i < ntiles; ++i) {
+    const unsigned g = gt + i;
+    const int st = g % kStages;
+    const unsigned par = (g / kStages) & 1u;
+    bool timed_out = !mbar_wait_bounded(&full[st], par, a.err, a.wait_limit_ns);
+    const unsigned char *stage = smem + st * StageSmem<KF>::kBytes;
+    const float4 *sA = reinterpret_cast<const float4 *>(stage);
+    const float4 *sB = reinterpret_cast<const float4 *>(stage + KF * 16);
+    const float4 *sC = reinterpret_cast<const float4 *>(stage + KF * 32);
+    const float *sD = reinterpret_cast<const float *>(stage + KF * 48);
+    if (!timed_out) {
+#pragma unroll 2
+      for (int k = 0; k < KF; ++k) {
+        const float4 A = sA[k];
+        const float4 B = sB[k];
+        const float4 C = sC[k];
+        const float Dv = sD[k];
+        // x1 relative to this thread's centre, from its hi/lo split
+        const float xrx = (A.x - cx) + B.x, xry = (A.y - cy) + B.y, xrz = (A.z - cz) + B.z;
+        const float L2 = A.w, Rn2 = B.w;
+        const float Lx = C.x, Ly = C.y, Lz = C.z, K = C.w;
+        unsigned nb = 0;
+#pragma unroll
+        for (int t = 0; t < T; ++t) {
+          const float rx = px[t] - xrx, ry = py[t] - xry, rz = pz[t] - xrz;  // r1 = P - x1
+          // r1 x r2 = L x r1 (no cancellation for far or collinear points)
+          const float cxv = Ly * rz - Lz * ry;
+          const float cyv = Lz * rx - Lx * rz;
+          const float czv = Lx * ry - Ly * rx;
+          const float r1s = rx * rx + ry * ry + rz * rz;
+          const float Ld = Lx * rx + Ly * ry + Lz * rz;
+          const float dot = r1s - Ld;          // r1 . r2
+          const float r2s = dot + (L2 - Ld);   // |r1 - L|^2
+          const float i1 = rsqrt_approx(r1s), i2 = rsqrt_approx(r2s);
+          const float gg = i1 * i2;
+          const float e = fmaf(dot, gg, 1.f);  // 1 + cos(theta) >= 1 for far pairs
+          float ub;
+          if (MODEL == kCoreVatistas) {
+            // Cnu / (r1 r2 (r1 r2 + r1.r2)) with h^2 = |c|^2/|L|^2 and rc^4 folded:
+            // Cnu = |c|^2 / sqrt(|c|^4 + (rc^2 |L|^2)^2)
+            const float c2 = cxv * cxv + cyv * cyv + czv * czv;
+            const float q = fmaf(c2, c2, Dv);
+            ub = K * ((i1 + i2) * gg) * c2 * rsqrt_approx((e * e) * q);
+          } else {
+            // (r1+r2)/(r1r2(r1r2+r1.r2) + d|L|^2) = (i1+i2) gg / (e + d|L|^2 gg^2)
+            ub = K * ((i1 + i2) * gg) * rcp_approx(fmaf(Dv, gg * gg, e));
+          }
+          const bool nr = dot < Rn2;
+          bool skip = nr;
+          if (CO) skip = skip || (fminf(r1s, r2s) > co2);
+          if (nr) nb |= (1u << t);
+          if (!skip) {
+            ax[t] = fmaf(ub, cxv, ax[t]);
+            ay[t] = fmaf(ub, cyv, ay[t]);
+            az[t] = fmaf(ub, czv, az[t]);
+          }
+        }
+        if (__any_sync(0xffffffffu, nb != 0u)) {
+          // Near-singular pairs of this filament: the reference formula in FP64,
+          // added to the per-target Kahan state as an exact hi + lo pair.
+          const int fidx = it.f_begin + i * KF + k;
+          const double4 RA = a.ra[fidx];
+          const double4 RB = a.rb[fidx];
+#pragma unroll 1
+          for (int t = 0; t < T; ++t) {
+            if (nb & (1u << t)) {
+              int local = tid * T + t;
+              if (local >= tl.t_count) local = tl.t_count - 1;
+              const double4 p = a.tp[tl.t_begin + local];
+              double u[3] = {0.0, 0.0, 0.0};
+              ref_pair<false>(RA, RB, p.x, p.y, p.z, rp, u[0], u[1], u[2]);
+              const int sl = tid * T + t;
+#pragma unroll
+              for (int c = 0; c < 3; ++c) {
+                const float hi = (float)u[c];
+                const float lo = (float)(u[c] - (double)hi);
+                float &sum = s_k[(2 * c) * kThreads * T + sl];
+                float &cmp = s_k[(2 * c + 1) * kThreads * T + sl];
+                kahan_add(sum, cmp, hi);
+                kahan_add(sum, cmp, lo);
+              }
+              ++near_cnt;
+            }
+          }
+        }
+      }
+      // Kahan-fold this tile's partial sums into the per-target totals.
+#pragma unroll
+      for (int t = 0; t < T; ++t) {
+        const int sl = tid * T + t;
+        kahan_add(s_k[0 * kThreads * T + sl], s_k[1 * kThreads * T + sl], ax[t]);
+        kahan_add(s_k[2 * kThreads * T + sl], s_k[3 * kThreads * T + sl], ay[t]);
+        kahan_add(s_k[4 * kThreads * T + sl], s_k[5 * kThreads * T + sl], az[t]);
+        ax[t] = ay[t] = az[t] = 0.f;
+      }
+    }
+    // Every thread is done with this stage before it is refilled.
+    if (__syncthreads_or(timed_out)) {
+      ok = false;
+      break;
+    }
+    if (tid == 0 && i + kStages < ntiles) {
+      issue_stage<KF>(a, smem + st * StageSmem<KF>::kBytes, &full[st],
+                      it.f_begin + (i + kStages) * KF);
+    }
+  }
+  if (!ok) {
+    // Let the copies already issued for this item land (bounded) before the
+    // CTA leaves, so no bulk copy targets shared memory of a finished CTA.
+    if (tid == 0) {
+      for (int j = i; j < ntiles && j < i + kStages; ++j) {
+        const unsigned g = gt + j;
+        mbar_wait_bounded(&full[g % kStages], (g / kStages) & 1u, a.err, a.wait_limit_ns);
+      }
+    }
+    return false;
+  }
+  gt += ntiles;
+  return true;
+}
+
+template <int T, int KF, int MODEL>
+__global__ void __launch_bounds__(kThreads) bs_f32c(const F32cArgs a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  float *s_k = reinterpret_cast<float *>(smem + kStages * StageSmem<KF>::kBytes);
+  uint64_t *full = reinterpret_cast<uint64_t *>(s_k + 6 * kThreads * T);
+  __shared__ int s_item;
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    for (int s = 0; s < kStages; ++s) mbar_init(&full[s], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  const bool co_on = co_can_trigger(a.bbox, a.co);
+  unsigned gt = 0;
+  unsigned near_cnt = 0;
+  while (true) {
+    if (tid == 0) s_item = (int)atomicAdd(a.work_ctr, 1u);
+    __syncthreads();
+    const int item_id = s_item;
+    __syncthreads();
+    if (item_id >= a.n_items) break;
+    const Item it = a.items[item_id];
+    const Tile tl = a.tiles[it.tile];
+    if (tl.t_count <= 0 || ((it.f_end - it.f_begin) % KF) != 0) {
+      if (tid == 0) atomicOr(a.err, kErrBadItem);
+      continue;
+    }
+    // This thread's T consecutive targets, relative to the FP32 image of the first.
+    float px[T], py[T], pz[T];
+    int l0 = tid * T;
+    if (l0 >= tl.t_count) l0 = tl.t_count - 1;
+    const double4 p0 = a.tp[tl.t_begin + l0];
+    const float cx = (float)p0.x, cy = (float)p0.y, cz = (float)p0.z;
+#pragma unroll
+    for (int t = 0; t < T; ++t) {
+      int l = tid * T + t;
+      if (l >= tl.t_count) l = tl.t_count - 1;
+      const double4 p = a.tp[tl.t_begin + l];
+      px[t] = (float)(p.x - (double)cx);
+      py[t] = (float)(p.y - (double)cy);
+      pz[t] = (float)(p.z - (double)cz);
+#pragma unroll
+      for (int c = 0; c < 6; ++c) s_k[c * kThreads * T + tid * T + t] = 0.f;
+    }
+    bool ok;
+    if (co_on)
+      ok = f32c_item<T, KF, MODEL, true>(a, it, tl, smem, full, s_k, gt, px, py, pz, cx, cy, cz,
+                                         near_cnt);
+    else
+      ok = f32c_item<T, KF, MODEL, false>(a, it, tl, smem, full, s_k, gt, px, py, pz, cx, cy, cz,
+                                          near_cnt);
+    if (!ok) return;
+    double *part = a.part + (size_t)item_id * 3 * a.tile_cap;
+#pragma unroll
+    for (int t = 0; t < T; ++t) {
+      const int l = tid * T + t;
+      if (l < tl.t_count) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          part[c * a.tile_cap + l] = (double)s_k[(2 * c) * kThreads * T + l] -
+                                     (double)s_k[(2 * c + 1) * kThreads * T + l];
+      }
+    }
+  }
+  if (a.near_ctr && near_cnt) atomicAdd(a.near_ctr, (unsigned long long)near_cnt);
+}
+
+// ------------------------------------------------------- FP64 direct sum
+constexpr int kF64Threads = 128;
+constexpr int kF64Tile = 128;  // filaments per shared-memory stage
+
+__global__ void __launch_bounds__(kF64Threads) bs_f64(const F32cArgs a) {
+  __shared__ double4 sA[2][kF64Tile], sB[2][kF64Tile];
+  __shared__ int s_item;
+  const int tid = threadIdx.x;
+  RefParams rp;
+  rp.model = a.model;
+  rp.d = a.d;
+  rp.n = a.n;
+  rp.co = a.co;
+  while (true) {
+    if (tid == 0) s_item = (int)atomicAdd(a.work_ctr, 1u);
+    __syncthreads();
+    const int item_id = s_item;
+    __syncthreads();
+    if (item_id >= a.n_items) break;
+    const Item it = a.items[item_id];
+    const Tile tl = a.tiles[it.tile];
+    int l = tid < tl.t_count ? tid : tl.t_count - 1;
+    const double4 p = a.tp[tl.t_begin + l];
+    double ux = 0.0, uy = 0.0, uz = 0.0;
+    const int ntiles = (it.f_end - it.f_begin) / kF64Tile;
+    // stage 0
+    sA[0][tid] = a.ra[it.f_begin + tid];
+    sB[0][tid] = a.rb[it.f_begin + tid];
+    __syncthreads();
+    for (int i = 0; i < ntiles; ++i) {
+      const int b = i & 1;
+      double4 nA, nB;
+      const bool more = i + 1 < ntiles;
+      if (more) {
+        nA = a.ra[it.f_begin + (i + 1) * kF64Tile + tid];
+        nB = a.rb[it.f_begin + (i + 1) * kF64Tile + tid];
+      }
+      for (int k = 0; k < kF64Tile; ++k) ref_pair(sA[b][k], sB[b][k], p.x, p.y, p.z, rp, ux, uy, uz);
+      if (more) {
+        sA[b ^ 1][tid] = nA;
+        sB[b ^ 1][tid] = nB;
+      }
+      __syncthreads();
+    }
+    if (tid < tl.t_count) {
+      double *part = a.part + (size_t)item_id * 3 * a.tile_cap;
+      part[tid] = ux;
+      part[a.tile_cap + tid] = uy;
+      part[2 * a.tile_cap + tid] = uz;
+    }
+  }
+}
+
+// --------------------------------------------------------------- reduce
+__global__ void bs_reduce(const Tile *__restrict__ tiles, const Group *__restrict__ groups,
+                          const double *__restrict__ part, int tile_cap) {
+  const Tile tl = tiles[blockIdx.x];
+  const Group g = groups[tl.group];
+  for (int l = threadIdx.x; l < tl.t_count; l += blockDim.x) {
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    for (int k = 0; k < tl.n_items; ++k) {
+      const double *p = part + (size_t)(tl.first_item + k) * 3 * tile_cap;
+      s0 += p[l];
+      s1 += p[tile_cap + l];
+      s2 += p[2 * tile_cap + l];
+    }
+    const long long local = tl.t_begin - g.t_begin + l;
+    const long long j = local / g.ns_p, i = local - j * g.ns_p;
+    double *o = g.out + i + 3 * g.ns_p * j;
+    if (g.accumulate) {
+      o[0] += s0;
+      o[g.ns_p] += s1;
+      o[2 * g.ns_p] += s2;
+    } else {
+      o[0] = s0;
+      o[g.ns_p] = s1;
+      o[2 * g.ns_p] = s2;
+    }
+  }
+}
+
+// --------------------------------------------------------------- lengths
+__global__ void bs_length(const double *__restrict__ F1, const double *__restrict__ F2,
+                          long long d0, long long nf, double *L) {
+  const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= nf) return;
+  const long long j = f / d0, i = f - j * d0;
+  const long long b = i + d0 * 3 * j;
+  const double dx = F2[b] - F1[b], dy = F2[b + d0] - F1[b + d0], dz = F2[b + 2 * d0] - F1[b + 2 * d0];
+  L[f] = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+}
+
+// ------------------------------------------------------- FP32 FMA peak probe
+// Each thread runs 8 independent FMA chains; nothing but FFMA issues in the
+// loop body, so the rate is the FP32 pipe's (the direct sum's roofline).
+__global__ void __launch_bounds__(256) bs_ffma_peak(float *out, int iters, float a, float b) {
+  float x0 = threadIdx.x * 1e-7f, x1 = x0 + 1e-3f, x2 = x0 + 2e-3f, x3 = x0 + 3e-3f;
+  float x4 = x0 + 4e-3f, x5 = x0 + 5e-3f, x6 = x0 + 6e-3f, x7 = x0 + 7e-3f;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      x0 = fmaf(x0, a, b);
+      x1 = fmaf(x1, a, b);
+      x2 = fmaf(x2, a, b);
+      x3 = fmaf(x3, a, b);
+      x4 = fmaf(x4, a, b);
+      x5 = fmaf(x5, a, b);
+      x6 = fmaf(x6, a, b);
+      x7 = fmaf(x7, a, b);
+    }
+  }
+  const float r = ((x0 + x1) + (x2 + x3)) + ((x4 + x5) + (x6 + x7));
+  if (r == 12345.678f) out[blockIdx.x * blockDim.x + threadIdx.x] = r;  // keeps the chains live
+}
+
+// ------------------------------------------------------- bounded-wait self-test
+// Waits on an mbarrier that nothing arrives on, with the given limit; the
+// bounded wait must give up, set the error word and let the kernel return.
+__global__ void bs_wait_selftest(unsigned *err, unsigned long long limit_ns) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) mbar_wait_bounded(&bar, 0u, err, limit_ns);
+  __syncthreads();
+}
+
+// ============================================================ host launchers
+namespace {
+template <int T, int KF, int MODEL>
+cudaError_t launch_f32c_t(const F32cArgs &a, int grid, cudaStream_t s) {
+  const size_t smem = f32c_smem_bytes_t<T, KF>();
+  static unsigned attr_set = 0;  // one bit per device: the attribute is per context
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 32 || !(attr_set & (1u << dev))) {
+    cudaError_t e = cudaFuncSetAttribute(bs_f32c<T, KF, MODEL>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    if (dev < 32) attr_set |= (1u << dev);
+  }
+  bs_f32c<T, KF, MODEL><<<grid, kThreads, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <int T, int KF, int MODEL>
+int occupancy_t() {
+  const size_t smem = f32c_smem_bytes_t<T, KF>();
+  cudaFuncSetAttribute(bs_f32c<T, KF, MODEL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)smem);
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bs_f32c<T, KF, MODEL>, kThreads, smem) !=
+      cudaSuccess)
+    return 1;
+  return n > 0 ? n : 1;
+}
+
+#define WINDS_F32C_DISPATCH(FN, ...)                                    \
+  switch (model * 100 + T * 10 + (KF == 32 ? 0 : KF == 64 ? 1 : 2)) {   \
+    case 0 * 100 + 20 + 0: return FN<2, 32, 0>(__VA_ARGS__);             \
+    case 0 * 100 + 20 + 1: return FN<2, 64, 0>(__VA_ARGS__);             \
+    case 0 * 100 + 40 + 0: return FN<4, 32, 0>(__VA_ARGS__);             \
+    case 0 * 100 + 40 + 1: return FN<4, 64, 0>(__VA_ARGS__);             \
+    case 0 * 100 + 80 + 0: return FN<8, 32, 0>(__VA_ARGS__);             \
+    case 0 * 100 + 80 + 1: return FN<8, 64, 0>(__VA_ARGS__);             \
+    case 1 * 100 + 20 + 0: return FN<2, 32, 1>(__VA_ARGS__);             \
+    case 1 * 100 + 20 + 1: return FN<2, 64, 1>(__VA_ARGS__);             \
+    case 1 * 100 + 40 + 0: return FN<4, 32, 1>(__VA_ARGS__);             \
+    case 1 * 100 + 40 + 1: return FN<4, 64, 1>(__VA_ARGS__);             \
+    case 1 * 100 + 80 + 0: return FN<8, 32, 1>(__VA_ARGS__);             \
+    case 1 * 100 + 80 + 1: return FN<8, 64, 1>(__VA_ARGS__);             \
+    default: break;                                                      \
+  }
+}  // namespace
+
+bool f32c_config_supported(int T, int KF) {
+  return (T == 2 || T == 4 || T == 8) && (KF == 32 || KF == 64);
+}
+
+int f32c_threads() { return kThreads; }
+int f64_threads() { return kF64Threads; }
+int f64_tile() { return kF64Tile; }
+
+cudaError_t launch_f32c(const F32cArgs &a, int model, int T, int KF, int grid, cudaStream_t s) {
+  WINDS_F32C_DISPATCH(launch_f32c_t, a, grid, s)
+  return cudaErrorInvalidValue;
+}
+
+int f32c_occupancy(int model, int T, int KF) {
+  WINDS_F32C_DISPATCH(occupancy_t)
+  return 1;
+}
+
+int f64_occupancy() {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bs_f64, kF64Threads, 0) != cudaSuccess)
+    return 1;
+  return n > 0 ? n : 1;
+}
+
+cudaError_t launch_f64(const F32cArgs &a, int grid, cudaStream_t s) {
+  bs_f64<<<grid, kF64Threads, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bbox_init(BBox *bb, cudaStream_t s) {
+  bs_bbox_init<<<1, 32, 0, s>>>(bb);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pack_filaments(const double *F1, const double *F2, const double *gam,
+                                  const double *rc, long long d0, long long nf, long long off,
+                                  int model, double dcut, const PackedFilaments &pf, BBox *bb,
+                                  cudaStream_t s) {
+  if (nf <= 0) return cudaSuccess;
+  const int bs = 256;
+  const long long grid = (nf + bs - 1) / bs;
+  bs_pack_filaments<<<(unsigned)grid, bs, 0, s>>>(F1, F2, gam, rc, d0, nf, off, model, dcut, pf.fa,
+                                                 pf.fb, pf.fc, pf.fd, pf.ra, pf.rb, bb);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pad_filaments(long long from, long long to, const PackedFilaments &pf,
+                                 cudaStream_t s) {
+  if (to <= from) return cudaSuccess;
+  const int bs = 256;
+  const long long grid = (to - from + bs - 1) / bs;
+  bs_pad_filaments<<<(unsigned)grid, bs, 0, s>>>(from, to, pf.fa, pf.fb, pf.fc, pf.fd, pf.ra, pf.rb);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pack_targets(const double *P, long long ns, long long np, long long off,
+                                double4 *tp, BBox *bb, cudaStream_t s) {
+  if (np <= 0) return cudaSuccess;
+  const int bs = 256;
+  const long long grid = (np + bs - 1) / bs;
+  bs_pack_targets<<<(unsigned)grid, bs, 0, s>>>(P, ns, np, off, tp, bb);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reduce(const Tile *tiles, int n_tiles, const Group *groups, const double *part,
+                          int tile_cap, cudaStream_t s) {
+  if (n_tiles <= 0) return cudaSuccess;
+  bs_reduce<<<n_tiles, 256, 0, s>>>(tiles, groups, part, tile_cap);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_length(const double *F1, const double *F2, long long d0, long long nf, double *L,
+                          cudaStream_t s) {
+  if (nf <= 0) return cudaSuccess;
+  const int bs = 256;
+  bs_length<<<(unsigned)((nf + bs - 1) / bs), bs, 0, s>>>(F1, F2, d0, nf, L);
+  return cudaGetLastError();
+}
+
+unsigned long long default_wait_limit_ns() { return kDefaultWaitNs; }
+
+cudaError_t launch_ffma_peak(float *out, int blocks, int iters, cudaStream_t s) {
+  bs_ffma_peak<<<blocks, 256, 0, s>>>(out, iters, 0.999999f, 1e-7f);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wait_selftest(unsigned *err, unsigned long long limit_ns, cudaStream_t s) {
+  bs_wait_selftest<<<1, 32, 0, s>>>(err, limit_ns);
+  return cudaGetLastError();
+}
+
+}  // namespace winds

@@ -1,0 +1,46 @@
+// bs_launch.h -- host-side launchers of the induced-velocity kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "bs_types.h"
+
+namespace winds {
+
+struct PackedFilaments {
+  float4 *fa, *fb, *fc;
+  float *fd;
+  double4 *ra, *rb;
+};
+
+// Filament ranges of work items are multiples of this (a multiple of every
+// FP32 tile size and of the FP64 stage).
+constexpr int kFilamentPad = 128;
+
+bool f32c_config_supported(int T, int KF);
+int f32c_threads();
+int f64_threads();
+int f64_tile();
+int f32c_occupancy(int model, int T, int KF);
+int f64_occupancy();
+unsigned long long default_wait_limit_ns();
+
+cudaError_t launch_bbox_init(BBox *bb, cudaStream_t s);
+cudaError_t launch_pack_filaments(const double *F1, const double *F2, const double *gam,
+                                  const double *rc, long long d0, long long nf, long long off,
+                                  int model, double dcut, const PackedFilaments &pf, BBox *bb,
+                                  cudaStream_t s);
+cudaError_t launch_pad_filaments(long long from, long long to, const PackedFilaments &pf,
+                                 cudaStream_t s);
+cudaError_t launch_pack_targets(const double *P, long long ns, long long np, long long off,
+                                double4 *tp, BBox *bb, cudaStream_t s);
+cudaError_t launch_f32c(const F32cArgs &a, int model, int T, int KF, int grid, cudaStream_t s);
+cudaError_t launch_f64(const F32cArgs &a, int grid, cudaStream_t s);
+cudaError_t launch_reduce(const Tile *tiles, int n_tiles, const Group *groups, const double *part,
+                          int tile_cap, cudaStream_t s);
+cudaError_t launch_ffma_peak(float *out, int blocks, int iters, cudaStream_t s);
+cudaError_t launch_wait_selftest(unsigned *err, unsigned long long limit_ns, cudaStream_t s);
+cudaError_t launch_length(const double *F1, const double *F2, long long d0, long long nf, double *L,
+                          cudaStream_t s);
+
+}  // namespace winds

@@ -1,0 +1,77 @@
+// bs_types.h -- plain structs shared by the host engine and the kernels.
+//
+// HBM layout of one evaluation (all per-context, grow-only buffers):
+//   packed filaments, padded to the filament tile (KF) with inert entries
+//     fa[f] = (x1_hi.x, x1_hi.y, x1_hi.z, |L|^2)   float4
+//     fb[f] = (x1_lo.x, x1_lo.y, x1_lo.z, Rn^2)    float4  (x1 = hi + lo exactly to ~2^-48)
+//     fc[f] = (L.x, L.y, L.z, gamma/4pi)           float4  (L = x2 - x1)
+//     fd[f] = (rc^2 |L|^2)^2 (Vatistas) or d |L|^2 (cut-off)   float
+//   raw FP64 filaments for near-singular terms and the FP64 path
+//     ra[f] = (x1, y1, z1, gamma)  rb[f] = (x2, y2, z2, rc^2)   double4
+//   targets  tp[t] = (x, y, z, 0) double4
+//   partial sums per work item: part[item][3][tile_cap] double
+#pragma once
+
+#include <stdint.h>
+
+namespace winds {
+
+enum : int { kCoreCutoff = 0, kCoreVatistas = 1 };
+
+enum : unsigned {
+  kErrWaitTimeout = 1u,  // a bounded mbarrier wait ran out
+  kErrBadItem = 2u,      // a work item pointed outside its tables
+};
+
+struct Group {          // one target set evaluated against one filament range
+  double *out;          // MATLAB-layout output [ns_p, 3, ...]
+  long long t_begin;    // first packed target
+  long long t_count;
+  long long ns_p;       // first dimension of the output layout
+  int f_begin;          // packed filament range, multiples of the tile size
+  int f_end;
+  int accumulate;       // 1: out += result, 0: out = result
+  int pad;
+};
+
+struct Tile {           // tile_cap consecutive targets of one group
+  long long t_begin;
+  int t_count;
+  int group;
+  int first_item;
+  int n_items;
+};
+
+struct Item {           // one tile against one filament chunk
+  int tile;
+  int f_begin;
+  int f_end;
+  int pad;
+};
+
+struct BBox {           // ordered-int keys of float bounds (see float_key)
+  int tmin[3], tmax[3]; // targets
+  int fmin[3], fmax[3]; // filament endpoints
+};
+
+struct F32cArgs {
+  const float4 *fa, *fb, *fc;
+  const float *fd;
+  const double4 *ra, *rb;
+  const double4 *tp;
+  const Group *groups;
+  const Tile *tiles;
+  const Item *items;
+  int n_items;
+  int tile_cap;
+  double *part;
+  unsigned *work_ctr;
+  unsigned *err;
+  unsigned long long *near_ctr;
+  const BBox *bbox;
+  int model;
+  double d, n, co;
+  unsigned long long wait_limit_ns;
+};
+
+}  // namespace winds

@@ -1,0 +1,86 @@
+// engine.h -- internal host-side types of libwinds_bs (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "bs_types.h"
+#include "winds_bs.h"
+
+namespace winds {
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  int ensure(size_t bytes, cudaStream_t s);  // grows (after a stream sync); keeps no contents
+  void release();
+};
+
+struct HostBuf {  // pinned
+  void *p = nullptr;
+  size_t cap = 0;
+  int ensure(size_t bytes);
+  void release();
+};
+
+struct TargetSpec {
+  const double *P;  // device, MATLAB layout [ns, 3, ...]
+  long long ns;
+  long long count;
+  double *out;      // device, P's layout
+  int accumulate;
+};
+
+struct GroupSpec {
+  double *out;
+  long long t_begin, t_count, ns_p;
+  int f_begin, f_end;
+  int accumulate;
+};
+
+struct Plan {
+  int tile_cap = 0;
+  std::vector<Group> groups;
+  std::vector<Tile> tiles;
+  std::vector<Item> items;
+};
+
+struct TuneChoice {
+  int T = 8;
+  int KF = 64;
+  double waves = 8.0;
+};
+
+struct Context {
+  int dev = 0;
+  int num_sms = 0;
+  int cc_major = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev_main0 = nullptr, ev_main1 = nullptr, ev_upload = nullptr;
+  // packed inputs
+  DevBuf fa, fb, fc, fd, ra, rb, tp;
+  // plan tables and partial sums
+  DevBuf groups, tiles, items, part;
+  // small words
+  DevBuf bbox, ctr, err, nearctr;
+  // device copies of host inputs/outputs (host API)
+  DevBuf in_P, in_F, out_u;
+  HostBuf htab, hstat;
+  Plan plan;
+  int launches = 0;
+  bool timed = false;
+  bool autotune = true;
+};
+
+int fail(int code, const char *fmt, ...);
+int cuda_fail(cudaError_t e, const char *what);
+Context *get_context(int *rc);
+int eval_device(Context *c, const winds_bs_family *fams, int nfam,
+                const std::vector<TargetSpec> &tsets, const winds_bs_params *prm, cudaStream_t s,
+                bool sequential);
+int autotune(Context *c, const std::vector<GroupSpec> &gs, int model, double dcut, double n,
+             double co, long long nt, long long nf, TuneChoice *best);
+int check_device_error(Context *c, cudaStream_t s);
+
+}  // namespace winds
