@@ -40,10 +40,16 @@ UNIT = "Gint/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison")
+    ap.add_argument("--workload", default="large", choices=["large", "medium"],
+                    help="large: 3x41x720 (the metric's case); medium: 3x41x180 for profiling")
+    ap.add_argument("--tiling", default=None,
+                    help="force the FP32 tiling 'T,KF,waves' instead of the autotuner's choice")
+    ap.add_argument("--quick", action="store_true",
+                    help="timed loop only (no FP64 comparison, e2e or CPU baseline)")
     return ap.parse_args()
 
 
@@ -59,23 +65,35 @@ class ClockSampler:
         self.idx = str(gpu_index)
         self.rows = []
         self.proc = None
+        self.mark = 0
 
-    def start(self):
+    def start(self, wait_s=5.0):
+        """Starts sampling and waits until the first sample arrives."""
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
         except OSError:
             self.proc = None
             return
         self.th = threading.Thread(target=self._read, daemon=True)
         self.th.start()
+        t0 = time.time()
+        while not self.rows and time.time() - t0 < wait_s and self.proc.poll() is None:
+            time.sleep(0.02)
+
+    def begin(self):
+        """Marks the start of the timed region (samples before it are dropped)."""
+        self.mark = len(self.rows)
 
     def _read(self):
+        self.errors = []
         for line in self.proc.stdout:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) >= 9 and parts[0] == self.idx:
                 self.rows.append(parts)
+            elif len(self.errors) < 3:
+                self.errors.append(line.strip())
 
     def stop(self):
         if self.proc is None:
@@ -86,17 +104,24 @@ class ClockSampler:
         except subprocess.TimeoutExpired:
             self.proc.kill()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
-        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[5 + k].lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+        rows = self.rows[self.mark:] or self.rows[-1:]
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        out = {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+               "reasons": reasons, "samples": len(self.rows) - self.mark}
+        if not self.rows and getattr(self, "errors", None):
+            out["error"] = " | ".join(self.errors)
+        return out
 
 
 # ------------------------------------------------------------------ workload
-def workload(seed):
+def workload(seed, kind="large"):
     synth = importlib.import_module("winds-master_b200.synth")
-    w = synth.make_wake(synth.large_case(seed=seed))
+    case = synth.large_case(seed=seed)
+    if kind == "medium":
+        case.nsteps = 180
+    w = synth.make_wake(case)
     fams = [synth.shed_filaments(w["dom"]) + (w["gamma_shed"], w["rc_shed"]),
             synth.trail_filaments(w["dom"]) + (w["gamma_trail"], w["rc_trail"])]
     pts = np.concatenate([synth.flat_points(w["dom"]), synth.flat_points(w["ll"])])
@@ -125,7 +150,7 @@ def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    _, fams, P, nf, nt = workload(1)
+    _, fams, P, nf, nt = workload(1, args.workload)
     cores = os.cpu_count()
     # size one step to about 3 s of CPU work
     rate, _ = cpu_rate(fams, P, 16)
@@ -167,7 +192,7 @@ def ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     wb = importlib.import_module("winds-master_b200")
     lib = wb.lib()
-    w, fams, P, nf, nt = workload(1 + rank)
+    w, fams, P, nf, nt = workload(1 + rank, args.workload)
     interactions = nf * nt
 
     def dev(a):
@@ -179,21 +204,30 @@ def ours(args):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     core = wb.bs.CORE_VATISTAS
 
-    # warm-up on the library stream (the first call autotunes the tiling)
+    torch.cuda.synchronize()
+    if args.tiling:
+        T, KF, waves = args.tiling.split(",")
+        wb.set_tuning(wb.bs.CORE_VATISTAS, nt, nf, int(T), int(KF), float(waves))
+    # warm-up on the library's own stream (the first call autotunes the tiling)
     for _ in range(max(1, args.warmup)):
         wb.eval_device(dfams, dP, core, 2.0, 1000.0, out, "f32c")
     wb.sync()
-    stream = torch.cuda.current_stream()
+    # timed work runs on a dedicated (non-default) stream shared with the events
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     sp = stream.cuda_stream
+    for _ in range(2):
+        wb.eval_device(dfams, dP, core, 2.0, 1000.0, out, "f32c", stream=sp)
     peak = C.c_double()
     lib.winds_bs_fp32_peak(C.byref(peak))
 
     clocks = ClockSampler(torch.cuda.current_device() if "CUDA_VISIBLE_DEVICES" not in os.environ
                           else int(os.environ["CUDA_VISIBLE_DEVICES"].split(",")[local]))
+    clocks.start()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    clocks.start()
+    clocks.begin()
     step_ms, main_ms = [], []
     launches = 0
     near_pairs = 0
@@ -224,7 +258,7 @@ def ours(args):
     # plain FP64 GPU direct sum (the comparison path) and the accuracy of FP32c against it
     fp64 = None
     rel_err = None
-    if not args.no_fp64:
+    if not (args.no_fp64 or args.quick):
         out64 = torch.zeros_like(out)
         wb.eval_device(dfams, dP, core, 2.0, 1000.0, out64, "f64", stream=sp)
         torch.cuda.synchronize()
@@ -245,19 +279,23 @@ def ours(args):
         rel_err = float(np.max(np.linalg.norm(a - b, axis=1) / np.linalg.norm(b, axis=1)))
 
     # end to end through the public host API: pinned host inputs, H2D + eval + D2H per step
-    pin = lambda a: torch.from_numpy(np.asfortranarray(a)).pin_memory().numpy()
-    hfams = [tuple(pin(x) for x in f) for f in fams]
-    hP = pin(P)
-    h2d = sum(sum(x.nbytes for x in f) for f in hfams) + hP.nbytes
-    d2h = hP.nbytes
-    wb.eval_host(hfams, hP, core, 2.0, 1000.0, "f32c")
-    e2e_t = []
-    for _ in range(max(1, min(args.steps, 5))):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
+    e2e_line = None
+    if not args.quick:
+        pin = lambda a: torch.from_numpy(np.asfortranarray(a)).pin_memory().numpy()
+        hfams = [tuple(pin(x) for x in f) for f in fams]
+        hP = pin(P)
+        h2d = sum(sum(x.nbytes for x in f) for f in hfams) + hP.nbytes
+        d2h = hP.nbytes
         wb.eval_host(hfams, hP, core, 2.0, 1000.0, "f32c")
-        e2e_t.append(time.perf_counter() - t0)
-    e2e = world * interactions / statistics.median(e2e_t) / 1e9
+        e2e_t = []
+        for _ in range(max(1, min(args.steps, 5))):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            wb.eval_host(hfams, hP, core, 2.0, 1000.0, "f32c")
+            e2e_t.append(time.perf_counter() - t0)
+        e2e = world * interactions / statistics.median(e2e_t) / 1e9
+        e2e_line = {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "timing": "wall clock around the synchronous host-API call"}
 
     mean_main = statistics.mean(main_ms)
     achieved = FLOP_PER_INTERACTION * interactions / (mean_main * 1e-3) / 1e12
@@ -268,7 +306,7 @@ def ours(args):
         traffic = tj.get("bytes_per_interaction", 0.0) * interactions
 
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not args.quick:
         rate, _ = cpu_rate(fams, P, 16)
         n = int(max(16, min(nt, 10.0 * rate * 1e9 / nf)))
         rate, dt = cpu_rate(fams, P, n, seed=1)
@@ -281,8 +319,9 @@ def ours(args):
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic",
-            "config": {"workload": "helical wake 3x41x720 (1 deg), Vatistas n=2, all shed+trailing "
-                       "filaments onto all wake nodes + lifting-line points", "targets": nt,
+            "config": {"workload": f"helical wake 3x41x{720 if args.workload == 'large' else 180} (1 deg), "
+                       "Vatistas n=2, all shed+trailing filaments onto all wake nodes + lifting-line "
+                       "points", "targets": nt,
                        "filaments": nf, "interactions_per_step": interactions,
                        "l2": "256 MB buffer written between timed steps",
                        "parallelism": f"replicated wakes x{world}" if world > 1 else "single GPU"},
@@ -292,14 +331,15 @@ def ours(args):
                          "kernel": "bs_f32c", "flop_per_interaction": FLOP_PER_INTERACTION,
                          "kernel_ms": mean_main},
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "timing": "wall clock around the synchronous host-API call"},
+            "e2e": e2e_line,
             "gpu_launches": launches,
             "clocks": clk,
             "plain_fp64_gint_per_s": fp64,
             "speedup_vs_plain_fp64": (value / world / fp64) if fp64 else None,
             "rel_err_max_vs_fp64": rel_err,
             "near_pairs_per_step": near_pairs,
+            "tiling": dict(zip(("targets_per_thread", "filaments_per_tile", "waves"),
+                               wb.get_tuning(core, nt, nf))),
         }
         print(json.dumps(line), flush=True)
     if world > 1:

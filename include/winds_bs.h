@@ -115,7 +115,7 @@ int winds_bs_sync(void *stream);
 
 /* Autotuner control. The first FP32 evaluation of a (core model, log2 targets,
  * log2 filaments) bucket on the library's own stream times the candidate
- * tilings (targets per thread T in {2,4,8}, filaments per tile KF in {32,64},
+ * tilings (targets per thread T in {2,4,8}, filaments per tile KF in {32,64,128},
  * work-queue depth) and caches the fastest; set_tuning / get_tuning read and
  * write that cache directly (e.g. to restore a saved choice). */
 int winds_bs_set_autotune(int on);

@@ -22,6 +22,8 @@
 
 #include <cfloat>
 
+#include <cub/device/device_radix_sort.cuh>
+
 namespace winds {
 
 // --------------------------------------------------------------- packing
@@ -128,7 +130,7 @@ __global__ void bs_pad_filaments(long long from, long long to, float4 *fa, float
 }
 
 __global__ void bs_pack_targets(const double *__restrict__ P, long long ns, long long np,
-                                long long off, double4 *tp, BBox *bb) {
+                                long long off, int group, double4 *tp, int *tgroup, BBox *bb) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
   if (t < np) {
@@ -136,11 +138,49 @@ __global__ void bs_pack_targets(const double *__restrict__ P, long long ns, long
     const long long b = i + ns * 3 * j;
     const double x = P[b], y = P[b + ns], z = P[b + 2 * ns];
     tp[off + t] = make_double4(x, y, z, 0.0);
+    tgroup[off + t] = group;
     lo[0] = hi[0] = (float)x;
     lo[1] = hi[1] = (float)y;
     lo[2] = hi[2] = (float)z;
   }
   bbox_accumulate(lo, hi, bb->tmin, bb->tmax);
+}
+
+// Spreads the low 10 bits of v so that they occupy every third bit.
+__device__ __forceinline__ unsigned long long spread3(unsigned v) {
+  unsigned long long x = v & 0x3ffu;
+  x = (x | (x << 16)) & 0x30000ffull;
+  x = (x | (x << 8)) & 0x300f00full;
+  x = (x | (x << 4)) & 0x30c30c3ull;
+  x = (x | (x << 2)) & 0x9249249ull;
+  return x;
+}
+
+// Sort key of a target: group id above a 30-bit Morton code of its position
+// in the targets' bounding box.
+__global__ void bs_target_keys(const double4 *__restrict__ tp, const int *__restrict__ tgroup,
+                               long long n, const BBox *bb, unsigned long long *keys, int *vals) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const double4 p = tp[t];
+  const double q[3] = {p.x, p.y, p.z};
+  unsigned long long code = 0;
+  for (int c = 0; c < 3; ++c) {
+    const double lo = key_float(bb->tmin[c]), hi = key_float(bb->tmax[c]);
+    const double w = hi > lo ? hi - lo : 1.0;
+    double u = (q[c] - lo) / w * 1023.999;
+    if (!(u >= 0.0)) u = 0.0;  // also catches NaN
+    if (u > 1023.0) u = 1023.0;
+    code |= spread3((unsigned)u) << c;
+  }
+  keys[t] = ((unsigned long long)(unsigned)tgroup[t] << 32) | code;
+  vals[t] = (int)t;
+}
+
+__global__ void bs_gather_targets(const double4 *__restrict__ src, const int *__restrict__ perm,
+                                  long long n, double4 *dst) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) dst[t] = src[perm[t]];
 }
 
 // Largest possible squared target-endpoint distance from the bounds; the
@@ -158,20 +198,24 @@ __device__ __forceinline__ bool co_can_trigger(const BBox *bb, double co) {
 
 // ------------------------------------------------------- FP32 direct sum
 constexpr int kThreads = 128;
-constexpr int kStages = 4;
+constexpr int kStagesMax = 4;
 constexpr uint64_t kDefaultWaitNs = 2000000000ull;  // 2 s per tile: far above any real latency
 
 template <int KF>
 struct StageSmem {
   static constexpr int kBytes = KF * 52;  // fa, fb, fc: 16 B each; fd: 4 B
+  static constexpr int kStages = KF >= 128 ? 3 : kStagesMax;  // filament stages in flight
 };
 
-// Dynamic shared memory: kStages filament stages, then the per-target Kahan
-// state (sum, compensation) x 3 components as floats, then the barriers.
+// Dynamic shared memory: the filament stages, the per-target Kahan state
+// (sum, compensation) x 3 components as floats, the near-singular bit words
+// of the current tile (KF/4 words per thread), then the barriers: full[s]
+// (bytes landed) and empty[s] (every warp done reading stage s).
 template <int T, int KF>
 __host__ __device__ constexpr size_t f32c_smem_bytes_t() {
-  return (size_t)kStages * StageSmem<KF>::kBytes + (size_t)6 * kThreads * T * sizeof(float) +
-         kStages * sizeof(uint64_t);
+  constexpr int S = StageSmem<KF>::kStages;
+  return (size_t)S * StageSmem<KF>::kBytes + (size_t)6 * kThreads * T * sizeof(float) +
+         (size_t)(KF / 4) * kThreads * sizeof(unsigned) + 2 * S * sizeof(uint64_t);
 }
 
 // Kahan step: (sum, comp) += v.
@@ -192,14 +236,28 @@ __device__ __forceinline__ void issue_stage(const F32cArgs &a, unsigned char *st
   bulk_g2s(stage + KF * 48, a.fd + f0, KF * 4, bar);
 }
 
+// Thread 0 hands global tile g (filaments f0 .. f0+KF) to the copy engine
+// once every warp has released the stage's previous use (tile g - S, S stages).
+template <int KF>
+__device__ __forceinline__ bool produce(const F32cArgs &a, unsigned char *smem, uint64_t *full,
+                                        uint64_t *empty, unsigned g, int f0) {
+  constexpr unsigned S = StageSmem<KF>::kStages;
+  const int st = g % S;
+  if (g >= S && !mbar_wait_bounded(&empty[st], ((g - S) / S) & 1u, a.err, a.wait_limit_ns))
+    return false;
+  issue_stage<KF>(a, smem + st * StageSmem<KF>::kBytes, &full[st], f0);
+  return true;
+}
+
 // One item: the thread's T targets against filaments [it.f_begin, it.f_end).
 // Returns false when a bounded wait ran out (the item is abandoned).
 template <int T, int KF, int MODEL, bool CO>
 __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, const Tile &tl,
-                                          unsigned char *smem, uint64_t *full, float *s_k,
+                                          unsigned char *smem, uint64_t *full,
+                                          uint64_t *empty, float *s_k, unsigned *s_nb,
                                           unsigned &gt, float (&px)[T], float (&py)[T],
                                           float (&pz)[T], float cx, float cy, float cz,
-                                          unsigned &near_cnt) {
+                                          float S2, unsigned &near_cnt) {
   const int tid = threadIdx.x;
   const int ntiles = (it.f_end - it.f_begin) / KF;
   const float co2 = (float)(a.co * a.co);
@@ -208,40 +266,53 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, con
   rp.d = a.d;
   rp.n = a.n;
   rp.co = a.co;
+  const int lane = tid & 31;
+  bool ok = true;
+  int issued = 0;  // tiles of this item handed to the copy engine (thread 0)
   if (tid == 0) {
-    for (int s = 0; s < kStages && s < ntiles; ++s) {
-      const int st = (gt + s) % kStages;
-      issue_stage<KF>(a, smem + st * StageSmem<KF>::kBytes, &full[st], it.f_begin + s * KF);
-    }
+    for (; issued < StageSmem<KF>::kStages && issued < ntiles; ++issued)
+      if (!produce<KF>(a, smem, full, empty, gt + issued, it.f_begin + issued * KF)) {
+        ok = false;
+        break;
+      }
   }
   float ax[T], ay[T], az[T];
 #pragma unroll
   for (int t = 0; t < T; ++t) ax[t] = ay[t] = az[t] = 0.f;
 
-  bool ok = true;
   int i = 0;
-  for (; i < ntiles; ++i) {
+  for (; ok && i < ntiles; ++i) {
     const unsigned g = gt + i;
-    const int st = g % kStages;
-    const unsigned par = (g / kStages) & 1u;
-    bool timed_out = !mbar_wait_bounded(&full[st], par, a.err, a.wait_limit_ns);
+    const int st = g % StageSmem<KF>::kStages;
+    const unsigned par = (g / StageSmem<KF>::kStages) & 1u;
+    const bool timed_out = !mbar_wait_bounded(&full[st], par, a.err, a.wait_limit_ns);
     const unsigned char *stage = smem + st * StageSmem<KF>::kBytes;
     const float4 *sA = reinterpret_cast<const float4 *>(stage);
     const float4 *sB = reinterpret_cast<const float4 *>(stage + KF * 16);
     const float4 *sC = reinterpret_cast<const float4 *>(stage + KF * 32);
     const float *sD = reinterpret_cast<const float *>(stage + KF * 48);
-    if (!timed_out) {
-#pragma unroll 2
-      for (int k = 0; k < KF; ++k) {
+    if (timed_out) {
+      ok = false;
+      break;
+    }
+    // Hot loop: filaments in groups of 4; the near-singular bits of a group
+    // (bit 8*j + t: filament 4*kk+j, target t) go to shared memory as one word.
+#pragma unroll 1
+    for (int kk = 0; kk < KF; kk += 4) {
+      unsigned nbits = 0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int k = kk + j;
         const float4 A = sA[k];
         const float4 B = sB[k];
         const float4 C = sC[k];
         const float Dv = sD[k];
         // x1 relative to this thread's centre, from its hi/lo split
         const float xrx = (A.x - cx) + B.x, xry = (A.y - cy) + B.y, xrz = (A.z - cz) + B.z;
-        const float L2 = A.w, Rn2 = B.w;
+        // near-singular threshold, raised for threads whose targets spread far
+        // from their centre (the FP32 differences lose ~eps * spread / |r1|)
+        const float L2 = A.w, Rn2 = fmaxf(B.w, S2);
         const float Lx = C.x, Ly = C.y, Lz = C.z, K = C.w;
-        unsigned nb = 0;
 #pragma unroll
         for (int t = 0; t < T; ++t) {
           const float rx = px[t] - xrx, ry = py[t] - xry, rz = pz[t] - xrz;  // r1 = P - x1
@@ -270,69 +341,72 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, con
           const bool nr = dot < Rn2;
           bool skip = nr;
           if (CO) skip = skip || (fminf(r1s, r2s) > co2);
-          if (nr) nb |= (1u << t);
+          if (nr) nbits |= (1u << (8 * j + t));
           if (!skip) {
             ax[t] = fmaf(ub, cxv, ax[t]);
             ay[t] = fmaf(ub, cyv, ay[t]);
             az[t] = fmaf(ub, czv, az[t]);
           }
         }
-        if (__any_sync(0xffffffffu, nb != 0u)) {
-          // Near-singular pairs of this filament: the reference formula in FP64,
-          // added to the per-target Kahan state as an exact hi + lo pair.
-          const int fidx = it.f_begin + i * KF + k;
-          const double4 RA = a.ra[fidx];
-          const double4 RB = a.rb[fidx];
+      }
+      s_nb[(kk / 4) * kThreads + tid] = nbits;
+    }
+    // This warp is done with the stage: release it to the producer.
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[st]);
+    // Thread 0 refills the stage released one tile ago (S - 1 tiles ahead).
+    if (tid == 0 && i >= 1 && issued < ntiles) {
+      if (!produce<KF>(a, smem, full, empty, gt + issued, it.f_begin + issued * KF)) {
+        ok = false;
+      } else {
+        ++issued;
+      }
+    }
+    // Kahan-fold this tile's partial sums into the per-target totals.
+#pragma unroll
+    for (int t = 0; t < T; ++t) {
+      const int sl = tid * T + t;
+      kahan_add(s_k[0 * kThreads * T + sl], s_k[1 * kThreads * T + sl], ax[t]);
+      kahan_add(s_k[2 * kThreads * T + sl], s_k[3 * kThreads * T + sl], ay[t]);
+      kahan_add(s_k[4 * kThreads * T + sl], s_k[5 * kThreads * T + sl], az[t]);
+      ax[t] = ay[t] = az[t] = 0.f;
+    }
+    // Near-singular pairs of this tile, each lane its own: the reference formula
+    // in FP64, added to the Kahan state as an exact hi + lo pair.
 #pragma unroll 1
-          for (int t = 0; t < T; ++t) {
-            if (nb & (1u << t)) {
-              int local = tid * T + t;
-              if (local >= tl.t_count) local = tl.t_count - 1;
-              const double4 p = a.tp[tl.t_begin + local];
-              double u[3] = {0.0, 0.0, 0.0};
-              ref_pair<false>(RA, RB, p.x, p.y, p.z, rp, u[0], u[1], u[2]);
-              const int sl = tid * T + t;
-#pragma unroll
-              for (int c = 0; c < 3; ++c) {
-                const float hi = (float)u[c];
-                const float lo = (float)(u[c] - (double)hi);
-                float &sum = s_k[(2 * c) * kThreads * T + sl];
-                float &cmp = s_k[(2 * c + 1) * kThreads * T + sl];
-                kahan_add(sum, cmp, hi);
-                kahan_add(sum, cmp, lo);
-              }
-              ++near_cnt;
-            }
-          }
-        }
-      }
-      // Kahan-fold this tile's partial sums into the per-target totals.
-#pragma unroll
-      for (int t = 0; t < T; ++t) {
+    for (int w = 0; w < KF / 4; ++w) {
+      unsigned bits = s_nb[w * kThreads + tid];
+      while (bits) {
+        const int b = __ffs(bits) - 1;
+        bits &= bits - 1u;
+        const int t = b & 7;
+        const int fidx = it.f_begin + i * KF + 4 * w + (b >> 3);
+        int local = tid * T + t;
+        if (local >= tl.t_count) local = tl.t_count - 1;
+        const double4 p = a.tp[tl.t_begin + local];
+        double u[3] = {0.0, 0.0, 0.0};
+        ref_pair<false>(a.ra[fidx], a.rb[fidx], p.x, p.y, p.z, rp, u[0], u[1], u[2]);
         const int sl = tid * T + t;
-        kahan_add(s_k[0 * kThreads * T + sl], s_k[1 * kThreads * T + sl], ax[t]);
-        kahan_add(s_k[2 * kThreads * T + sl], s_k[3 * kThreads * T + sl], ay[t]);
-        kahan_add(s_k[4 * kThreads * T + sl], s_k[5 * kThreads * T + sl], az[t]);
-        ax[t] = ay[t] = az[t] = 0.f;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const float hi = (float)u[c];
+          const float lo = (float)(u[c] - (double)hi);
+          kahan_add(s_k[(2 * c) * kThreads * T + sl], s_k[(2 * c + 1) * kThreads * T + sl], hi);
+          kahan_add(s_k[(2 * c) * kThreads * T + sl], s_k[(2 * c + 1) * kThreads * T + sl], lo);
+        }
+        ++near_cnt;
       }
-    }
-    // Every thread is done with this stage before it is refilled.
-    if (__syncthreads_or(timed_out)) {
-      ok = false;
-      break;
-    }
-    if (tid == 0 && i + kStages < ntiles) {
-      issue_stage<KF>(a, smem + st * StageSmem<KF>::kBytes, &full[st],
-                      it.f_begin + (i + kStages) * KF);
     }
   }
-  if (!ok) {
-    // Let the copies already issued for this item land (bounded) before the
-    // CTA leaves, so no bulk copy targets shared memory of a finished CTA.
+  // A bounded wait that ran out anywhere abandons the item for the whole CTA.
+  if (__syncthreads_or(!ok)) {
+    // Let the copies already issued land (bounded) before the CTA leaves, so
+    // no bulk copy targets the shared memory of a finished CTA.
     if (tid == 0) {
-      for (int j = i; j < ntiles && j < i + kStages; ++j) {
+      constexpr int S = StageSmem<KF>::kStages;
+      for (int j = (issued > S ? issued - S : 0); j < issued; ++j) {
         const unsigned g = gt + j;
-        mbar_wait_bounded(&full[g % kStages], (g / kStages) & 1u, a.err, a.wait_limit_ns);
+        mbar_wait_bounded(&full[g % S], (g / S) & 1u, a.err, a.wait_limit_ns);
       }
     }
     return false;
@@ -344,12 +418,17 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, con
 template <int T, int KF, int MODEL>
 __global__ void __launch_bounds__(kThreads) bs_f32c(const F32cArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
-  float *s_k = reinterpret_cast<float *>(smem + kStages * StageSmem<KF>::kBytes);
-  uint64_t *full = reinterpret_cast<uint64_t *>(s_k + 6 * kThreads * T);
+  float *s_k = reinterpret_cast<float *>(smem + StageSmem<KF>::kStages * StageSmem<KF>::kBytes);
+  unsigned *s_nb = reinterpret_cast<unsigned *>(s_k + 6 * kThreads * T);
+  uint64_t *full = reinterpret_cast<uint64_t *>(s_nb + (KF / 4) * kThreads);
+  uint64_t *empty = full + StageSmem<KF>::kStages;
   __shared__ int s_item;
   const int tid = threadIdx.x;
   if (tid == 0) {
-    for (int s = 0; s < kStages; ++s) mbar_init(&full[s], 1);
+    for (int s = 0; s < StageSmem<KF>::kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kThreads / 32);
+    }
     fence_mbar_init();
   }
   __syncthreads();
@@ -370,6 +449,7 @@ __global__ void __launch_bounds__(kThreads) bs_f32c(const F32cArgs a) {
     }
     // This thread's T consecutive targets, relative to the FP32 image of the first.
     float px[T], py[T], pz[T];
+    float spread2 = 0.f;
     int l0 = tid * T;
     if (l0 >= tl.t_count) l0 = tl.t_count - 1;
     const double4 p0 = a.tp[tl.t_begin + l0];
@@ -382,16 +462,18 @@ __global__ void __launch_bounds__(kThreads) bs_f32c(const F32cArgs a) {
       px[t] = (float)(p.x - (double)cx);
       py[t] = (float)(p.y - (double)cy);
       pz[t] = (float)(p.z - (double)cz);
+      spread2 = fmaxf(spread2, px[t] * px[t] + py[t] * py[t] + pz[t] * pz[t]);
 #pragma unroll
       for (int c = 0; c < 6; ++c) s_k[c * kThreads * T + tid * T + t] = 0.f;
     }
+    const float S2 = 0.09f * spread2;  // pairs closer than 0.3 x spread go to FP64
     bool ok;
     if (co_on)
-      ok = f32c_item<T, KF, MODEL, true>(a, it, tl, smem, full, s_k, gt, px, py, pz, cx, cy, cz,
-                                         near_cnt);
+      ok = f32c_item<T, KF, MODEL, true>(a, it, tl, smem, full, empty, s_k, s_nb, gt, px, py, pz,
+                                         cx, cy, cz, S2, near_cnt);
     else
-      ok = f32c_item<T, KF, MODEL, false>(a, it, tl, smem, full, s_k, gt, px, py, pz, cx, cy, cz,
-                                          near_cnt);
+      ok = f32c_item<T, KF, MODEL, false>(a, it, tl, smem, full, empty, s_k, s_nb, gt, px, py,
+                                          pz, cx, cy, cz, S2, near_cnt);
     if (!ok) return;
     double *part = a.part + (size_t)item_id * 3 * a.tile_cap;
 #pragma unroll
@@ -463,7 +545,8 @@ __global__ void __launch_bounds__(kF64Threads) bs_f64(const F32cArgs a) {
 
 // --------------------------------------------------------------- reduce
 __global__ void bs_reduce(const Tile *__restrict__ tiles, const Group *__restrict__ groups,
-                          const double *__restrict__ part, int tile_cap) {
+                          const double *__restrict__ part, const int *__restrict__ perm,
+                          int tile_cap) {
   const Tile tl = tiles[blockIdx.x];
   const Group g = groups[tl.group];
   for (int l = threadIdx.x; l < tl.t_count; l += blockDim.x) {
@@ -474,7 +557,7 @@ __global__ void bs_reduce(const Tile *__restrict__ tiles, const Group *__restric
       s1 += p[tile_cap + l];
       s2 += p[2 * tile_cap + l];
     }
-    const long long local = tl.t_begin - g.t_begin + l;
+    const long long local = (long long)perm[tl.t_begin + l] - g.t_begin;
     const long long j = local / g.ns_p, i = local - j * g.ns_p;
     double *o = g.out + i + 3 * g.ns_p * j;
     if (g.accumulate) {
@@ -567,26 +650,25 @@ int occupancy_t() {
   return n > 0 ? n : 1;
 }
 
-#define WINDS_F32C_DISPATCH(FN, ...)                                    \
-  switch (model * 100 + T * 10 + (KF == 32 ? 0 : KF == 64 ? 1 : 2)) {   \
-    case 0 * 100 + 20 + 0: return FN<2, 32, 0>(__VA_ARGS__);             \
-    case 0 * 100 + 20 + 1: return FN<2, 64, 0>(__VA_ARGS__);             \
-    case 0 * 100 + 40 + 0: return FN<4, 32, 0>(__VA_ARGS__);             \
-    case 0 * 100 + 40 + 1: return FN<4, 64, 0>(__VA_ARGS__);             \
-    case 0 * 100 + 80 + 0: return FN<8, 32, 0>(__VA_ARGS__);             \
-    case 0 * 100 + 80 + 1: return FN<8, 64, 0>(__VA_ARGS__);             \
-    case 1 * 100 + 20 + 0: return FN<2, 32, 1>(__VA_ARGS__);             \
-    case 1 * 100 + 20 + 1: return FN<2, 64, 1>(__VA_ARGS__);             \
-    case 1 * 100 + 40 + 0: return FN<4, 32, 1>(__VA_ARGS__);             \
-    case 1 * 100 + 40 + 1: return FN<4, 64, 1>(__VA_ARGS__);             \
-    case 1 * 100 + 80 + 0: return FN<8, 32, 1>(__VA_ARGS__);             \
-    case 1 * 100 + 80 + 1: return FN<8, 64, 1>(__VA_ARGS__);             \
-    default: break;                                                      \
+#define WINDS_F32C_CASE(FN, M, TT, KK, ...) \
+  case M * 1000 + TT * 100 + KK / 32: return FN<TT, KK, M>(__VA_ARGS__);
+#define WINDS_F32C_DISPATCH(FN, ...)                                                    \
+  switch (model * 1000 + T * 100 + KF / 32) {                                          \
+    WINDS_F32C_CASE(FN, 0, 2, 32, __VA_ARGS__) WINDS_F32C_CASE(FN, 0, 2, 64, __VA_ARGS__) \
+    WINDS_F32C_CASE(FN, 0, 2, 128, __VA_ARGS__) WINDS_F32C_CASE(FN, 0, 4, 32, __VA_ARGS__) \
+    WINDS_F32C_CASE(FN, 0, 4, 64, __VA_ARGS__) WINDS_F32C_CASE(FN, 0, 4, 128, __VA_ARGS__) \
+    WINDS_F32C_CASE(FN, 0, 8, 32, __VA_ARGS__) WINDS_F32C_CASE(FN, 0, 8, 64, __VA_ARGS__) \
+    WINDS_F32C_CASE(FN, 0, 8, 128, __VA_ARGS__) WINDS_F32C_CASE(FN, 1, 2, 32, __VA_ARGS__) \
+    WINDS_F32C_CASE(FN, 1, 2, 64, __VA_ARGS__) WINDS_F32C_CASE(FN, 1, 2, 128, __VA_ARGS__) \
+    WINDS_F32C_CASE(FN, 1, 4, 32, __VA_ARGS__) WINDS_F32C_CASE(FN, 1, 4, 64, __VA_ARGS__) \
+    WINDS_F32C_CASE(FN, 1, 4, 128, __VA_ARGS__) WINDS_F32C_CASE(FN, 1, 8, 32, __VA_ARGS__) \
+    WINDS_F32C_CASE(FN, 1, 8, 64, __VA_ARGS__) WINDS_F32C_CASE(FN, 1, 8, 128, __VA_ARGS__) \
+    default: break;                                                                     \
   }
 }  // namespace
 
 bool f32c_config_supported(int T, int KF) {
-  return (T == 2 || T == 4 || T == 8) && (KF == 32 || KF == 64);
+  return (T == 2 || T == 4 || T == 8) && (KF == 32 || KF == 64 || KF == 128);
 }
 
 int f32c_threads() { return kThreads; }
@@ -642,18 +724,40 @@ cudaError_t launch_pad_filaments(long long from, long long to, const PackedFilam
 }
 
 cudaError_t launch_pack_targets(const double *P, long long ns, long long np, long long off,
-                                double4 *tp, BBox *bb, cudaStream_t s) {
+                                int group, double4 *tp, int *tgroup, BBox *bb, cudaStream_t s) {
   if (np <= 0) return cudaSuccess;
   const int bs = 256;
   const long long grid = (np + bs - 1) / bs;
-  bs_pack_targets<<<(unsigned)grid, bs, 0, s>>>(P, ns, np, off, tp, bb);
+  bs_pack_targets<<<(unsigned)grid, bs, 0, s>>>(P, ns, np, off, group, tp, tgroup, bb);
   return cudaGetLastError();
 }
 
+cudaError_t launch_target_keys(const double4 *tp, const int *tgroup, long long n, const BBox *bb,
+                               unsigned long long *keys, int *vals, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  bs_target_keys<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(tp, tgroup, n, bb, keys, vals);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather_targets(const double4 *src, const int *perm, long long n, double4 *dst,
+                                  cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  bs_gather_targets<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(src, perm, n, dst);
+  return cudaGetLastError();
+}
+
+// Sorts (key, value) pairs with CUB's radix sort; temp == nullptr queries the
+// scratch size into *temp_bytes.
+cudaError_t sort_target_keys(void *temp, size_t *temp_bytes, const unsigned long long *kin,
+                             unsigned long long *kout, const int *vin, int *vout, long long n,
+                             cudaStream_t s) {
+  return cub::DeviceRadixSort::SortPairs(temp, *temp_bytes, kin, kout, vin, vout, (int)n, 0, 64, s);
+}
+
 cudaError_t launch_reduce(const Tile *tiles, int n_tiles, const Group *groups, const double *part,
-                          int tile_cap, cudaStream_t s) {
+                          const int *perm, int tile_cap, cudaStream_t s) {
   if (n_tiles <= 0) return cudaSuccess;
-  bs_reduce<<<n_tiles, 256, 0, s>>>(tiles, groups, part, tile_cap);
+  bs_reduce<<<n_tiles, 256, 0, s>>>(tiles, groups, part, perm, tile_cap);
   return cudaGetLastError();
 }
 

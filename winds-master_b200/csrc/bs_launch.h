@@ -33,11 +33,18 @@ cudaError_t launch_pack_filaments(const double *F1, const double *F2, const doub
 cudaError_t launch_pad_filaments(long long from, long long to, const PackedFilaments &pf,
                                  cudaStream_t s);
 cudaError_t launch_pack_targets(const double *P, long long ns, long long np, long long off,
-                                double4 *tp, BBox *bb, cudaStream_t s);
+                                int group, double4 *tp, int *tgroup, BBox *bb, cudaStream_t s);
+cudaError_t launch_target_keys(const double4 *tp, const int *tgroup, long long n, const BBox *bb,
+                               unsigned long long *keys, int *vals, cudaStream_t s);
+cudaError_t launch_gather_targets(const double4 *src, const int *perm, long long n, double4 *dst,
+                                  cudaStream_t s);
+cudaError_t sort_target_keys(void *temp, size_t *temp_bytes, const unsigned long long *kin,
+                             unsigned long long *kout, const int *vin, int *vout, long long n,
+                             cudaStream_t s);
 cudaError_t launch_f32c(const F32cArgs &a, int model, int T, int KF, int grid, cudaStream_t s);
 cudaError_t launch_f64(const F32cArgs &a, int grid, cudaStream_t s);
 cudaError_t launch_reduce(const Tile *tiles, int n_tiles, const Group *groups, const double *part,
-                          int tile_cap, cudaStream_t s);
+                          const int *perm, int tile_cap, cudaStream_t s);
 cudaError_t launch_ffma_peak(float *out, int blocks, int iters, cudaStream_t s);
 cudaError_t launch_wait_selftest(unsigned *err, unsigned long long limit_ns, cudaStream_t s);
 cudaError_t launch_length(const double *F1, const double *F2, long long d0, long long nf, double *L,

@@ -8,7 +8,9 @@
 //     fd[f] = (rc^2 |L|^2)^2 (Vatistas) or d |L|^2 (cut-off)   float
 //   raw FP64 filaments for near-singular terms and the FP64 path
 //     ra[f] = (x1, y1, z1, gamma)  rb[f] = (x2, y2, z2, rc^2)   double4
-//   targets  tp[t] = (x, y, z, 0) double4
+//   targets  tp[t] = (x, y, z, 0) double4, sorted by (group, Morton code of the
+//            position) so the T targets of a thread are close together;
+//            perm[t] = index of sorted target t in the packed input order
 //   partial sums per work item: part[item][3][tile_cap] double
 #pragma once
 

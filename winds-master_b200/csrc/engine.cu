@@ -50,7 +50,9 @@ const char *last_error() { return g_last_error.c_str(); }
 int DevBuf::ensure(size_t bytes, cudaStream_t s) {
   if (bytes <= cap) return WINDS_BS_OK;
   if (p) {
-    cudaError_t e = cudaStreamSynchronize(s);
+    // the old buffer may still be read on any stream of this device
+    (void)s;
+    cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return cuda_fail(e, "sync before buffer growth");
     cudaFree(p);
     p = nullptr;
@@ -160,7 +162,8 @@ void shutdown_all() {
     Context *c = kv.second;
     cudaSetDevice(c->dev);
     cudaStreamSynchronize(c->stream);
-    for (DevBuf *b : {&c->fa, &c->fb, &c->fc, &c->fd, &c->ra, &c->rb, &c->tp, &c->groups,
+    for (DevBuf *b : {&c->fa, &c->fb, &c->fc, &c->fd, &c->ra, &c->rb, &c->tp, &c->tp_raw,
+                      &c->tgroup, &c->keys, &c->vals, &c->perm, &c->sort_tmp, &c->groups,
                       &c->tiles, &c->items, &c->part, &c->bbox, &c->ctr, &c->err, &c->nearctr,
                       &c->in_P, &c->in_F, &c->out_u})
       b->release();
@@ -281,8 +284,18 @@ int pack_inputs(Context *c, const winds_bs_family *fams, int nfam,
       (rc = c->fc.ensure(nfp * sizeof(float4), s)) || (rc = c->fd.ensure(nfp * sizeof(float), s)) ||
       (rc = c->ra.ensure(nfp * sizeof(double4), s)) ||
       (rc = c->rb.ensure(nfp * sizeof(double4), s)) ||
-      (rc = c->tp.ensure(std::max<long long>(nt, 1) * sizeof(double4), s)))
+      (rc = c->tp.ensure(std::max<long long>(nt, 1) * sizeof(double4), s)) ||
+      (rc = c->tp_raw.ensure(std::max<long long>(nt, 1) * sizeof(double4), s)) ||
+      (rc = c->tgroup.ensure(std::max<long long>(nt, 1) * sizeof(int), s)) ||
+      (rc = c->keys.ensure(std::max<long long>(nt, 1) * 2 * sizeof(unsigned long long), s)) ||
+      (rc = c->vals.ensure(std::max<long long>(nt, 1) * sizeof(int), s)) ||
+      (rc = c->perm.ensure(std::max<long long>(nt, 1) * sizeof(int), s)))
     return rc;
+  size_t sort_bytes = 0;
+  if (sort_target_keys(nullptr, &sort_bytes, nullptr, nullptr, nullptr, nullptr, nt, s) !=
+      cudaSuccess)
+    return fail(WINDS_BS_ERR_CUDA, "target sort size query failed");
+  if ((rc = c->sort_tmp.ensure(sort_bytes + 256, s))) return rc;
   PackedFilaments pf{(float4 *)c->fa.p, (float4 *)c->fb.p, (float4 *)c->fc.p,
                      (float *)c->fd.p, (double4 *)c->ra.p, (double4 *)c->rb.p};
   cudaError_t e = launch_bbox_init((BBox *)c->bbox.p, s);
@@ -301,12 +314,26 @@ int pack_inputs(Context *c, const winds_bs_family *fams, int nfam,
     c->launches += nfp > nf;
   }
   long long toff = 0;
+  int gid = 0;
   for (const TargetSpec &t : tsets) {
     if (e != cudaSuccess) break;
-    e = launch_pack_targets(t.P, t.ns, t.count, toff, (double4 *)c->tp.p, (BBox *)c->bbox.p, s);
+    e = launch_pack_targets(t.P, t.ns, t.count, toff, gid++, (double4 *)c->tp_raw.p,
+                            (int *)c->tgroup.p, (BBox *)c->bbox.p, s);
     c->launches += t.count > 0;
     toff += t.count;
   }
+  // Sort targets by (set, Morton code) so each thread's targets lie close together.
+  unsigned long long *k0 = (unsigned long long *)c->keys.p, *k1 = k0 + std::max<long long>(nt, 1);
+  if (e == cudaSuccess)
+    e = launch_target_keys((const double4 *)c->tp_raw.p, (const int *)c->tgroup.p, nt,
+                           (const BBox *)c->bbox.p, k0, (int *)c->vals.p, s);
+  if (e == cudaSuccess && nt > 0)
+    e = sort_target_keys(c->sort_tmp.p, &sort_bytes, k0, k1, (const int *)c->vals.p,
+                         (int *)c->perm.p, nt, s);
+  if (e == cudaSuccess)
+    e = launch_gather_targets((const double4 *)c->tp_raw.p, (const int *)c->perm.p, nt,
+                              (double4 *)c->tp.p, s);
+  c->launches += nt > 0 ? 5 : 0;  // keys, 3 radix-sort passes (library), gather (approx.)
   if (e != cudaSuccess) return cuda_fail(e, "pack kernels");
   *nf_real = nf;
   *nf_pad = nfp;
@@ -414,7 +441,7 @@ int run_direct_sum(Context *c, const std::vector<GroupSpec> &gs, int model, doub
   c->timed = time_main;
   if (e != cudaSuccess) return cuda_fail(e, "direct-sum launch");
   e = launch_reduce((const Tile *)c->tiles.p, (int)pl.tiles.size(), (const Group *)c->groups.p,
-                    (const double *)c->part.p, tile_cap, s);
+                    (const double *)c->part.p, (const int *)c->perm.p, tile_cap, s);
   c->launches += 1;
   if (e != cudaSuccess) return cuda_fail(e, "reduce launch");
   return WINDS_BS_OK;
@@ -506,8 +533,8 @@ int eval_device(Context *c, const winds_bs_family *fams, int nfam,
 int autotune(Context *c, const std::vector<GroupSpec> &gs, int model, double dcut, double n,
              double co, long long nt, long long nf, TuneChoice *best) {
   const int Ts[3] = {2, 4, 8};
-  const int KFs[2] = {32, 64};
-  const double Ws[2] = {4.0, 8.0};
+  const int KFs[3] = {32, 64, 128};
+  const double Ws[3] = {8.0, 16.0, 32.0};
   float best_ms = 1e30f;
   TuneChoice bc = default_choice(nt);
   cudaEvent_t e0, e1;

@@ -58,8 +58,8 @@ struct Context {
   int cc_major = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev_main0 = nullptr, ev_main1 = nullptr, ev_upload = nullptr;
-  // packed inputs
-  DevBuf fa, fb, fc, fd, ra, rb, tp;
+  // packed inputs; targets sorted (tp) from their packed order (tp_raw)
+  DevBuf fa, fb, fc, fd, ra, rb, tp, tp_raw, tgroup, keys, vals, perm, sort_tmp;
   // plan tables and partial sums
   DevBuf groups, tiles, items, part;
   // small words
