@@ -97,6 +97,28 @@ int winds_bs_eval_host(const winds_bs_family *fams, int nfam, const double *P,
                        const long long pdims[4], const winds_bs_params *prm,
                        double *uind);
 
+/* The same evaluation as winds_bs_eval_device for callers that must not
+ * allocate device memory. No counterpart in the reference: it exists because
+ * winds_bs_eval_device grows its buffers with cudaMalloc, which a host that
+ * owns all device memory through its own pool cannot allow and which, by
+ * synchronising the device, stalls a solver that calls the engine every step.
+ * All scratch lives in one static __device__ array of
+ * WINDS_BS_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds
+ * until exit. Inputs, outputs and semantics are those of
+ * winds_bs_eval_device (device pointers; stream NULL = the default stream).
+ * Limits: at most WINDS_BS_NOALLOC_MAX_FILAMENTS filaments and
+ * WINDS_BS_NOALLOC_MAX_TARGETS targets per call (WINDS_BS_ERR_ARG beyond).
+ * The call waits for its stream and reports device-side errors. Its first
+ * call on a device looks up the array's device address: make that call
+ * before any stream capture. Calls share the array: calls that overlap on the
+ * GPU race. */
+#define WINDS_BS_NOALLOC_SCRATCH_BYTES (64ull << 20)
+#define WINDS_BS_NOALLOC_MAX_FILAMENTS 131072
+#define WINDS_BS_NOALLOC_MAX_TARGETS 65536
+int winds_bs_eval_device_noalloc(const winds_bs_family *fams, int nfam, const double *P,
+                                 const long long pdims[4], const winds_bs_params *prm,
+                                 double *uind, void *stream);
+
 /* Filament lengths sqrt(|F2-F1|^2), MATLAB layout [dims0,1,dims2,dims3].
  * Replaces core/FilamentLength.m:27-44. Device pointers. */
 int winds_bs_length_device(const double *F1, const double *F2, const long long dims[4],

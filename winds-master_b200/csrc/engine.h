@@ -74,6 +74,10 @@ struct Context {
 };
 
 int fail(int code, const char *fmt, ...);
+int resolve_model(const winds_bs_params *prm, int *model, double *dcut, double *n, int *prec);
+int validate_family(const winds_bs_family &f);
+TuneChoice default_choice(long long nt);
+bool lookup_tune(int model, long long nt, long long nf, TuneChoice *out);
 int cuda_fail(cudaError_t e, const char *what);
 Context *get_context(int *rc);
 int eval_device(Context *c, const winds_bs_family *fams, int nfam,
