@@ -64,14 +64,32 @@ __device__ __forceinline__ uint64_t global_timer_ns() {
   return t;
 }
 
+// try_wait that lets the hardware suspend the thread for up to `hint_ns`
+// while the phase is incomplete (no busy spinning).
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t *bar, uint32_t parity,
+                                                    uint32_t hint_ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return ok != 0;
+}
+
 // Waits for the barrier phase with the given parity for at most `limit_ns`
-// nanoseconds. On timeout it sets kErrWaitTimeout in *err and returns false.
+// nanoseconds (the timer is read once per 32 suspended tries). On timeout it
+// sets kErrWaitTimeout in *err and returns false.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, unsigned *err,
                                                   uint64_t limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = global_timer_ns();
   while (true) {
-    if (mbar_try_wait(bar, parity)) return true;
+#pragma unroll 1
+    for (int k = 0; k < 32; ++k)
+      if (mbar_try_wait_sleep(bar, parity, 20000u)) return true;
     if (global_timer_ns() - t0 > limit_ns) {
       atomicOr(err, kErrWaitTimeout);
       return false;

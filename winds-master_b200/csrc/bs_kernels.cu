@@ -249,6 +249,62 @@ __device__ __forceinline__ bool produce(const F32cArgs &a, unsigned char *smem, 
   return true;
 }
 
+// Non-blocking variant: issues tile g only if its stage is already free.
+template <int KF>
+__device__ __forceinline__ bool try_produce(const F32cArgs &a, unsigned char *smem, uint64_t *full,
+                                            uint64_t *empty, unsigned g, int f0) {
+  constexpr unsigned S = StageSmem<KF>::kStages;
+  const int st = g % S;
+  if (g >= S && !mbar_try_wait(&empty[st], ((g - S) / S) & 1u)) return false;
+  issue_stage<KF>(a, smem + st * StageSmem<KF>::kBytes, &full[st], f0);
+  return true;
+}
+
+// One target-filament interaction in FP32, accumulated into (ax, ay, az).
+// With NEAR it also tests r1.r2 < Rn^2: such pairs are skipped and recorded
+// in `bits` (they are redone in FP64 after the tile).
+template <int MODEL, bool CO, bool NEAR>
+__device__ __forceinline__ void interact(float px, float py, float pz, float xrx, float xry,
+                                         float xrz, float Lx, float Ly, float Lz, float L2,
+                                         float K, float Dv, float Rn2, float co2, float &ax,
+                                         float &ay, float &az, unsigned &bits, unsigned bit) {
+  const float rx = px - xrx, ry = py - xry, rz = pz - xrz;  // r1 = P - x1
+  // r1 x r2 = L x r1 (no cancellation for far or collinear points)
+  const float cxv = Ly * rz - Lz * ry;
+  const float cyv = Lz * rx - Lx * rz;
+  const float czv = Lx * ry - Ly * rx;
+  const float r1s = rx * rx + ry * ry + rz * rz;
+  const float Ld = Lx * rx + Ly * ry + Lz * rz;
+  const float dot = r1s - Ld;          // r1 . r2
+  const float r2s = dot + (L2 - Ld);   // |r1 - L|^2
+  const float i1 = rsqrt_approx(r1s), i2 = rsqrt_approx(r2s);
+  const float gg = i1 * i2;
+  const float e = fmaf(dot, gg, 1.f);  // 1 + cos(theta) >= 1 for far pairs
+  float ub;
+  if (MODEL == kCoreVatistas) {
+    // Cnu / (r1 r2 (r1 r2 + r1.r2)) with h^2 = |c|^2/|L|^2 and rc^4 folded:
+    // Cnu = |c|^2 / sqrt(|c|^4 + (rc^2 |L|^2)^2)
+    const float c2 = cxv * cxv + cyv * cyv + czv * czv;
+    const float q = fmaf(c2, c2, Dv);
+    ub = K * ((i1 + i2) * gg) * c2 * rsqrt_approx((e * e) * q);
+  } else {
+    // (r1+r2)/(r1r2(r1r2+r1.r2) + d|L|^2) = (i1+i2) gg / (e + d|L|^2 gg^2)
+    ub = K * ((i1 + i2) * gg) * rcp_approx(fmaf(Dv, gg * gg, e));
+  }
+  bool skip = false;
+  if (NEAR) {
+    const bool nr = dot < Rn2;
+    skip = nr;
+    if (nr) bits |= bit;
+  }
+  if (CO) skip = skip || (fminf(r1s, r2s) > co2);
+  if (!skip) {
+    ax = fmaf(ub, cxv, ax);
+    ay = fmaf(ub, cyv, ay);
+    az = fmaf(ub, czv, az);
+  }
+}
+
 // One item: the thread's T targets against filaments [it.f_begin, it.f_end).
 // Returns false when a bounded wait ran out (the item is abandoned).
 template <int T, int KF, int MODEL, bool CO>
@@ -285,7 +341,14 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, con
     const unsigned g = gt + i;
     const int st = g % StageSmem<KF>::kStages;
     const unsigned par = (g / StageSmem<KF>::kStages) & 1u;
-    const bool timed_out = !mbar_wait_bounded(&full[st], par, a.err, a.wait_limit_ns);
+    // Tile i must have been handed out before anyone waits for it.
+    if (tid == 0 && issued <= i) {
+      if (produce<KF>(a, smem, full, empty, gt + issued, it.f_begin + issued * KF))
+        ++issued;
+      else
+        ok = false;
+    }
+    const bool timed_out = !ok || !mbar_wait_bounded(&full[st], par, a.err, a.wait_limit_ns);
     const unsigned char *stage = smem + st * StageSmem<KF>::kBytes;
     const float4 *sA = reinterpret_cast<const float4 *>(stage);
     const float4 *sB = reinterpret_cast<const float4 *>(stage + KF * 16);
@@ -314,53 +377,20 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, con
         const float L2 = A.w, Rn2 = fmaxf(B.w, S2);
         const float Lx = C.x, Ly = C.y, Lz = C.z, K = C.w;
 #pragma unroll
-        for (int t = 0; t < T; ++t) {
-          const float rx = px[t] - xrx, ry = py[t] - xry, rz = pz[t] - xrz;  // r1 = P - x1
-          // r1 x r2 = L x r1 (no cancellation for far or collinear points)
-          const float cxv = Ly * rz - Lz * ry;
-          const float cyv = Lz * rx - Lx * rz;
-          const float czv = Lx * ry - Ly * rx;
-          const float r1s = rx * rx + ry * ry + rz * rz;
-          const float Ld = Lx * rx + Ly * ry + Lz * rz;
-          const float dot = r1s - Ld;          // r1 . r2
-          const float r2s = dot + (L2 - Ld);   // |r1 - L|^2
-          const float i1 = rsqrt_approx(r1s), i2 = rsqrt_approx(r2s);
-          const float gg = i1 * i2;
-          const float e = fmaf(dot, gg, 1.f);  // 1 + cos(theta) >= 1 for far pairs
-          float ub;
-          if (MODEL == kCoreVatistas) {
-            // Cnu / (r1 r2 (r1 r2 + r1.r2)) with h^2 = |c|^2/|L|^2 and rc^4 folded:
-            // Cnu = |c|^2 / sqrt(|c|^4 + (rc^2 |L|^2)^2)
-            const float c2 = cxv * cxv + cyv * cyv + czv * czv;
-            const float q = fmaf(c2, c2, Dv);
-            ub = K * ((i1 + i2) * gg) * c2 * rsqrt_approx((e * e) * q);
-          } else {
-            // (r1+r2)/(r1r2(r1r2+r1.r2) + d|L|^2) = (i1+i2) gg / (e + d|L|^2 gg^2)
-            ub = K * ((i1 + i2) * gg) * rcp_approx(fmaf(Dv, gg * gg, e));
-          }
-          const bool nr = dot < Rn2;
-          bool skip = nr;
-          if (CO) skip = skip || (fminf(r1s, r2s) > co2);
-          if (nr) nbits |= (1u << (8 * j + t));
-          if (!skip) {
-            ax[t] = fmaf(ub, cxv, ax[t]);
-            ay[t] = fmaf(ub, cyv, ay[t]);
-            az[t] = fmaf(ub, czv, az[t]);
-          }
-        }
+        for (int t = 0; t < T; ++t)
+          interact<MODEL, CO, true>(px[t], py[t], pz[t], xrx, xry, xrz, Lx, Ly, Lz, L2, K, Dv,
+                                    Rn2, co2, ax[t], ay[t], az[t], nbits, 1u << (8 * j + t));
       }
       s_nb[(kk / 4) * kThreads + tid] = nbits;
     }
     // This warp is done with the stage: release it to the producer.
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[st]);
-    // Thread 0 refills the stage released one tile ago (S - 1 tiles ahead).
-    if (tid == 0 && i >= 1 && issued < ntiles) {
-      if (!produce<KF>(a, smem, full, empty, gt + issued, it.f_begin + issued * KF)) {
-        ok = false;
-      } else {
+    // Thread 0 refills every stage whose readers are all done, without waiting.
+    if (tid == 0) {
+      while (issued < ntiles && issued <= i + (int)StageSmem<KF>::kStages &&
+             try_produce<KF>(a, smem, full, empty, gt + issued, it.f_begin + issued * KF))
         ++issued;
-      }
     }
     // Kahan-fold this tile's partial sums into the per-target totals.
 #pragma unroll
@@ -415,8 +445,15 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, con
   return true;
 }
 
+// Resident CTAs per SM the register allocation is capped for: 6 for T <= 4
+// (80 registers), 4 for T = 8 (128 registers).
+template <int T>
+struct MinBlocks {
+  static constexpr int value = T <= 4 ? 6 : 4;
+};
+
 template <int T, int KF, int MODEL>
-__global__ void __launch_bounds__(kThreads) bs_f32c(const F32cArgs a) {
+__global__ void __launch_bounds__(kThreads, MinBlocks<T>::value) bs_f32c(const F32cArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   float *s_k = reinterpret_cast<float *>(smem + StageSmem<KF>::kStages * StageSmem<KF>::kBytes);
   unsigned *s_nb = reinterpret_cast<unsigned *>(s_k + 6 * kThreads * T);
@@ -632,6 +669,10 @@ cudaError_t launch_f32c_t(const F32cArgs &a, int grid, cudaStream_t s) {
     cudaError_t e = cudaFuncSetAttribute(bs_f32c<T, KF, MODEL>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(bs_f32c<T, KF, MODEL>,
+                             cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return e;
     if (dev < 32) attr_set |= (1u << dev);
   }
   bs_f32c<T, KF, MODEL><<<grid, kThreads, smem, s>>>(a);
@@ -643,6 +684,8 @@ int occupancy_t() {
   const size_t smem = f32c_smem_bytes_t<T, KF>();
   cudaFuncSetAttribute(bs_f32c<T, KF, MODEL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)smem);
+  cudaFuncSetAttribute(bs_f32c<T, KF, MODEL>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                       (int)cudaSharedmemCarveoutMaxShared);
   int n = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bs_f32c<T, KF, MODEL>, kThreads, smem) !=
       cudaSuccess)
