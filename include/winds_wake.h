@@ -1,0 +1,106 @@
+/*
+ * winds_wake.h -- C ABI of the device-resident free-wake time step of
+ * libwinds_bs: many rotor cases, each with its own span resolution and wake
+ * length, stepped together; every step evaluates all cases' induced
+ * velocities in one persistent direct-sum launch per evaluation and can be
+ * replayed as one CUDA graph.
+ *
+ * What it replaces in the reference (ndevelder/WInDS-Master), per step:
+ *   Γ bookkeeping          WInDS.m:131-140, numerical/pcc.m:43-49
+ *   core growth + stretch  core/vcore.m:30-51, core/FilamentLength.m:27-44,
+ *                          core/filamentmod.m:23-41
+ *   induced velocity       WInDS.m:148-168 (two BiotSavart(Mex) calls),
+ *                          numerical/pcc.m:55-71 (two more for the corrector)
+ *   convection             numerical/fe.m:31, ab2.m:38-39, ab4.m:77-81, pcc.m:37-75
+ *
+ * Differences from the reference loop, all deliberate:
+ *   * each case's wake keeps `na` age columns: the oldest column is dropped
+ *     every step (the reference grows the wake by one column per step);
+ *   * the integrators start in their full form when history exists (the
+ *     reference switches on fixed step indices: ab2.m:35, ab4.m:74, pcc.m:40);
+ *   * filament stretching compares new and previous lengths by column index
+ *     as filamentmod.m does, whenever a previous step exists.
+ * Arrays use WInDS's MATLAB layout [span, xyz, age, blade], column-major.
+ */
+#ifndef WINDS_WAKE_H
+#define WINDS_WAKE_H
+
+#include "winds_bs.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WINDS_INTEG_FE 0
+#define WINDS_INTEG_AB2 1
+#define WINDS_INTEG_AB4 2
+#define WINDS_INTEG_PCC 3
+
+typedef struct winds_wake_batch winds_wake_batch;
+
+/* One rotor case. Host arrays are copied at creation. */
+typedef struct {
+  int nst;            /* span nodes (trailing filaments per age column); ns = nst-1 stations */
+  int nb;             /* blades */
+  int na;             /* age columns kept in the wake */
+  int nsteps;         /* time steps of kinematics and wind provided */
+  double dt;          /* time step (1/user.t(3)) */
+  double t0;          /* time of step 0 */
+  const double *quarter;  /* [nst,3,nsteps,nb] quarter-chord nodes per step (pos.quarter) */
+  const double *trailing; /* [nst,3,nsteps,nb] trailing-edge nodes per step (pos.trail)   */
+  const double *wind;     /* [3,nsteps] freestream vector per step (wind.infty')         */
+  double shear;           /* power-law exponent: wind * ((H+z)/H)^shear (0: uniform)     */
+  double hub_height;      /* H                                                          */
+  int core_mode;      /* 0: vcore.m, rc^2 = r0^2 + 4 alpha nu (1+a1 Re) t (absolute time)
+                         1: age form rc^2 = rc0^2 + 4 alpha delta nu (1+a1 Re) age       */
+  double r0, rc0, alpha, nu, a1, delta;
+  const double *dom;         /* [nst,3,na,nb] initial node positions (wake.domain)      */
+  const double *bound;       /* [nst-1,nb] bound circulation (shed column 1)            */
+  const double *trail_gamma; /* [nst,na-1,nb] trailing circulation (wake.gamma.trail)   */
+} winds_wake_case;
+
+typedef struct {
+  int integrator;      /* WINDS_INTEG_* */
+  int core_model;      /* WINDS_CORE_* of the direct sum */
+  double d;            /* cut-off d, or Vatistas index */
+  double co;           /* reach cut-off */
+  int precision;       /* WINDS_PREC_* */
+  int pcc_double_add;  /* 1: the corrector's induced velocity is also added to the next
+                          step's velocity (numerical/pcc.m:71 then WInDS.m:168) */
+  int stretch;         /* 1: filament stretching (user.roll = 'true') */
+} winds_wake_params;
+
+/* Creates the batch on the current device and uploads every case. */
+int winds_wake_create(const winds_wake_case *cases, int ncases, const winds_wake_params *prm,
+                      winds_wake_batch **out);
+
+/* Advances every case by `nsteps` steps. use_graph: capture one step into a
+ * CUDA graph on the first call and replay it. Synchronous. */
+int winds_wake_step(winds_wake_batch *b, int nsteps, int use_graph);
+
+/* Copies one case's state to host arrays (any pointer may be NULL):
+ * dom [nst,3,na,nb], bound [ns,nb], shed [ns,na,nb], trail [nst,na-1,nb],
+ * rc_shed / rc_trail (effective squared cores of the last evaluation, same
+ * shapes), uind [nst,3,na,nb] (induced velocity of the last step's first
+ * evaluation). */
+int winds_wake_get_state(winds_wake_batch *b, int icase, double *dom, double *bound,
+                         double *shed, double *trail, double *rc_shed, double *rc_trail,
+                         double *uind);
+
+/* Replaces one case's bound circulation [ns,nb] (e.g. after a Kutta-Joukowski
+ * iteration); it enters at the next step's bookkeeping. */
+int winds_wake_set_bound(winds_wake_batch *b, int icase, const double *bound);
+
+/* Device time of the last step (ms, CUDA events around the whole step),
+ * interactions per step over all cases and evaluations, and the number of
+ * kernels one step launches. */
+int winds_wake_stats(winds_wake_batch *b, double *step_ms, long long *interactions,
+                     int *launches_per_step);
+
+void winds_wake_destroy(winds_wake_batch *b);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WINDS_WAKE_H */

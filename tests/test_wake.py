@@ -1,0 +1,74 @@
+"""CPU tests of the free-wake step oracle (oracle/wake_ref.py) on properties
+the reference's step must have."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+
+@pytest.fixture(scope="module")
+def wake_ref():
+    import wake_ref as w
+    return w
+
+
+def _case(synth, wake_ref, gamma_zero=False, **kw):
+    rc = synth.RotorCase(nst=6, nsteps=9, dpsi_deg=10.0, seed=3, **kw)
+    c = synth.make_wake_case(rc, nsteps=8)
+    if gamma_zero:
+        c["bound"][:] = 0.0
+        c["trail_gamma"][:] = 0.0
+    return wake_ref.WakeCaseRef(**{k: c[k] for k in wake_ref.WakeCaseRef.__dataclass_fields__})
+
+
+@pytest.mark.parametrize("integ", ["fe", "ab2", "ab4", "pcc"])
+def test_zero_circulation_convects_with_freestream(synth, wake_ref, integ):
+    """No vorticity: every integrator moves the wake rigidly with the wind,
+    except where ab2/ab4 pad the shifted velocity history with zeros
+    (ab2.m:39, ab4.m:79-81: the youngest columns)."""
+    c = _case(synth, wake_ref, gamma_zero=True)
+    w = wake_ref.WakeRef(c, integrator=integ)
+    first = {"fe": 2, "pcc": 2, "ab2": 3, "ab4": 5}[integ]
+    for _ in range(4):
+        before = w.dom.copy()
+        w.step()
+        assert np.abs(w.uind).max() == 0.0
+        np.testing.assert_allclose(w.dom[:, :, first:], before[:, :, first - 1:-1] + c.dt * np.array(
+            [c.wind[0, 0], 0.0, 0.0])[None, :, None, None], rtol=0, atol=1e-12)
+        np.testing.assert_array_equal(w.dom[:, :, 0], c.quarter[:, :, w.step_idx])
+
+
+def test_bookkeeping_conserves_circulation(synth, wake_ref):
+    """Kelvin: every trailing column sums to zero across the span and the shed
+    columns close the trailing ones (WInDS.m:131-140)."""
+    c = _case(synth, wake_ref)
+    shed, trail = wake_ref.bookkeeping(c.bound, c.trail_gamma)
+    np.testing.assert_allclose(trail.sum(axis=0), 0.0, atol=1e-11)
+    np.testing.assert_allclose(shed[:, 1:].sum(axis=1) + trail[:-1].cumsum(axis=0)[:, 0], 0.0,
+                               atol=1e-10)
+    np.testing.assert_array_equal(shed[:, 0], c.bound)
+
+
+def test_rigid_translation_has_no_stretch(synth, wake_ref):
+    c = _case(synth, wake_ref)
+    sh, tr = wake_ref.lengths(c.dom)
+    moved = c.dom + np.array([1.5, -0.5, 2.0])[None, :, None, None]
+    sh2, tr2 = wake_ref.lengths(moved)
+    shed, trail = wake_ref.bookkeeping(c.bound, c.trail_gamma)
+    a = wake_ref.cores(c, shed, trail, 0.0, (sh2, tr2), (sh, tr), True)
+    b = wake_ref.cores(c, shed, trail, 0.0, (sh, tr), None, False)
+    for x, y in zip(a, b):
+        np.testing.assert_allclose(x, y, rtol=1e-12)
+
+
+def test_core_growth_formula(synth, wake_ref):
+    """Age form rc^2 = rc0^2 + 4 alpha delta nu (1 + a1 Re) age; vcore.m form
+    r0^2 + 4 alpha nu (1 + a1 Re) t."""
+    c = _case(synth, wake_ref)
+    g = np.array([0.0, 3.0, -7.0])
+    age = np.array([0.0, 0.5, 2.0])
+    np.testing.assert_allclose(wake_ref.core(c, g, age),
+                               c.rc0 ** 2 + 4 * c.alpha * c.delta * c.nu * (1 + c.a1 * np.abs(g) / c.nu) * age)
+    c.core_mode = 0
+    np.testing.assert_allclose(wake_ref.core(c, g, 1.5),
+                               c.r0 ** 2 + 4 * c.alpha * c.nu * (1 + c.a1 * np.abs(g) / c.nu) * 1.5)

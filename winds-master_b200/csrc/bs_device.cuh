@@ -5,6 +5,7 @@
 // near-singular fix-up of the FP32 kernel).
 #pragma once
 
+#include <cfloat>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -130,6 +131,88 @@ __host__ __device__ inline float key_float(int k) {
   float f;
   memcpy(&f, &i, sizeof(f));
   return f;
+}
+
+// Block-level min/max of three floats, then one atomic per block and bound.
+__device__ __forceinline__ void bbox_accumulate(const float lo[3], const float hi[3], int *gmin,
+                                                int *gmax) {
+  __shared__ float smin[3][32], smax[3][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  float l[3] = {lo[0], lo[1], lo[2]}, h[3] = {hi[0], hi[1], hi[2]};
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    for (int o = 16; o > 0; o >>= 1) {
+      l[c] = fminf(l[c], __shfl_xor_sync(0xffffffffu, l[c], o));
+      h[c] = fmaxf(h[c], __shfl_xor_sync(0xffffffffu, h[c], o));
+    }
+    if (lane == 0) {
+      smin[c][warp] = l[c];
+      smax[c][warp] = h[c];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    const int c = threadIdx.x;
+    float a = FLT_MAX, b = -FLT_MAX;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      a = fminf(a, smin[c][w]);
+      b = fmaxf(b, smax[c][w]);
+    }
+    atomicMin(&gmin[c], float_key(a));
+    atomicMax(&gmax[c], float_key(b));
+  }
+}
+
+// ------------------------------------------------------- filament packing
+// Writes filament f in the packed layout (see bs_types.h): FP32 hi/lo x1,
+// |L|^2, near-singular radius Rn^2 = max(|L|^2, 9 rc^2), L, gamma/4pi and the
+// core term, plus the FP64 copy. A NaN/Inf ubar is zeroed by the reference
+// (core/BiotSavart.m:111); with finite endpoints that happens exactly when
+// gamma (or, Vatistas, rc; or, cut-off, d*|L|^2) is not finite, so such
+// filaments get gamma/4pi = 0 and contribute nothing.
+__device__ __forceinline__ void pack_filament(long long f, double x1, double y1, double z1,
+                                              double x2, double y2, double z2, double g, double r,
+                                              int model, double dcut, float4 *fa, float4 *fb,
+                                              float4 *fc, float *fd, double4 *ra, double4 *rb) {
+  ra[f] = make_double4(x1, y1, z1, g);
+  rb[f] = make_double4(x2, y2, z2, r);
+  const double Lx = x2 - x1, Ly = y2 - y1, Lz = z2 - z1;
+  const double L2 = Lx * Lx + Ly * Ly + Lz * Lz;
+  double K = g / k4Pi;
+  double D;
+  if (model == kCoreVatistas) {
+    D = (r * L2) * (r * L2);
+    if (!isfinite(r)) K = 0.0;
+    if (!(D >= 1e-30)) D = 1e-30;
+    if (D > 1e30) D = 1e30;
+  } else {
+    D = dcut * L2;
+    if (!isfinite(D)) K = 0.0, D = 0.0;
+  }
+  if (!isfinite(g)) K = 0.0;
+  // Near-singular region: r1.r2 < Rn^2, a ball around the midpoint of radius
+  // sqrt(|L|^2/4 + Rn^2) that contains every point within 3 core radii.
+  double Rn2 = L2;
+  if (isfinite(r) && 9.0 * r > Rn2) Rn2 = 9.0 * r;
+  if (!(Rn2 > 1e-20)) Rn2 = 1e-20;
+  const float hx = (float)x1, hy = (float)y1, hz = (float)z1;
+  fa[f] = make_float4(hx, hy, hz, (float)L2);
+  fb[f] = make_float4((float)(x1 - (double)hx), (float)(y1 - (double)hy), (float)(z1 - (double)hz),
+                      (float)Rn2);
+  fc[f] = make_float4((float)Lx, (float)Ly, (float)Lz, (float)K);
+  fd[f] = (float)D;
+}
+
+// Inert filament (far away, zero length, zero circulation) for padding.
+__device__ __forceinline__ void pack_inert(long long f, float4 *fa, float4 *fb, float4 *fc,
+                                           float *fd, double4 *ra, double4 *rb) {
+  const double far = 1e18;
+  fa[f] = make_float4((float)far, (float)far, (float)far, 0.f);
+  fb[f] = make_float4(0.f, 0.f, 0.f, 0.f);
+  fc[f] = make_float4(0.f, 0.f, 0.f, 0.f);
+  fd[f] = 1.f;
+  ra[f] = make_double4(far, far, far, 0.0);
+  rb[f] = make_double4(far, far, far, 0.0);
 }
 
 // ---------------------------------------------------- FP64 reference pair term

@@ -36,36 +36,6 @@ __global__ void bs_bbox_init(BBox *bb) {
   }
 }
 
-// Block-level min/max of three floats, then one atomic per block and bound.
-__device__ __forceinline__ void bbox_accumulate(const float lo[3], const float hi[3], int *gmin,
-                                                int *gmax) {
-  __shared__ float smin[3][32], smax[3][32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  float l[3] = {lo[0], lo[1], lo[2]}, h[3] = {hi[0], hi[1], hi[2]};
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    for (int o = 16; o > 0; o >>= 1) {
-      l[c] = fminf(l[c], __shfl_xor_sync(0xffffffffu, l[c], o));
-      h[c] = fmaxf(h[c], __shfl_xor_sync(0xffffffffu, h[c], o));
-    }
-    if (lane == 0) {
-      smin[c][warp] = l[c];
-      smax[c][warp] = h[c];
-    }
-  }
-  __syncthreads();
-  if (threadIdx.x < 3) {
-    const int c = threadIdx.x;
-    float a = FLT_MAX, b = -FLT_MAX;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-      a = fminf(a, smin[c][w]);
-      b = fmaxf(b, smax[c][w]);
-    }
-    atomicMin(&gmin[c], float_key(a));
-    atomicMax(&gmax[c], float_key(b));
-  }
-}
-
 __global__ void bs_pack_filaments(const double *__restrict__ F1, const double *__restrict__ F2,
                                   const double *__restrict__ gam, const double *__restrict__ rc,
                                   long long d0, long long nf, long long off, int model, double dcut,
@@ -79,36 +49,7 @@ __global__ void bs_pack_filaments(const double *__restrict__ F1, const double *_
     const double x1 = F1[b], y1 = F1[b + d0], z1 = F1[b + 2 * d0];
     const double x2 = F2[b], y2 = F2[b + d0], z2 = F2[b + 2 * d0];
     const double g = gam[f], r = rc[f];
-    ra[off + f] = make_double4(x1, y1, z1, g);
-    rb[off + f] = make_double4(x2, y2, z2, r);
-    const double Lx = x2 - x1, Ly = y2 - y1, Lz = z2 - z1;
-    const double L2 = Lx * Lx + Ly * Ly + Lz * Lz;
-    double K = g / k4Pi;
-    // A NaN/Inf ubar is zeroed by the reference (core/BiotSavart.m:111); with
-    // finite endpoints that happens exactly when gamma (or, Vatistas, rc; or,
-    // cut-off, d*|L|^2) is not finite, so such filaments contribute nothing.
-    double D;
-    if (model == kCoreVatistas) {
-      D = (r * L2) * (r * L2);
-      if (!isfinite(r)) K = 0.0;
-      if (!(D >= 1e-30)) D = 1e-30;
-      if (D > 1e30) D = 1e30;
-    } else {
-      D = dcut * L2;
-      if (!isfinite(D)) K = 0.0, D = 0.0;
-    }
-    if (!isfinite(g)) K = 0.0;
-    // Near-singular region: r1.r2 < Rn^2, a ball around the midpoint of radius
-    // sqrt(|L|^2/4 + Rn^2) that contains every point within 3 core radii.
-    double Rn2 = L2;
-    if (isfinite(r) && 9.0 * r > Rn2) Rn2 = 9.0 * r;
-    if (!(Rn2 > 1e-20)) Rn2 = 1e-20;
-    const float hx = (float)x1, hy = (float)y1, hz = (float)z1;
-    fa[off + f] = make_float4(hx, hy, hz, (float)L2);
-    fb[off + f] = make_float4((float)(x1 - (double)hx), (float)(y1 - (double)hy),
-                              (float)(z1 - (double)hz), (float)Rn2);
-    fc[off + f] = make_float4((float)Lx, (float)Ly, (float)Lz, (float)K);
-    fd[off + f] = (float)D;
+    pack_filament(off + f, x1, y1, z1, x2, y2, z2, g, r, model, dcut, fa, fb, fc, fd, ra, rb);
     lo[0] = (float)fmin(x1, x2), lo[1] = (float)fmin(y1, y2), lo[2] = (float)fmin(z1, z2);
     hi[0] = (float)fmax(x1, x2), hi[1] = (float)fmax(y1, y2), hi[2] = (float)fmax(z1, z2);
   }
@@ -120,13 +61,7 @@ __global__ void bs_pad_filaments(long long from, long long to, float4 *fa, float
                                  float *fd, double4 *ra, double4 *rb) {
   const long long f = from + (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= to) return;
-  const double far = 1e18;
-  fa[f] = make_float4((float)far, (float)far, (float)far, 0.f);
-  fb[f] = make_float4(0.f, 0.f, 0.f, 0.f);
-  fc[f] = make_float4(0.f, 0.f, 0.f, 0.f);
-  fd[f] = 1.f;
-  ra[f] = make_double4(far, far, far, 0.0);
-  rb[f] = make_double4(far, far, far, 0.0);
+  pack_inert(f, fa, fb, fc, fd, ra, rb);
 }
 
 __global__ void bs_pack_targets(const double *__restrict__ P, long long ns, long long np,

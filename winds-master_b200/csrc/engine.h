@@ -74,6 +74,8 @@ struct Context {
 };
 
 int fail(int code, const char *fmt, ...);
+void build_plan(Plan &pl, const std::vector<GroupSpec> &gs, int tile_cap, int resident,
+                double waves, int chunk_quantum);
 int resolve_model(const winds_bs_params *prm, int *model, double *dcut, double *n, int *prec);
 int validate_family(const winds_bs_family &f);
 TuneChoice default_choice(long long nt);

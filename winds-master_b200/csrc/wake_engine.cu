@@ -1,0 +1,544 @@
+// wake_engine.cu -- host side of the batched free-wake step (include/winds_wake.h).
+//
+// One batch holds every case's state in shared device buffers. A step is a
+// fixed sequence of kernel launches on the batch's stream:
+//   bookkeeping -> [pack filaments + targets -> sort -> direct sum -> reduce]
+//   -> convect (fe/ab2/ab4, or pcc predictor) -> (pcc: bookkeeping for p+1
+//   -> [direct sum at the predicted nodes] -> corrector) -> commit.
+// All sizes are fixed at creation (each wake keeps na columns), so the plan
+// tables of the persistent direct-sum kernel are built once and the whole
+// step can be captured once as a CUDA graph and replayed. The step counter
+// lives on the device, so a replayed graph reads the right kinematics row.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "bs_launch.h"
+#include "engine.h"
+#include "wake_launch.h"
+#include "winds_wake.h"
+
+using namespace winds;
+
+struct winds_wake_batch {
+  int dev = 0;
+  int ncases = 0;
+  winds_wake_params prm{};
+  int model = kCoreVatistas, prec = WINDS_PREC_F32C;
+  double dcut = 0.0, nidx = 2.0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<WakeCase> cases;
+  long long nodes = 0, shed_n = 0, trail_n = 0, bound_n = 0, fil_pad = 0, kin_n = 0, wind_n = 0;
+  long long max_nodes = 0, max_cols = 0, max_fil = 0, max_slots = 0;
+  long long interactions = 0;
+  int launches = 0;
+  // state and work buffers
+  DevBuf cases_d, step_d;
+  DevBuf dom, dom_pred, dom_new, vel, h1, h2, h3, uind, uind_pred;
+  DevBuf bound, trail_prev, shed_cur, trail_cur, shed_next, trail_next;
+  DevBuf rc_s, rc_t, len_old_s, len_old_t, len_s, len_t, len_ps, len_pt;
+  DevBuf quarter, trailing, wind;
+  // direct-sum buffers
+  DevBuf fa, fb, fc, fd, ra, rb, tp, tp_raw, tgroup, keys, vals, perm, sort_tmp;
+  DevBuf groups_main, groups_pred, tiles, items, part, bbox, ctr, err, nearctr;
+  size_t sort_bytes = 0;
+  int n_tiles = 0, n_items = 0, tile_cap = 0, grid = 0;
+  TuneChoice ch;
+  long long steps_done = 0;
+  long long min_nsteps = 0;  // kinematics rows available in every case
+};
+
+namespace {
+
+template <class T>
+T *P(DevBuf &b) {
+  return static_cast<T *>(b.p);
+}
+
+int alloc_all(winds_wake_batch *b) {
+  cudaStream_t s = b->stream;
+  const size_t n3 = (size_t)b->nodes * 3 * sizeof(double);
+  int rc;
+  for (DevBuf *x : {&b->dom, &b->dom_pred, &b->dom_new, &b->vel, &b->h1, &b->h2, &b->h3, &b->uind,
+                    &b->uind_pred})
+    if ((rc = x->ensure(n3, s))) return rc;
+  const size_t sb = std::max<long long>(b->shed_n, 1) * sizeof(double);
+  const size_t tb = std::max<long long>(b->trail_n, 1) * sizeof(double);
+  for (DevBuf *x : {&b->shed_cur, &b->shed_next, &b->rc_s, &b->len_old_s, &b->len_s, &b->len_ps})
+    if ((rc = x->ensure(sb, s))) return rc;
+  for (DevBuf *x : {&b->trail_prev, &b->trail_cur, &b->trail_next, &b->rc_t, &b->len_old_t,
+                    &b->len_t, &b->len_pt})
+    if ((rc = x->ensure(tb, s))) return rc;
+  if ((rc = b->bound.ensure(b->bound_n * sizeof(double), s)) ||
+      (rc = b->quarter.ensure(b->kin_n * sizeof(double), s)) ||
+      (rc = b->trailing.ensure(b->kin_n * sizeof(double), s)) ||
+      (rc = b->wind.ensure(b->wind_n * sizeof(double), s)) ||
+      (rc = b->cases_d.ensure(b->ncases * sizeof(WakeCase), s)) ||
+      (rc = b->step_d.ensure(4 * sizeof(int), s)))
+    return rc;
+  const long long nf = b->fil_pad, nt = std::max<long long>(b->nodes, 1);
+  if ((rc = b->fa.ensure(nf * sizeof(float4), s)) || (rc = b->fb.ensure(nf * sizeof(float4), s)) ||
+      (rc = b->fc.ensure(nf * sizeof(float4), s)) || (rc = b->fd.ensure(nf * sizeof(float), s)) ||
+      (rc = b->ra.ensure(nf * sizeof(double4), s)) || (rc = b->rb.ensure(nf * sizeof(double4), s)) ||
+      (rc = b->tp.ensure(nt * sizeof(double4), s)) ||
+      (rc = b->tp_raw.ensure(nt * sizeof(double4), s)) ||
+      (rc = b->tgroup.ensure(nt * sizeof(int), s)) ||
+      (rc = b->keys.ensure(nt * 2 * sizeof(unsigned long long), s)) ||
+      (rc = b->vals.ensure(nt * sizeof(int), s)) || (rc = b->perm.ensure(nt * sizeof(int), s)) ||
+      (rc = b->bbox.ensure(sizeof(BBox), s)) || (rc = b->ctr.ensure(64, s)) ||
+      (rc = b->err.ensure(64, s)) || (rc = b->nearctr.ensure(64, s)))
+    return rc;
+  if (sort_target_keys(nullptr, &b->sort_bytes, nullptr, nullptr, nullptr, nullptr, b->nodes, s) !=
+      cudaSuccess)
+    return fail(WINDS_BS_ERR_CUDA, "target sort size query failed");
+  return b->sort_tmp.ensure(b->sort_bytes + 256, s);
+}
+
+// Direct-sum plan: case c's nodes (one group) against case c's filaments.
+int build_plans(winds_wake_batch *b) {
+  std::vector<GroupSpec> gs;
+  for (const WakeCase &c : b->cases) {
+    GroupSpec g;
+    g.out = P<double>(b->uind) + c.node_off * 3;
+    g.t_begin = c.node_off;
+    g.t_count = (long long)c.nst * c.na * c.nb;
+    g.ns_p = c.nst;
+    g.f_begin = (int)c.fil_off;
+    g.f_end = (int)(c.fil_off + c.fil_pad);
+    g.accumulate = 0;
+    gs.push_back(g);
+  }
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->dev);
+  int resident, quantum;
+  if (b->prec == WINDS_PREC_F64) {
+    b->tile_cap = f64_threads();
+    resident = f64_occupancy() * sms;
+    quantum = f64_tile();
+  } else {
+    b->tile_cap = f32c_threads() * b->ch.T;
+    resident = f32c_occupancy(b->model, b->ch.T, b->ch.KF) * sms;
+    quantum = kFilamentPad;
+  }
+  Plan pl;
+  build_plan(pl, gs, b->tile_cap, resident, b->ch.waves, quantum);
+  b->n_tiles = (int)pl.tiles.size();
+  b->n_items = (int)pl.items.size();
+  b->grid = std::max(1, std::min(b->n_items, resident));
+  std::vector<Group> gp = pl.groups;
+  for (size_t k = 0; k < gp.size(); ++k) gp[k].out = P<double>(b->uind_pred) + b->cases[k].node_off * 3;
+  int rc;
+  cudaStream_t s = b->stream;
+  if ((rc = b->groups_main.ensure(pl.groups.size() * sizeof(Group), s)) ||
+      (rc = b->groups_pred.ensure(gp.size() * sizeof(Group), s)) ||
+      (rc = b->tiles.ensure(pl.tiles.size() * sizeof(Tile), s)) ||
+      (rc = b->items.ensure(pl.items.size() * sizeof(Item), s)) ||
+      (rc = b->part.ensure((size_t)b->n_items * 3 * b->tile_cap * sizeof(double), s)))
+    return rc;
+  cudaError_t e;
+  if ((e = cudaMemcpy(b->groups_main.p, pl.groups.data(), pl.groups.size() * sizeof(Group),
+                      cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMemcpy(b->groups_pred.p, gp.data(), gp.size() * sizeof(Group),
+                      cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMemcpy(b->tiles.p, pl.tiles.data(), pl.tiles.size() * sizeof(Tile),
+                      cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMemcpy(b->items.p, pl.items.data(), pl.items.size() * sizeof(Item),
+                      cudaMemcpyHostToDevice)) != cudaSuccess)
+    return cuda_fail(e, "wake plan upload");
+  return WINDS_BS_OK;
+}
+
+// One induced-velocity evaluation of every case (nodes of `dom`, Γ, cores).
+cudaError_t enqueue_eval(winds_wake_batch *b, const double *dom, const double *shed,
+                         const double *trail, int step_add, const double *lold_s,
+                         const double *lold_t, int have_old, double *lnew_s, double *lnew_t,
+                         double *rc_s, double *rc_t, DevBuf &groups, int &launches) {
+  cudaStream_t s = b->stream;
+  const WakeCase *cd = P<const WakeCase>(b->cases_d);
+  PackedFilaments pf{P<float4>(b->fa), P<float4>(b->fb), P<float4>(b->fc), P<float>(b->fd),
+                     P<double4>(b->ra), P<double4>(b->rb)};
+  BBox *bb = P<BBox>(b->bbox);
+  cudaError_t e = launch_bbox_init(bb, s);
+  if (e == cudaSuccess)
+    e = launch_wake_filaments(cd, b->ncases, b->max_fil, P<const int>(b->step_d), step_add, dom,
+                              shed, trail, lold_s, lold_t, have_old, b->prm.stretch, lnew_s, lnew_t,
+                              rc_s, rc_t, b->model, b->dcut, pf, bb, s);
+  if (e == cudaSuccess)
+    e = launch_wake_targets(cd, b->ncases, b->max_nodes, dom, P<double4>(b->tp_raw),
+                            P<int>(b->tgroup), bb, s);
+  unsigned long long *k0 = P<unsigned long long>(b->keys), *k1 = k0 + std::max<long long>(b->nodes, 1);
+  if (e == cudaSuccess)
+    e = launch_target_keys(P<const double4>(b->tp_raw), P<const int>(b->tgroup), b->nodes, bb, k0,
+                           P<int>(b->vals), s);
+  if (e == cudaSuccess)
+    e = sort_target_keys(b->sort_tmp.p, &b->sort_bytes, k0, k1, P<const int>(b->vals),
+                         P<int>(b->perm), b->nodes, s);
+  if (e == cudaSuccess)
+    e = launch_gather_targets(P<const double4>(b->tp_raw), P<const int>(b->perm), b->nodes,
+                              P<double4>(b->tp), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(b->ctr.p, 0, sizeof(unsigned), s);
+  F32cArgs a;
+  a.fa = pf.fa;
+  a.fb = pf.fb;
+  a.fc = pf.fc;
+  a.fd = pf.fd;
+  a.ra = pf.ra;
+  a.rb = pf.rb;
+  a.tp = P<const double4>(b->tp);
+  a.groups = P<const Group>(groups);
+  a.tiles = P<const Tile>(b->tiles);
+  a.items = P<const Item>(b->items);
+  a.n_items = b->n_items;
+  a.tile_cap = b->tile_cap;
+  a.part = P<double>(b->part);
+  a.work_ctr = P<unsigned>(b->ctr);
+  a.err = P<unsigned>(b->err);
+  a.near_ctr = P<unsigned long long>(b->nearctr);
+  a.bbox = bb;
+  a.model = b->model;
+  a.d = b->dcut;
+  a.n = b->nidx;
+  a.co = b->prm.co;
+  a.wait_limit_ns = default_wait_limit_ns();
+  if (e == cudaSuccess)
+    e = b->prec == WINDS_PREC_F64 ? launch_f64(a, b->grid, s)
+                                  : launch_f32c(a, b->model, b->ch.T, b->ch.KF, b->grid, s);
+  if (e == cudaSuccess)
+    e = launch_reduce(P<const Tile>(b->tiles), b->n_tiles, P<const Group>(groups),
+                      P<const double>(b->part), P<const int>(b->perm), b->tile_cap, s);
+  launches += 12;  // bbox, filaments, targets, keys, sort (4), gather, memset, sum, reduce
+  return e;
+}
+
+cudaError_t enqueue_step(winds_wake_batch *b, int &launches) {
+  cudaStream_t s = b->stream;
+  const WakeCase *cd = P<const WakeCase>(b->cases_d);
+  const int *step = P<const int>(b->step_d);
+  launches = 0;
+  const bool pcc = b->prm.integrator == WINDS_INTEG_PCC;
+  cudaError_t e = launch_wake_bookkeep(cd, b->ncases, b->max_cols, P<const double>(b->bound),
+                                       P<const double>(b->trail_prev), P<double>(b->shed_cur),
+                                       P<double>(b->trail_cur), s);
+  ++launches;
+  // have_old: lengths of a previous step exist from step 1 on (read on device
+  // through the counter would need a branch in the kernel; the host tracks it)
+  if (e == cudaSuccess)
+    e = enqueue_eval(b, P<const double>(b->dom), P<const double>(b->shed_cur),
+                     P<const double>(b->trail_cur), 0, P<const double>(b->len_old_s),
+                     P<const double>(b->len_old_t), 1, P<double>(b->len_s), P<double>(b->len_t),
+                     P<double>(b->rc_s), P<double>(b->rc_t), b->groups_main, launches);
+  int mode = kConvectFE;
+  if (b->prm.integrator == WINDS_INTEG_AB2) mode = kConvectAB2;
+  if (b->prm.integrator == WINDS_INTEG_AB4) mode = kConvectAB4;
+  const double *carry = pcc && b->prm.pcc_double_add ? P<const double>(b->uind_pred) : nullptr;
+  if (e == cudaSuccess)
+    e = launch_wake_convect(cd, b->ncases, b->max_nodes, step, mode, P<const double>(b->dom),
+                            P<const double>(b->uind), carry, nullptr, nullptr, P<double>(b->vel),
+                            P<const double>(b->h1), P<const double>(b->h2), P<const double>(b->h3),
+                            P<const double>(b->quarter), P<const double>(b->trailing),
+                            P<const double>(b->wind), pcc ? P<double>(b->dom_pred) : P<double>(b->dom_new), s);
+  ++launches;
+  if (pcc) {
+    if (e == cudaSuccess)
+      e = launch_wake_bookkeep(cd, b->ncases, b->max_cols, P<const double>(b->bound),
+                               P<const double>(b->trail_cur), P<double>(b->shed_next),
+                               P<double>(b->trail_next), s);
+    ++launches;
+    if (e == cudaSuccess)
+      e = enqueue_eval(b, P<const double>(b->dom_pred), P<const double>(b->shed_next),
+                       P<const double>(b->trail_next), 1, P<const double>(b->len_s),
+                       P<const double>(b->len_t), 1, P<double>(b->len_ps), P<double>(b->len_pt),
+                       nullptr, nullptr, b->groups_pred, launches);
+    if (e == cudaSuccess)
+      e = launch_wake_convect(cd, b->ncases, b->max_nodes, step, kConvectCorrector,
+                              P<const double>(b->dom), nullptr, nullptr, P<const double>(b->dom_pred),
+                              P<const double>(b->uind_pred), P<double>(b->vel), nullptr, nullptr,
+                              nullptr, P<const double>(b->quarter), P<const double>(b->trailing),
+                              P<const double>(b->wind), P<double>(b->dom_new), s);
+    ++launches;
+  }
+  const int keep_hist = b->prm.integrator == WINDS_INTEG_AB2 || b->prm.integrator == WINDS_INTEG_AB4;
+  if (e == cudaSuccess)
+    e = launch_wake_commit(cd, b->ncases, b->max_slots, P<int>(b->step_d), P<double>(b->dom),
+                           P<const double>(b->dom_new), P<double>(b->vel), P<double>(b->h1),
+                           P<double>(b->h2), P<double>(b->h3), keep_hist, P<double>(b->trail_prev),
+                           P<const double>(b->trail_cur), P<double>(b->len_old_s),
+                           P<const double>(b->len_s), P<double>(b->len_old_t),
+                           P<const double>(b->len_t), s);
+  ++launches;
+  return e;
+}
+
+}  // namespace
+
+extern "C" {
+
+int winds_wake_create(const winds_wake_case *cases, int ncases, const winds_wake_params *prm,
+                      winds_wake_batch **out) {
+  if (!out || !prm || ncases <= 0 || !cases) return fail(WINDS_BS_ERR_ARG, "bad batch arguments");
+  *out = nullptr;
+  winds_bs_params bp;
+  std::memset(&bp, 0, sizeof(bp));
+  bp.core_model = prm->core_model;
+  bp.d = prm->d;
+  bp.co = prm->co;
+  bp.precision = prm->precision;
+  int model, prec, rc;
+  double dcut, nidx;
+  if ((rc = resolve_model(&bp, &model, &dcut, &nidx, &prec))) return rc;
+  if (prm->integrator < WINDS_INTEG_FE || prm->integrator > WINDS_INTEG_PCC)
+    return fail(WINDS_BS_ERR_ARG, "unknown integrator %d", prm->integrator);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0)
+    return fail(WINDS_BS_ERR_NODEV, "no CUDA device is visible");
+  winds_wake_batch *b = new winds_wake_batch();
+  cudaGetDevice(&b->dev);
+  b->ncases = ncases;
+  b->prm = *prm;
+  b->model = model;
+  b->prec = prec;
+  b->dcut = dcut;
+  b->nidx = nidx;
+  cudaError_t e;
+  if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaEventCreate(&b->ev0)) != cudaSuccess || (e = cudaEventCreate(&b->ev1)) != cudaSuccess) {
+    delete b;
+    return cuda_fail(e, "wake stream/events");
+  }
+  long long node = 0, sh = 0, tr = 0, bd = 0, fil = 0, kin = 0, wnd = 0;
+  for (int k = 0; k < ncases; ++k) {
+    const winds_wake_case &h = cases[k];
+    if (h.nst < 2 || h.nb < 1 || h.na < 3 || h.nsteps < 2 || !(h.dt > 0) || !h.quarter ||
+        !h.trailing || !h.wind || !h.dom || !h.bound || !h.trail_gamma) {
+      winds_wake_destroy(b);
+      return fail(WINDS_BS_ERR_ARG, "case %d: bad sizes or null arrays", k);
+    }
+    WakeCase c;
+    std::memset(&c, 0, sizeof(c));
+    c.nst = h.nst, c.nb = h.nb, c.na = h.na, c.nsteps = h.nsteps;
+    c.node_off = node, c.shed_off = sh, c.trail_off = tr, c.bound_off = bd, c.fil_off = fil;
+    c.fil_count = (long long)(h.nst - 1) * h.na * h.nb + (long long)h.nst * (h.na - 1) * h.nb;
+    c.fil_pad = (c.fil_count + kFilamentPad - 1) / kFilamentPad * kFilamentPad;
+    c.kin_off = kin, c.wind_off = wnd;
+    c.dt = h.dt, c.t0 = h.t0, c.shear = h.shear, c.hub = h.hub_height > 0 ? h.hub_height : 1.0;
+    c.r0 = h.r0, c.rc0 = h.rc0, c.alpha = h.alpha, c.nu = h.nu, c.a1 = h.a1, c.delta = h.delta;
+    c.core_mode = h.core_mode;
+    const long long nn = (long long)h.nst * h.na * h.nb;
+    node += nn;
+    sh += (long long)(h.nst - 1) * h.na * h.nb;
+    tr += (long long)h.nst * (h.na - 1) * h.nb;
+    bd += (long long)(h.nst - 1) * h.nb;
+    fil += c.fil_pad;
+    kin += (long long)h.nst * 3 * h.nsteps * h.nb;
+    wnd += 3LL * h.nsteps;
+    b->max_nodes = std::max(b->max_nodes, nn);
+    b->max_cols = std::max<long long>(b->max_cols, (long long)h.na * h.nb);
+    b->max_fil = std::max(b->max_fil, c.fil_pad);
+    b->max_slots = std::max(b->max_slots, nn);
+    b->interactions += nn * c.fil_count;
+    b->min_nsteps = k == 0 ? h.nsteps : std::min<long long>(b->min_nsteps, h.nsteps);
+    b->cases.push_back(c);
+  }
+  b->nodes = node, b->shed_n = sh, b->trail_n = tr, b->bound_n = bd, b->fil_pad = fil;
+  b->kin_n = kin, b->wind_n = wnd;
+  if (prm->integrator == WINDS_INTEG_PCC) b->interactions *= 2;
+  if (fil > (1ll << 30) || node > (1ll << 30)) {
+    winds_wake_destroy(b);
+    return fail(WINDS_BS_ERR_ARG, "batch too large");
+  }
+  b->ch = default_choice(node);
+  b->ch.waves = 32.0;
+  if (prec == WINDS_PREC_F32C) lookup_tune(model, node, fil, &b->ch);
+  if ((rc = alloc_all(b)) || (rc = build_plans(b))) {
+    winds_wake_destroy(b);
+    return rc;
+  }
+  // upload cases and initial state
+  std::vector<double> tmp;
+  e = cudaMemcpy(b->cases_d.p, b->cases.data(), ncases * sizeof(WakeCase), cudaMemcpyHostToDevice);
+  for (int k = 0; k < ncases && e == cudaSuccess; ++k) {
+    const winds_wake_case &h = cases[k];
+    const WakeCase &c = b->cases[k];
+    const long long nn = (long long)h.nst * h.na * h.nb;
+    const long long nkin = (long long)h.nst * 3 * h.nsteps * h.nb;
+    const long long ntr = (long long)h.nst * (h.na - 1) * h.nb;
+    e = cudaMemcpy(P<double>(b->dom) + c.node_off * 3, h.dom, nn * 3 * sizeof(double),
+                   cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(P<double>(b->bound) + c.bound_off, h.bound,
+                     (size_t)(h.nst - 1) * h.nb * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(P<double>(b->quarter) + c.kin_off, h.quarter, nkin * sizeof(double),
+                     cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(P<double>(b->trailing) + c.kin_off, h.trailing, nkin * sizeof(double),
+                     cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(P<double>(b->wind) + c.wind_off, h.wind, 3 * h.nsteps * sizeof(double),
+                     cudaMemcpyHostToDevice);
+    // the stored trailing columns are those of the step before: trail_prev(:,k) = trail(:,k+1)
+    if (e == cudaSuccess) {
+      tmp.assign(ntr, 0.0);
+      const int m = h.na - 1;
+      for (int bl = 0; bl < h.nb; ++bl)
+        for (int j = 0; j + 1 < m; ++j)
+          for (int i = 0; i < h.nst; ++i)
+            tmp[i + (long long)h.nst * (j + (long long)m * bl)] =
+                h.trail_gamma[i + (long long)h.nst * ((j + 1) + (long long)m * bl)];
+      e = cudaMemcpy(P<double>(b->trail_prev) + c.trail_off, tmp.data(), ntr * sizeof(double),
+                     cudaMemcpyHostToDevice);
+    }
+  }
+  const size_t n3 = (size_t)b->nodes * 3 * sizeof(double);
+  for (DevBuf *x : {&b->uind_pred, &b->vel, &b->h1, &b->h2, &b->h3, &b->uind, &b->dom_new, &b->dom_pred})
+    if (e == cudaSuccess) e = cudaMemset(x->p, 0, n3);
+  // no previous lengths yet: copying the initial lengths makes the first strain zero
+  if (e == cudaSuccess) e = cudaMemset(b->step_d.p, 0, 4 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(b->err.p, 0, 64);
+  if (e != cudaSuccess) {
+    winds_wake_destroy(b);
+    return cuda_fail(e, "wake upload");
+  }
+  {
+    // initial lengths = current lengths (zero strain at the first step)
+    int l = 0;
+    cudaError_t e2 = launch_wake_bookkeep(P<const WakeCase>(b->cases_d), b->ncases, b->max_cols,
+                                          P<const double>(b->bound), P<const double>(b->trail_prev),
+                                          P<double>(b->shed_cur), P<double>(b->trail_cur), b->stream);
+    if (e2 == cudaSuccess)
+      e2 = enqueue_eval(b, P<const double>(b->dom), P<const double>(b->shed_cur),
+                        P<const double>(b->trail_cur), 0, P<const double>(b->len_old_s),
+                        P<const double>(b->len_old_t), 0, P<double>(b->len_old_s),
+                        P<double>(b->len_old_t), nullptr, nullptr, b->groups_pred, l);
+    if (e2 == cudaSuccess) e2 = cudaStreamSynchronize(b->stream);
+    // that evaluation wrote the predicted-induction buffer: no carry at step 0
+    if (e2 == cudaSuccess) e2 = cudaMemset(b->uind_pred.p, 0, n3);
+    if (e2 != cudaSuccess) {
+      winds_wake_destroy(b);
+      return cuda_fail(e2, "wake initial lengths");
+    }
+  }
+  *out = b;
+  return WINDS_BS_OK;
+}
+
+int winds_wake_step(winds_wake_batch *b, int nsteps, int use_graph) {
+  if (!b || nsteps < 0) return fail(WINDS_BS_ERR_ARG, "bad step arguments");
+  if (b->steps_done + nsteps >= b->min_nsteps)
+    return fail(WINDS_BS_ERR_ARG, "kinematics cover %lld steps; %lld done, %d more requested",
+                b->min_nsteps - 1, b->steps_done, nsteps);
+  cudaSetDevice(b->dev);
+  cudaError_t e = cudaSuccess;
+  for (int k = 0; k < nsteps && e == cudaSuccess; ++k) {
+    if (use_graph) {
+      if (!b->exec) {
+        e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+        int l = 0;
+        cudaError_t e2 = e == cudaSuccess ? enqueue_step(b, l) : e;
+        cudaGraph_t g = nullptr;
+        e = cudaStreamEndCapture(b->stream, &g);
+        if (e2 != cudaSuccess) e = e2;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, g, 0);
+        b->graph = g;
+        b->launches = l;
+        if (e != cudaSuccess) break;
+      }
+      cudaEventRecord(b->ev0, b->stream);
+      e = cudaGraphLaunch(b->exec, b->stream);
+      cudaEventRecord(b->ev1, b->stream);
+    } else {
+      cudaEventRecord(b->ev0, b->stream);
+      e = enqueue_step(b, b->launches);
+      cudaEventRecord(b->ev1, b->stream);
+    }
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "wake step");
+  b->steps_done += nsteps;
+  e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "wake step sync");
+  unsigned word = 0;
+  cudaMemcpy(&word, b->err.p, sizeof(word), cudaMemcpyDeviceToHost);
+  if (word) {
+    cudaMemset(b->err.p, 0, sizeof(unsigned));
+    return fail(word & kErrWaitTimeout ? WINDS_BS_ERR_TIMEOUT : WINDS_BS_ERR_CUDA,
+                "device reported error word 0x%x", word);
+  }
+  return WINDS_BS_OK;
+}
+
+int winds_wake_get_state(winds_wake_batch *b, int icase, double *dom, double *bound, double *shed,
+                         double *trail, double *rc_shed, double *rc_trail, double *uind) {
+  if (!b || icase < 0 || icase >= b->ncases) return fail(WINDS_BS_ERR_ARG, "bad case index");
+  cudaSetDevice(b->dev);
+  cudaStreamSynchronize(b->stream);
+  const WakeCase &c = b->cases[icase];
+  const size_t nn = (size_t)c.nst * c.na * c.nb, ns = (size_t)(c.nst - 1) * c.na * c.nb,
+               nt = (size_t)c.nst * (c.na - 1) * c.nb, nbd = (size_t)(c.nst - 1) * c.nb;
+  cudaError_t e = cudaSuccess;
+  auto get = [&](double *dst, DevBuf &src, long long off, size_t n) {
+    if (dst && e == cudaSuccess)
+      e = cudaMemcpy(dst, P<double>(src) + off, n * sizeof(double), cudaMemcpyDeviceToHost);
+  };
+  get(dom, b->dom, c.node_off * 3, nn * 3);
+  get(bound, b->bound, c.bound_off, nbd);
+  get(shed, b->shed_cur, c.shed_off, ns);
+  get(trail, b->trail_cur, c.trail_off, nt);
+  get(rc_shed, b->rc_s, c.shed_off, ns);
+  get(rc_trail, b->rc_t, c.trail_off, nt);
+  get(uind, b->uind, c.node_off * 3, nn * 3);
+  return e == cudaSuccess ? WINDS_BS_OK : cuda_fail(e, "wake state read");
+}
+
+int winds_wake_set_bound(winds_wake_batch *b, int icase, const double *bound) {
+  if (!b || icase < 0 || icase >= b->ncases || !bound) return fail(WINDS_BS_ERR_ARG, "bad arguments");
+  cudaSetDevice(b->dev);
+  const WakeCase &c = b->cases[icase];
+  cudaError_t e = cudaMemcpyAsync(P<double>(b->bound) + c.bound_off, bound,
+                                  (size_t)(c.nst - 1) * c.nb * sizeof(double),
+                                  cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  return e == cudaSuccess ? WINDS_BS_OK : cuda_fail(e, "bound upload");
+}
+
+int winds_wake_stats(winds_wake_batch *b, double *step_ms, long long *interactions,
+                     int *launches_per_step) {
+  if (!b) return fail(WINDS_BS_ERR_ARG, "null batch");
+  cudaSetDevice(b->dev);
+  cudaStreamSynchronize(b->stream);
+  if (step_ms) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+    *step_ms = ms;
+  }
+  if (interactions) *interactions = b->interactions;
+  if (launches_per_step) *launches_per_step = b->launches;
+  return WINDS_BS_OK;
+}
+
+void winds_wake_destroy(winds_wake_batch *b) {
+  if (!b) return;
+  cudaSetDevice(b->dev);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  for (DevBuf *x : {&b->cases_d, &b->step_d, &b->dom, &b->dom_pred, &b->dom_new, &b->vel, &b->h1,
+                    &b->h2, &b->h3, &b->uind, &b->uind_pred, &b->bound, &b->trail_prev,
+                    &b->shed_cur, &b->trail_cur, &b->shed_next, &b->trail_next, &b->rc_s,
+                    &b->rc_t, &b->len_old_s, &b->len_old_t, &b->len_s, &b->len_t, &b->len_ps,
+                    &b->len_pt, &b->quarter, &b->trailing, &b->wind, &b->fa, &b->fb, &b->fc,
+                    &b->fd, &b->ra, &b->rb, &b->tp, &b->tp_raw, &b->tgroup, &b->keys, &b->vals,
+                    &b->perm, &b->sort_tmp, &b->groups_main, &b->groups_pred, &b->tiles,
+                    &b->items, &b->part, &b->bbox, &b->ctr, &b->err, &b->nearctr})
+    x->release();
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+}  // extern "C"

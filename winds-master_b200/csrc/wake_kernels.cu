@@ -1,0 +1,329 @@
+// wake_kernels.cu -- device kernels of the batched free-wake step (all cases in
+// one launch each; blockIdx.y is the case). HBM-bound O(nodes) work around the
+// direct sum:
+//   wake_bookkeep    Γ bookkeeping, WInDS.m:131-140 / numerical/pcc.m:43-49
+//   wake_filaments   FilamentLength + vcore + filamentmod + packing for the
+//                    direct sum (core/FilamentLength.m:27-44, core/vcore.m:30-51,
+//                    core/filamentmod.m:23-41)
+//   wake_targets     node positions -> direct-sum targets
+//   wake_convect     fe / ab2 / ab4 / pcc predictor and corrector
+//                    (numerical/fe.m:31, ab2.m:38-39, ab4.m:77-81, pcc.m:37-75)
+//   wake_commit      end of step: new positions, Γ and length history, counter
+#include "bs_device.cuh"
+#include "wake_launch.h"
+#include "wake_types.h"
+
+namespace winds {
+
+namespace {
+
+__device__ __forceinline__ double node_comp(const double *dom, const WakeCase &c, int i, int comp,
+                                            int j, int b) {
+  return dom[c.node_off * 3 + i + (long long)c.nst * (comp + 3 * (j + (long long)c.na * b))];
+}
+__device__ __forceinline__ long long node_idx(const WakeCase &c, int i, int comp, int j, int b) {
+  return c.node_off * 3 + i + (long long)c.nst * (comp + 3 * (j + (long long)c.na * b));
+}
+
+// Freestream at (x,y,z) for step s: wind(:,s) * ((H + z)/H)^shear.
+__device__ __forceinline__ void wind_at(const WakeCase &c, const double *wind, int s, double z,
+                                        double &wx, double &wy, double &wz) {
+  const double *w = wind + c.wind_off + 3 * (long long)s;
+  double f = 1.0;
+  if (c.shear != 0.0) f = pow(fmax(c.hub + z, 1e-3) / c.hub, c.shear);
+  wx = w[0] * f;
+  wy = w[1] * f;
+  wz = w[2] * f;
+}
+
+__device__ __forceinline__ double core_sq(const WakeCase &c, double gamma, double t) {
+  const double Re = fabs(gamma / c.nu);
+  if (c.core_mode == 0) return c.r0 * c.r0 + 4.0 * c.alpha * c.nu * (1.0 + c.a1 * Re) * t;
+  return c.rc0 * c.rc0 + 4.0 * c.alpha * c.delta * c.nu * (1.0 + c.a1 * Re) * t;
+}
+
+// trail(i, k, b) of the step being formed: column 0 from the bound circulation
+// (diff([0; G; 0])), column k >= 1 from the previous step's column k-1.
+__device__ __forceinline__ double trail_col(const WakeCase &c, const double *bound,
+                                            const double *trail_prev, int i, int k, int b) {
+  const int ns = c.nst - 1;
+  if (k == 0) {
+    const double *G = bound + c.bound_off + (long long)ns * b;
+    const double hi = i < ns ? G[i] : 0.0;
+    const double lo = i > 0 ? G[i - 1] : 0.0;
+    return hi - lo;
+  }
+  return trail_prev[c.trail_off + i + (long long)c.nst * ((k - 1) + (long long)(c.na - 1) * b)];
+}
+
+}  // namespace
+
+__global__ void wake_bookkeep(const WakeCase *cases, const double *bound, const double *trail_prev,
+                              double *shed, double *trail) {
+  const WakeCase c = cases[blockIdx.y];
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;  // (column j, blade b)
+  if (u >= c.na * c.nb) return;
+  const int j = u % c.na, b = u / c.na;
+  const int ns = c.nst - 1, m = c.na - 1;  // m trailing columns
+  if (j < m) {
+    for (int i = 0; i < c.nst; ++i)
+      trail[c.trail_off + i + (long long)c.nst * (j + (long long)m * b)] =
+          trail_col(c, bound, trail_prev, i, j, b);
+  }
+  // shed(:, 0) = G; shed(:, j) = C_j - C_{j-1}, C_k = cumsum over span of trail(1:end-1, k),
+  // C_m = 0 (WInDS.m:139-140)
+  double cj = 0.0, cjm1 = 0.0;
+  for (int i = 0; i < ns; ++i) {
+    double v;
+    if (j == 0) {
+      v = bound[c.bound_off + i + (long long)ns * b];
+    } else {
+      cjm1 += trail_col(c, bound, trail_prev, i, j - 1, b);
+      if (j < m) cj += trail_col(c, bound, trail_prev, i, j, b);
+      v = cj - cjm1;
+    }
+    shed[c.shed_off + i + (long long)ns * (j + (long long)c.na * b)] = v;
+  }
+}
+
+__global__ void wake_filaments(const WakeCase *cases, const int *step, int step_add,
+                               const double *dom, const double *shed, const double *trail,
+                               const double *len_old_s, const double *len_old_t, int have_old,
+                               int stretch, double *len_s, double *len_t, double *rc_s,
+                               double *rc_t, int model, double dcut, PackedFilaments pf,
+                               BBox *bb) {
+  const WakeCase c = cases[blockIdx.y];
+  const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+  const int ns = c.nst - 1;
+  const long long nsh = (long long)ns * c.na * c.nb;
+  if (f < c.fil_count) {
+    const int s = *step + step_add;
+    const double t_abs = c.t0 + s * c.dt;
+    int i, j, b, m;
+    double x1, y1, z1, x2, y2, z2, g, age;
+    long long slot;
+    const double *lold;
+    double *lnew, *rcout;
+    if (f < nsh) {  // shed: dom(i) -> dom(i+1) at column j
+      i = (int)(f % ns);
+      j = (int)((f / ns) % c.na);
+      b = (int)(f / ((long long)ns * c.na));
+      m = c.na;
+      x1 = node_comp(dom, c, i, 0, j, b), y1 = node_comp(dom, c, i, 1, j, b);
+      z1 = node_comp(dom, c, i, 2, j, b);
+      x2 = node_comp(dom, c, i + 1, 0, j, b), y2 = node_comp(dom, c, i + 1, 1, j, b);
+      z2 = node_comp(dom, c, i + 1, 2, j, b);
+      slot = c.shed_off + f;
+      g = shed[slot];
+      age = j * c.dt;
+      lold = len_old_s, lnew = len_s, rcout = rc_s;
+    } else {  // trailing: dom(:, j+1) -> dom(:, j)
+      const long long k = f - nsh;
+      i = (int)(k % c.nst);
+      j = (int)((k / c.nst) % (c.na - 1));
+      b = (int)(k / ((long long)c.nst * (c.na - 1)));
+      m = c.na - 1;
+      x1 = node_comp(dom, c, i, 0, j + 1, b), y1 = node_comp(dom, c, i, 1, j + 1, b);
+      z1 = node_comp(dom, c, i, 2, j + 1, b);
+      x2 = node_comp(dom, c, i, 0, j, b), y2 = node_comp(dom, c, i, 1, j, b);
+      z2 = node_comp(dom, c, i, 2, j, b);
+      slot = c.trail_off + k;
+      g = trail[slot];
+      age = (j + 0.5) * c.dt;
+      lold = len_old_t, lnew = len_t, rcout = rc_t;
+    }
+    const double dx = x2 - x1, dy = y2 - y1, dz = z2 - z1;
+    const double L = sqrt(dx * dx + dy * dy + dz * dz);  // |L| (FilamentLength.m:43)
+    double rc = core_sq(c, g, c.core_mode == 0 ? t_abs : age);
+    if (stretch && have_old && j >= 1 && j <= m - 2) {
+      // filamentmod.m:29-41: lengths square-rooted again, same column index
+      const double a = sqrt(L), o = sqrt(lold[slot]);
+      const double strain = (a - o) / o;
+      rc = rc * (1.0 / (1.0 + strain));
+    }
+    lnew[slot] = L;
+    if (rcout) rcout[slot] = rc;
+    pack_filament(c.fil_off + f, x1, y1, z1, x2, y2, z2, g, rc, model, dcut, pf.fa, pf.fb, pf.fc,
+                  pf.fd, pf.ra, pf.rb);
+    lo[0] = (float)fmin(x1, x2), lo[1] = (float)fmin(y1, y2), lo[2] = (float)fmin(z1, z2);
+    hi[0] = (float)fmax(x1, x2), hi[1] = (float)fmax(y1, y2), hi[2] = (float)fmax(z1, z2);
+  } else if (f < c.fil_pad) {
+    pack_inert(c.fil_off + f, pf.fa, pf.fb, pf.fc, pf.fd, pf.ra, pf.rb);
+  }
+  bbox_accumulate(lo, hi, bb->fmin, bb->fmax);
+}
+
+__global__ void wake_targets(const WakeCase *cases, const double *dom, double4 *tp, int *tgroup,
+                             BBox *bb) {
+  const WakeCase c = cases[blockIdx.y];
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n = (long long)c.nst * c.na * c.nb;
+  float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+  if (t < n) {
+    const long long jk = t / c.nst, i = t - jk * c.nst;
+    const long long base = c.node_off * 3 + i + c.nst * 3 * jk;
+    const double x = dom[base], y = dom[base + c.nst], z = dom[base + 2 * c.nst];
+    tp[c.node_off + t] = make_double4(x, y, z, 0.0);
+    tgroup[c.node_off + t] = (int)blockIdx.y;
+    lo[0] = hi[0] = (float)x;
+    lo[1] = hi[1] = (float)y;
+    lo[2] = hi[2] = (float)z;
+  }
+  bbox_accumulate(lo, hi, bb->tmin, bb->tmax);
+}
+
+// One thread per source node (i, j, b). Modes (WakeConvectMode): the node's
+// velocity wind + uind (+ carry) is stored in `vel`, and the node's convected
+// position is pushed to column j+1 of `out` (columns 0-1 of `out` come from
+// the kinematics of step s+1). The corrector reads the stored velocity and
+// the predicted positions/induction of column j+1.
+__global__ void wake_convect(const WakeCase *cases, const int *step, int mode, const double *dom,
+                             const double *uind, const double *carry, const double *pred,
+                             const double *uind_pred, double *vel, const double *h1,
+                             const double *h2, const double *h3, const double *quarter,
+                             const double *trailing, const double *wind, double *out) {
+  const WakeCase c = cases[blockIdx.y];
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n = (long long)c.nst * c.na * c.nb;
+  if (t >= n) return;
+  const int s = *step;
+  const int i = (int)(t % c.nst), j = (int)((t / c.nst) % c.na), b = (int)(t / ((long long)c.nst * c.na));
+  double v[3];
+  if (mode != kConvectCorrector) {
+    double w[3];
+    wind_at(c, wind, s, node_comp(dom, c, i, 2, j, b), w[0], w[1], w[2]);
+    for (int k = 0; k < 3; ++k) {
+      const long long q = node_idx(c, i, k, j, b);
+      v[k] = w[k] + uind[q] + (carry ? carry[q] : 0.0);
+      vel[q] = v[k];
+    }
+  } else {
+    for (int k = 0; k < 3; ++k) v[k] = vel[node_idx(c, i, k, j, b)];
+  }
+  if (j == 0) {  // columns 0-1 of the new domain: kinematics of step s+1
+    for (int k = 0; k < 3; ++k) {
+      const long long kq = c.kin_off + i + (long long)c.nst * (k + 3 * ((s + 1) + (long long)c.nsteps * b));
+      out[node_idx(c, i, k, 0, b)] = quarter[kq];
+      out[node_idx(c, i, k, 1, b)] = trailing[kq];
+    }
+    return;
+  }
+  if (j > c.na - 2) return;  // the oldest column leaves the truncated wake
+  const double dt = c.dt;
+  double x[3];
+  for (int k = 0; k < 3; ++k) x[k] = node_comp(dom, c, i, k, j, b);
+  if (mode == kConvectCorrector) {
+    double w[3];
+    wind_at(c, wind, s + 1, node_comp(pred, c, i, 2, j + 1, b), w[0], w[1], w[2]);
+    for (int k = 0; k < 3; ++k) {
+      const double v1 = w[k] + uind_pred[node_idx(c, i, k, j + 1, b)];
+      out[node_idx(c, i, k, j + 1, b)] = x[k] + dt / 2 * (v1 + v[k]);
+    }
+    return;
+  }
+  const int hist = s < 3 ? s : 3;  // velocities of earlier steps available
+  for (int k = 0; k < 3; ++k) {
+    double nx;
+    if (mode == kConvectAB2 && hist >= 1) {
+      const double p1 = j >= 2 ? h1[node_idx(c, i, k, j - 1, b)] : 0.0;
+      nx = x[k] + dt / 2 * (3.0 * v[k] - p1);
+    } else if (mode == kConvectAB4 && hist >= 3) {
+      const double p1 = j >= 2 ? h1[node_idx(c, i, k, j - 1, b)] : 0.0;
+      const double p2 = j >= 3 ? h2[node_idx(c, i, k, j - 2, b)] : 0.0;
+      const double p3 = j >= 4 ? h3[node_idx(c, i, k, j - 3, b)] : 0.0;
+      nx = x[k] + dt / 24 * (55.0 * v[k] - 59.0 * p1 + 37.0 * p2 - 9.0 * p3);
+    } else {  // forward Euler (also the pcc predictor)
+      nx = x[k] + dt * v[k];
+    }
+    out[node_idx(c, i, k, j + 1, b)] = nx;
+  }
+}
+
+// End of step: positions, velocity history, previous trailing Γ and lengths.
+__global__ void wake_commit(const WakeCase *cases, int *step, double *dom, const double *dom_new,
+                            double *vel, double *h1, double *h2, double *h3, int keep_hist,
+                            double *trail_prev, const double *trail_cur, double *len_old_s,
+                            const double *len_s, double *len_old_t, const double *len_t) {
+  const WakeCase c = cases[blockIdx.y];
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nn = (long long)c.nst * c.na * c.nb;
+  const long long nsh = (long long)(c.nst - 1) * c.na * c.nb;
+  const long long ntr = (long long)c.nst * (c.na - 1) * c.nb;
+  if (t < nn) {
+    for (int k = 0; k < 3; ++k) {
+      const long long q = c.node_off * 3 + k * nn + t;  // any bijection of the case's slice
+      dom[q] = dom_new[q];
+      if (keep_hist) {
+        h3[q] = h2[q];
+        h2[q] = h1[q];
+        h1[q] = vel[q];
+      }
+    }
+  }
+  if (t < nsh) len_old_s[c.shed_off + t] = len_s[c.shed_off + t];
+  if (t < ntr) {
+    trail_prev[c.trail_off + t] = trail_cur[c.trail_off + t];
+    len_old_t[c.trail_off + t] = len_t[c.trail_off + t];
+  }
+  // every kernel of this step that reads the counter ran before this one
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) step[0] += 1;
+}
+
+// ------------------------------------------------------------ launchers
+static dim3 case_grid(long long max_per_case, int ncases, int bs) {
+  return dim3((unsigned)((max_per_case + bs - 1) / bs), (unsigned)ncases);
+}
+
+cudaError_t launch_wake_bookkeep(const WakeCase *cases, int ncases, long long max_cols,
+                                 const double *bound, const double *trail_prev, double *shed,
+                                 double *trail, cudaStream_t s) {
+  wake_bookkeep<<<case_grid(max_cols, ncases, 128), 128, 0, s>>>(cases, bound, trail_prev, shed,
+                                                                  trail);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wake_filaments(const WakeCase *cases, int ncases, long long max_fil_pad,
+                                  const int *step, int step_add, const double *dom,
+                                  const double *shed, const double *trail,
+                                  const double *len_old_s, const double *len_old_t, int have_old,
+                                  int stretch, double *len_s, double *len_t, double *rc_s,
+                                  double *rc_t, int model, double dcut,
+                                  const PackedFilaments &pf, BBox *bb, cudaStream_t s) {
+  wake_filaments<<<case_grid(max_fil_pad, ncases, 256), 256, 0, s>>>(
+      cases, step, step_add, dom, shed, trail, len_old_s, len_old_t, have_old, stretch, len_s,
+      len_t, rc_s, rc_t, model, dcut, pf, bb);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wake_targets(const WakeCase *cases, int ncases, long long max_nodes,
+                                const double *dom, double4 *tp, int *tgroup, BBox *bb,
+                                cudaStream_t s) {
+  wake_targets<<<case_grid(max_nodes, ncases, 256), 256, 0, s>>>(cases, dom, tp, tgroup, bb);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wake_convect(const WakeCase *cases, int ncases, long long max_nodes,
+                                const int *step, int mode, const double *dom, const double *uind,
+                                const double *carry, const double *pred, const double *uind_pred,
+                                double *vel, const double *h1, const double *h2, const double *h3,
+                                const double *quarter, const double *trailing, const double *wind,
+                                double *out, cudaStream_t s) {
+  wake_convect<<<case_grid(max_nodes, ncases, 256), 256, 0, s>>>(
+      cases, step, mode, dom, uind, carry, pred, uind_pred, vel, h1, h2, h3, quarter, trailing,
+      wind, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wake_commit(const WakeCase *cases, int ncases, long long max_slots, int *step,
+                               double *dom, const double *dom_new, double *vel, double *h1,
+                               double *h2, double *h3, int keep_hist, double *trail_prev,
+                               const double *trail_cur, double *len_old_s, const double *len_s,
+                               double *len_old_t, const double *len_t, cudaStream_t s) {
+  wake_commit<<<case_grid(max_slots, ncases, 256), 256, 0, s>>>(
+      cases, step, dom, dom_new, vel, h1, h2, h3, keep_hist, trail_prev, trail_cur, len_old_s,
+      len_s, len_old_t, len_t);
+  return cudaGetLastError();
+}
+
+}  // namespace winds

@@ -222,3 +222,98 @@ def near_singular_targets(x1, x2, rc_sq, n, rng, frac_rc=0.5):
     perp /= np.maximum(np.linalg.norm(perp, axis=1, keepdims=True), 1e-300)
     dist = rng.uniform(0.05, frac_rc, size=n)[:, None] * np.sqrt(rc_sq[idx])[:, None]
     return base + dist * perp
+
+
+# ----------------------------------------------------------------- time stepping
+def blade_geometry(case: RotorCase):
+    """Cosine-spaced node radii, linear chord 3.5 -> 1.4 m and twist 13 -> 0 deg
+    from root to tip (the synthetic blade of the configurations)."""
+    r = cosine_nodes(case.r_root, case.R, case.nst)
+    s = (r - case.r_root) / (case.R - case.r_root)
+    chord = 3.5 + (1.4 - 3.5) * s
+    twist = np.radians(13.0 * (1.0 - s))
+    return r, chord, twist
+
+
+def blade_nodes(case: RotorCase, t: float, pitch_deg: float = 0.0):
+    """Quarter-chord and trailing-edge nodes ``[nst, 3, nb]`` at time ``t``
+    (rigid rotor turning at ``case.omega`` about the x axis, yawed about z)."""
+    r, chord, twist = blade_geometry(case)
+    psi = 2.0 * np.pi * np.arange(case.nb) / case.nb + case.omega * t      # [nb]
+    cp, sp = np.cos(psi)[None, :], np.sin(psi)[None, :]
+    rr = r[:, None]
+    # rotor frame: x axial (downwind), y/z in the plane; tangential t = d/dpsi
+    q = np.stack([np.zeros_like(rr * cp), rr * cp, rr * sp], axis=1)       # [nst,3,nb]
+    tang = np.stack([np.zeros_like(cp + 0 * rr), -sp + 0 * rr, cp + 0 * rr], axis=1)
+    th = (twist + np.radians(pitch_deg))[:, None]
+    d = -np.cos(th)[:, None, :] * tang
+    d[:, 0, :] += np.sin(th)
+    te = q + 0.75 * chord[:, None, None] * d
+    yaw = np.radians(case.yaw_deg)
+
+    def rot(v):
+        x, y, z = v[:, 0], v[:, 1], v[:, 2]
+        return np.stack([x * np.cos(yaw) - y * np.sin(yaw), x * np.sin(yaw) + y * np.cos(yaw), z], axis=1)
+
+    return rot(q), rot(te)
+
+
+def make_wake_case(case: RotorCase, nsteps: int, t0: float = 0.0, jitter: float = 0.0,
+                   a1: float = 0.0) -> dict:
+    """Initial state, kinematics and wind of one rotor for the device time step.
+
+    The wake keeps ``na = case.nsteps + 1`` age columns: column 0 the
+    quarter-chord nodes, column 1 the trailing-edge nodes at ``t0``, column
+    ``j >= 2`` the trailing-edge node of ``j - 1`` steps earlier convected by
+    the freestream. Γ history as in :func:`make_wake`; core model: age form
+    with the configurations' rc0, delta, nu."""
+    rng = np.random.Generator(np.random.PCG64(case.seed))
+    nst, nb, na, ns, dt = case.nst, case.nb, case.na, case.ns, case.dt
+    quarter = np.zeros((nst, 3, nsteps, nb))
+    trailing = np.zeros((nst, 3, nsteps, nb))
+    for s in range(nsteps):
+        quarter[:, :, s, :], trailing[:, :, s, :] = blade_nodes(case, t0 + s * dt)
+    dom = np.zeros((nst, 3, na, nb))
+    q0, te0 = blade_nodes(case, t0)
+    dom[:, :, 0, :], dom[:, :, 1, :] = q0, te0
+    for j in range(2, na):
+        age = (j - 1) * dt
+        _, te = blade_nodes(case, t0 - age)
+        height = case.hub_height + te[:, 2, :]
+        speed = case.U * np.power(np.maximum(height, 1.0) / case.hub_height, case.shear)
+        te[:, 0, :] += speed * age
+        dom[:, :, j, :] = te
+    if jitter > 0:
+        dom[:, :, 2:, :] += rng.normal(0.0, jitter, size=dom[:, :, 2:, :].shape)
+    r = cosine_nodes(case.r_root, case.R, nst)
+    r_mid = 0.5 * (r[1:] + r[:-1])
+    G = elliptic_bound(case, r_mid)[:, None, None] * (
+        1.0 + case.gamma_noise * rng.standard_normal((ns, na, nb)))
+    trail = trail_from_bound(G[:, : na - 1, :])          # [nst, na-1, nb]
+    wind = np.zeros((3, nsteps))
+    wind[0, :] = case.U
+    f = np.asfortranarray
+    return dict(nst=nst, nb=nb, na=na, nsteps=nsteps, dt=dt, t0=t0,
+                quarter=f(quarter), trailing=f(trailing), wind=f(wind), shear=case.shear,
+                hub_height=case.hub_height, core_mode=1, r0=case.rc0, rc0=case.rc0,
+                alpha=ALPHA_RL, nu=case.nu, a1=a1, delta=case.delta,
+                dom=f(dom), bound=f(G[:, 0, :]), trail_gamma=f(trail))
+
+
+def batch_cases(n: int, seed: int = 0, steps_range=(60, 720), nodes_range=(17, 41),
+                U_range=(5.0, 25.0), tsr_range=(4.0, 10.0), yaw_range=(0.0, 30.0),
+                shear_range=(0.0, 0.3), dpsi_deg: float = 10.0):
+    """``n`` uneven rotor cases drawn uniformly from the seed: wake steps,
+    span nodes, wind speed, tip-speed ratio, yaw and shear exponent."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for k in range(n):
+        U = float(rng.uniform(*U_range))
+        tsr = float(rng.uniform(*tsr_range))
+        omega = tsr * U / 63.0
+        out.append(RotorCase(nst=int(rng.integers(nodes_range[0], nodes_range[1] + 1)),
+                             nsteps=int(rng.integers(steps_range[0], steps_range[1] + 1)),
+                             dpsi_deg=dpsi_deg, omega_rpm=omega * 60 / (2 * np.pi), U=U,
+                             yaw_deg=float(rng.uniform(*yaw_range)),
+                             shear=float(rng.uniform(*shear_range)), seed=seed * 1000 + k))
+    return out

@@ -1,0 +1,109 @@
+"""ctypes binding of ``include/winds_wake.h``: the device-resident free-wake
+time step of many rotor cases at once (the WInDS main loop's induced
+velocity, bookkeeping, core growth and convection: ``WInDS.m:127-179``).
+
+``WakeBatch(cases, ...)`` takes case dicts as :func:`synth.make_wake_case`
+returns them (WInDS-layout arrays), ``step(n, graph=True)`` advances every
+case, ``state(i)`` reads one case back.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from .bs import _check, lib, parse_core
+
+INTEG = {"fe": 0, "ab2": 1, "ab4": 2, "pcc": 3}
+
+
+class WakeCaseC(C.Structure):
+    _fields_ = [("nst", C.c_int), ("nb", C.c_int), ("na", C.c_int), ("nsteps", C.c_int),
+                ("dt", C.c_double), ("t0", C.c_double),
+                ("quarter", C.c_void_p), ("trailing", C.c_void_p), ("wind", C.c_void_p),
+                ("shear", C.c_double), ("hub_height", C.c_double), ("core_mode", C.c_int),
+                ("r0", C.c_double), ("rc0", C.c_double), ("alpha", C.c_double), ("nu", C.c_double),
+                ("a1", C.c_double), ("delta", C.c_double),
+                ("dom", C.c_void_p), ("bound", C.c_void_p), ("trail_gamma", C.c_void_p)]
+
+
+class WakeParamsC(C.Structure):
+    _fields_ = [("integrator", C.c_int), ("core_model", C.c_int), ("d", C.c_double),
+                ("co", C.c_double), ("precision", C.c_int), ("pcc_double_add", C.c_int),
+                ("stretch", C.c_int)]
+
+
+def _bind():
+    L = lib()
+    if not hasattr(L, "_wake_bound"):
+        L.winds_wake_create.argtypes = [C.POINTER(WakeCaseC), C.c_int, C.POINTER(WakeParamsC),
+                                        C.POINTER(C.c_void_p)]
+        L.winds_wake_step.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        L.winds_wake_get_state.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 7
+        L.winds_wake_set_bound.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        L.winds_wake_stats.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_longlong),
+                                       C.POINTER(C.c_int)]
+        L.winds_wake_destroy.argtypes = [C.c_void_p]
+        L._wake_bound = True
+    return L
+
+
+class WakeBatch:
+    def __init__(self, cases, integrator="pcc", d="visc2", co=1000.0, precision="f32c",
+                 pcc_double_add=True, stretch=True):
+        L = _bind()
+        self._keep = []
+        arr = (WakeCaseC * len(cases))()
+        for k, c in enumerate(cases):
+            a = arr[k]
+            for f in ("nst", "nb", "na", "nsteps", "core_mode"):
+                setattr(a, f, int(c[f]))
+            for f in ("dt", "t0", "shear", "hub_height", "r0", "rc0", "alpha", "nu", "a1", "delta"):
+                setattr(a, f, float(c[f]))
+            for f in ("quarter", "trailing", "wind", "dom", "bound", "trail_gamma"):
+                x = np.asfortranarray(c[f], dtype=np.float64)
+                self._keep.append(x)
+                setattr(a, f, x.ctypes.data)
+        core, dv = parse_core(d)
+        p = WakeParamsC(INTEG[integrator], core, dv, float(co),
+                        {"f32c": 0, "f64": 1}[precision], int(pcc_double_add), int(stretch))
+        h = C.c_void_p()
+        _check(L.winds_wake_create(arr, len(cases), C.byref(p), C.byref(h)))
+        self.h = h
+        self.cases = [dict(nst=c["nst"], nb=c["nb"], na=c["na"]) for c in cases]
+
+    def step(self, n=1, graph=False):
+        _check(_bind().winds_wake_step(self.h, int(n), 1 if graph else 0))
+
+    def state(self, i):
+        c = self.cases[i]
+        nst, nb, na = c["nst"], c["nb"], c["na"]
+        ns = nst - 1
+        out = dict(dom=np.zeros((nst, 3, na, nb), order="F"), bound=np.zeros((ns, nb), order="F"),
+                   shed=np.zeros((ns, na, nb), order="F"), trail=np.zeros((nst, na - 1, nb), order="F"),
+                   rc_shed=np.zeros((ns, na, nb), order="F"),
+                   rc_trail=np.zeros((nst, na - 1, nb), order="F"),
+                   uind=np.zeros((nst, 3, na, nb), order="F"))
+        ks = ("dom", "bound", "shed", "trail", "rc_shed", "rc_trail", "uind")
+        _check(_bind().winds_wake_get_state(self.h, i, *[out[k].ctypes.data for k in ks]))
+        return out
+
+    def set_bound(self, i, bound):
+        b = np.asfortranarray(bound, dtype=np.float64)
+        _check(_bind().winds_wake_set_bound(self.h, i, b.ctypes.data))
+
+    def stats(self):
+        ms, n, l = C.c_double(), C.c_longlong(), C.c_int()
+        _check(_bind().winds_wake_stats(self.h, C.byref(ms), C.byref(n), C.byref(l)))
+        return ms.value, n.value, l.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            _bind().winds_wake_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
