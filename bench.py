@@ -48,6 +48,8 @@ def parse():
                     help="large: 3x41x720 (the metric's case); medium: 3x41x180 for profiling")
     ap.add_argument("--tiling", default=None,
                     help="force the FP32 tiling 'T,KF,waves' instead of the autotuner's choice")
+    ap.add_argument("--wake-steps", type=int, default=3,
+                    help="timed pcc steps of the 64-case batched wake (0: skip)")
     ap.add_argument("--quick", action="store_true",
                     help="timed loop only (no FP64 comparison, e2e or CPU baseline)")
     return ap.parse_args()
@@ -177,6 +179,39 @@ def reference_arm(args):
                 "the Vatistas workload runs on the FP64 C restatement of core/BiotSavart.m",
     }
     print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ batched wake
+def wake_bench(args, seed=2, ncases=64):
+    """64 uneven rotor cases (wake steps 60-720, span nodes 17-41, U 5-25 m/s,
+    TSR 4-10, yaw 0-30 deg, shear 0-0.3), pcc predictor-corrector step: the
+    FP32-compensated batched engine replaying one CUDA graph per step, against
+    the plain FP64 path (each case on its own, eager, FP64 direct sum)."""
+    synth = importlib.import_module("winds-master_b200.synth")
+    wake = importlib.import_module("winds-master_b200.wake")
+    rcases = synth.batch_cases(ncases, seed=seed)
+    warm = 1
+    cases = [synth.make_wake_case(rc, nsteps=warm + args.wake_steps + 3, jitter=0.05)
+             for rc in rcases]
+    b = wake.WakeBatch(cases, integrator="pcc", precision="f32c")
+    b.step(warm, graph=True)
+    b.step(args.wake_steps, graph=True)
+    ms, inter, launches = b.stats()
+    b.close()
+    plain_ms = 0.0
+    for c in cases:
+        p = wake.WakeBatch([c], integrator="pcc", precision="f64")
+        p.step(1)
+        p.step(1)
+        plain_ms += p.stats()[0]
+        p.close()
+    return {"cases": ncases, "integrator": "pcc", "graph": True,
+            "steps_per_s": 1000.0 / ms, "ms_per_step": ms,
+            "interactions_per_step": inter, "gint_per_s": inter / (ms * 1e-3) / 1e9,
+            "launches_per_step": launches,
+            "plain_fp64_steps_per_s": 1000.0 / plain_ms,
+            "speedup_vs_plain_fp64": plain_ms / ms,
+            "nodes": int(sum(c["nst"] * c["na"] * c["nb"] for c in cases))}
 
 
 # ------------------------------------------------------------------ our arm
@@ -313,6 +348,9 @@ def ours(args):
         cpu = {"value": rate, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                "sample": f"{n} sampled targets x {nf} filaments ({dt:.1f} s), FP64 C restatement "
                          "of core/BiotSavart.m, OpenMP"}
+    wake_line = None
+    if rank == 0 and args.wake_steps > 0 and not args.quick:
+        wake_line = wake_bench(args)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -340,6 +378,7 @@ def ours(args):
             "near_pairs_per_step": near_pairs,
             "tiling": dict(zip(("targets_per_thread", "filaments_per_tile", "waves"),
                                wb.get_tuning(core, nt, nf))),
+            "wake_batch": wake_line,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

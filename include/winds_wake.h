@@ -91,9 +91,9 @@ int winds_wake_get_state(winds_wake_batch *b, int icase, double *dom, double *bo
  * iteration); it enters at the next step's bookkeeping. */
 int winds_wake_set_bound(winds_wake_batch *b, int icase, const double *bound);
 
-/* Device time of the last step (ms, CUDA events around the whole step),
- * interactions per step over all cases and evaluations, and the number of
- * kernels one step launches. */
+/* Mean device time per step of the last winds_wake_step call (ms, CUDA
+ * events around its steps), interactions per step over all cases and
+ * evaluations, and the number of kernels one step launches. */
 int winds_wake_stats(winds_wake_batch *b, double *step_ms, long long *interactions,
                      int *launches_per_step);
 

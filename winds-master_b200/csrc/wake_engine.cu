@@ -51,6 +51,7 @@ struct winds_wake_batch {
   TuneChoice ch;
   long long steps_done = 0;
   long long min_nsteps = 0;  // kinematics rows available in every case
+  int timed_steps = 0;       // steps between ev0 and ev1
 };
 
 namespace {
@@ -434,29 +435,29 @@ int winds_wake_step(winds_wake_batch *b, int nsteps, int use_graph) {
                 b->min_nsteps - 1, b->steps_done, nsteps);
   cudaSetDevice(b->dev);
   cudaError_t e = cudaSuccess;
+  if (use_graph && !b->exec && nsteps > 0) {
+    // capture one step (launches nothing) before the timed steps
+    e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+    int l = 0;
+    cudaError_t e2 = e == cudaSuccess ? enqueue_step(b, l) : e;
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(b->stream, &g);
+    if (e2 != cudaSuccess) e = e2;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, g, 0);
+    b->graph = g;
+    b->launches = l;
+    if (e != cudaSuccess) return cuda_fail(e, "wake step capture");
+  }
+  b->timed_steps = nsteps;
+  if (nsteps > 0) cudaEventRecord(b->ev0, b->stream);
   for (int k = 0; k < nsteps && e == cudaSuccess; ++k) {
     if (use_graph) {
-      if (!b->exec) {
-        e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
-        int l = 0;
-        cudaError_t e2 = e == cudaSuccess ? enqueue_step(b, l) : e;
-        cudaGraph_t g = nullptr;
-        e = cudaStreamEndCapture(b->stream, &g);
-        if (e2 != cudaSuccess) e = e2;
-        if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, g, 0);
-        b->graph = g;
-        b->launches = l;
-        if (e != cudaSuccess) break;
-      }
-      cudaEventRecord(b->ev0, b->stream);
       e = cudaGraphLaunch(b->exec, b->stream);
-      cudaEventRecord(b->ev1, b->stream);
     } else {
-      cudaEventRecord(b->ev0, b->stream);
       e = enqueue_step(b, b->launches);
-      cudaEventRecord(b->ev1, b->stream);
     }
   }
+  if (nsteps > 0) cudaEventRecord(b->ev1, b->stream);
   if (e != cudaSuccess) return cuda_fail(e, "wake step");
   b->steps_done += nsteps;
   e = cudaStreamSynchronize(b->stream);
@@ -512,8 +513,8 @@ int winds_wake_stats(winds_wake_batch *b, double *step_ms, long long *interactio
   cudaStreamSynchronize(b->stream);
   if (step_ms) {
     float ms = 0.f;
-    cudaEventElapsedTime(&ms, b->ev0, b->ev1);
-    *step_ms = ms;
+    if (b->timed_steps > 0) cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+    *step_ms = b->timed_steps > 0 ? ms / b->timed_steps : 0.0;
   }
   if (interactions) *interactions = b->interactions;
   if (launches_per_step) *launches_per_step = b->launches;

@@ -302,18 +302,21 @@ def make_wake_case(case: RotorCase, nsteps: int, t0: float = 0.0, jitter: float 
 
 def batch_cases(n: int, seed: int = 0, steps_range=(60, 720), nodes_range=(17, 41),
                 U_range=(5.0, 25.0), tsr_range=(4.0, 10.0), yaw_range=(0.0, 30.0),
-                shear_range=(0.0, 0.3), dpsi_deg: float = 10.0):
+                shear_range=(0.0, 0.3), dpsi_deg=None):
     """``n`` uneven rotor cases drawn uniformly from the seed: wake steps,
-    span nodes, wind speed, tip-speed ratio, yaw and shear exponent."""
+    span nodes, wind speed, tip-speed ratio, yaw and shear exponent. Without
+    ``dpsi_deg`` every wake spans two revolutions (azimuth step 720/steps deg)."""
     rng = np.random.Generator(np.random.PCG64(seed))
     out = []
     for k in range(n):
         U = float(rng.uniform(*U_range))
         tsr = float(rng.uniform(*tsr_range))
         omega = tsr * U / 63.0
-        out.append(RotorCase(nst=int(rng.integers(nodes_range[0], nodes_range[1] + 1)),
-                             nsteps=int(rng.integers(steps_range[0], steps_range[1] + 1)),
-                             dpsi_deg=dpsi_deg, omega_rpm=omega * 60 / (2 * np.pi), U=U,
+        nst = int(rng.integers(nodes_range[0], nodes_range[1] + 1))
+        steps = int(rng.integers(steps_range[0], steps_range[1] + 1))
+        out.append(RotorCase(nst=nst, nsteps=steps,
+                             dpsi_deg=dpsi_deg if dpsi_deg else 720.0 / steps,
+                             omega_rpm=omega * 60 / (2 * np.pi), U=U,
                              yaw_deg=float(rng.uniform(*yaw_range)),
                              shear=float(rng.uniform(*shear_range)), seed=seed * 1000 + k))
     return out
