@@ -37,6 +37,7 @@ extern "C" {
 #define WINDS_BS_ERR_TIMEOUT 3  /* a bounded device wait ran out; context stays usable */
 #define WINDS_BS_ERR_NOMEM 4    /* device or pinned allocation failed */
 #define WINDS_BS_ERR_NODEV 5    /* no CUDA device, or the library was built without one */
+#define WINDS_BS_ERR_DIVERGED 6 /* Kutta-Joukowski: Cl is NaN (KuttaJoukowski.m:272-274) */
 
 /* Core models of core/BiotSavart.m:102-109. */
 #define WINDS_CORE_CUTOFF 0   /* ubar = G/4pi (r1+r2)/(r1r2(r1r2+r1.r2) + d|L|^2)      (:108) */

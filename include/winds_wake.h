@@ -97,6 +97,46 @@ int winds_wake_set_bound(winds_wake_batch *b, int icase, const double *bound);
 int winds_wake_stats(winds_wake_batch *b, double *step_ms, long long *interactions,
                      int *launches_per_step);
 
+/* ----------------------------------------------- Kutta-Joukowski (optional)
+ * With a lifting line set, every step runs the fixed-point iteration of
+ * core/KuttaJoukowski.m:42-49 after the convection (as WInDS.m:182 does after
+ * pcc): each iteration evaluates every case's shed and trailing filaments at
+ * its lifting-line points (kj(), :215-227) with the step's cores, transforms
+ * to the blade frame, interpolates the airfoil tables and relaxes the bound
+ * circulation; a case stops when max |dg/(|Γ|+1)| <= tol or after maxiter. */
+typedef struct {
+  const double *ll;        /* [ns,3,nsteps,nb] lifting-line points (pos.bound)          */
+  const double *bxn;       /* [ns,3,nsteps,nb] blade-frame unit vectors (pos.nodes.bxn) */
+  const double *byn;       /* [ns,3,nsteps,nb]                                         */
+  const double *bzn;       /* [ns,3,nsteps,nb]                                         */
+  const double *vblade;    /* [ns,3,nsteps,nb] blade-frame velocity (vel.blade)         */
+  const double *chord;     /* [ns]                                                     */
+  const int *foil;         /* [ns] airfoil table of each station (0-based, blade.NFoil) */
+  int n_foils;
+  const int *foil_points;  /* [n_foils] entries of each table                          */
+  const double *aoa;       /* concatenated tables: AoA (deg, ascending), Cl, Cd        */
+  const double *cl;
+  const double *cd;
+} winds_kj_case;
+
+typedef struct {
+  double relax;  /* fixed-point relaxation (user.relax) */
+  double tol;    /* convergence tolerance (user.tol)   */
+  int maxiter;   /* iteration cap (user.maxiter)       */
+} winds_kj_params;
+
+/* Attaches one lifting line per case (host arrays copied) and enables the
+ * iteration in every later winds_wake_step. */
+int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_kj_params *prm);
+
+/* Iterations and final residual of each case in the last step, and the number
+ * of lifting-line induced-velocity evaluations that step ran. */
+int winds_wake_kj_stats(winds_wake_batch *b, int *iterations, double *residual,
+                        long long *ll_evaluations);
+
+/* Cl, Cd and AoA [ns,nb] of one case from the last iteration of the last step. */
+int winds_wake_get_perf(winds_wake_batch *b, int icase, double *cl, double *cd, double *aoa);
+
 void winds_wake_destroy(winds_wake_batch *b);
 
 #ifdef __cplusplus

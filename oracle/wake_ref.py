@@ -158,6 +158,10 @@ class WakeRef:
         w = wind_at(self.c, s, self._nodes(dom))
         return np.moveaxis(w, -1, 1)
 
+    def _before_commit(self, s):
+        """Runs after the convection of step ``s``, with the step's positions,
+        Γ and cores still current (the Kutta-Joukowski solve: WInDS.m:182)."""
+
     def step(self):
         """One time step p -> p+1; returns the induced velocity at p."""
         c, s = self.c, self.step_idx
@@ -202,6 +206,7 @@ class WakeRef:
         else:
             raise ValueError(self.integ)
         self.vel_hist = [vel] + self.vel_hist[:2]
+        self._before_commit(s)
         self.dom = np.asfortranarray(new)
         self.trail_prev = self.trail
         self.step_idx += 1

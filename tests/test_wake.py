@@ -72,3 +72,33 @@ def test_core_growth_formula(synth, wake_ref):
     c.core_mode = 0
     np.testing.assert_allclose(wake_ref.core(c, g, 1.5),
                                c.r0 ** 2 + 4 * c.alpha * c.nu * (1 + c.a1 * np.abs(g) / c.nu) * 1.5)
+
+
+def test_kj_oracle_interp1_is_nan_outside():
+    import kj_ref
+    x = np.array([-2.0, 0.0, 3.0])
+    y = np.array([1.0, 2.0, 5.0])
+    out = kj_ref.interp1(x, y, np.array([-3.0, -1.0, 1.5, 3.0, 4.0, np.nan]))
+    assert np.isnan(out[0]) and np.isnan(out[4]) and np.isnan(out[5])
+    np.testing.assert_allclose(out[1:4], [1.5, 3.5, 5.0])
+
+
+def test_kj_oracle_fixed_point(synth):
+    """The fixed point contracts and leaves the shed column equal to the
+    converged bound circulation (core/KuttaJoukowski.m:42-49, kj() :277-290)."""
+    import kj_ref
+    import wake_ref
+    r = synth.RotorCase(nst=7, nsteps=8, dpsi_deg=10.0, seed=5, jitter=0.0)
+    c = synth.make_wake_case(r, nsteps=6)
+    kj = synth.make_kj_case(r, nsteps=c["nsteps"], t0=c["t0"])
+    ref = kj_ref.KJWakeRef(wake_ref.WakeCaseRef(**{k: c[k] for k in wake_ref.WakeCaseRef.__dataclass_fields__}),
+                           kj, relax=0.3, tol=1e-5, maxiter=60)
+    ref.step()
+    assert ref.kj_iters < 60 and ref.kj_res <= 1e-5
+    np.testing.assert_array_equal(ref.shed[:, 0], ref.bound)
+    np.testing.assert_allclose(ref.trail[:, 0].sum(0), 0.0, atol=1e-12)
+    # a table too narrow for the flow's angle of attack diverges
+    bad = dict(kj, aoa=np.array([-0.5, 0.5]), cl=np.array([0.0, 0.1]), cd=np.array([0.01, 0.01]),
+               foil_points=np.array([2], dtype=np.int32))
+    with pytest.raises(kj_ref.KJDiverged):
+        kj_ref.kj_solve(bad, 0, c["dom"], ref.trail_prev, ref.rcs, ref.rct, ref.bound)

@@ -24,7 +24,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libwinds_bs.so")
 
 WINDS_BS_OK = 0
-ERR_NAMES = {1: "ARG", 2: "CUDA", 3: "TIMEOUT", 4: "NOMEM", 5: "NODEV"}
+ERR_NAMES = {1: "ARG", 2: "CUDA", 3: "TIMEOUT", 4: "NOMEM", 5: "NODEV", 6: "DIVERGED"}
 CORE_CUTOFF, CORE_VATISTAS = 0, 1
 PREC_F32C, PREC_F64 = 0, 1
 FLAG_SEQUENTIAL = 1

@@ -1,0 +1,34 @@
+// kj_launch.h -- per-case table and launchers of the Kutta-Joukowski kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "bs_types.h"
+#include "wake_types.h"
+
+namespace winds {
+
+struct KJCase {
+  long long frame_off;    // ns*3*nsteps*nb per case: ll, bxn, byn, bzn, vblade
+  long long t_off;        // first lifting-line target (ns*nb per case)
+  long long station_off;  // first station (ns per case): chord, foil
+  int foil_base;          // this case's first entry in the foil offset table
+  int n_foils;
+};
+
+cudaError_t launch_kj_targets(const WakeCase *cases, const KJCase *kc, int ncases, int max_st,
+                              const int *step, const double *ll, double4 *tp, BBox *bb,
+                              cudaStream_t s);
+cudaError_t launch_kj_update(const WakeCase *cases, const KJCase *kc, int ncases, int max_st,
+                             const int *step, const double *uindb, const double *bxn,
+                             const double *byn, const double *bzn, const double *vblade,
+                             const double *chord, const int *foil, const int *foil_off,
+                             const double *aoa_t, const double *cl_t, const double *cd_t,
+                             double relax, double *bound, const int *converged,
+                             unsigned long long *res_max, int *diverged, double *cl_out,
+                             double *cd_out, double *aoa_out, cudaStream_t s);
+cudaError_t launch_kj_check(int ncases, double tol, int *converged, int *iters,
+                            unsigned long long *res_max, double *res_last, int *active,
+                            cudaStream_t s);
+
+}  // namespace winds

@@ -17,6 +17,7 @@
 
 #include "bs_launch.h"
 #include "engine.h"
+#include "kj_launch.h"
 #include "wake_launch.h"
 #include "winds_wake.h"
 
@@ -52,6 +53,19 @@ struct winds_wake_batch {
   long long steps_done = 0;
   long long min_nsteps = 0;  // kinematics rows available in every case
   int timed_steps = 0;       // steps between ev0 and ev1
+  // Kutta-Joukowski lifting lines
+  bool kj = false;
+  winds_kj_params kjp{};
+  std::vector<KJCase> kjc;
+  long long n_ll = 0, frames_n = 0, stations_n = 0;
+  int max_st = 0;
+  DevBuf kjc_d, ll, bxn, byn, bzn, vblade, chord, foil, foil_off, aoa_t, cl_t, cd_t;
+  DevBuf tp_ll, perm_ll, uindb, kj_groups, kj_tiles, kj_items, kj_part;
+  DevBuf conv, iters, res_max, res_last, active, diverged, cl_o, cd_o, aoa_o;
+  int kj_ntiles = 0, kj_nitems = 0, kj_grid = 0, kj_tile_cap = 0, kj_T = 2, kj_KF = 64;
+  long long kj_evals = 0;
+  cudaGraphExec_t exec_pre = nullptr, exec_kj = nullptr, exec_post = nullptr;
+  cudaGraph_t g_pre = nullptr, g_kj = nullptr, g_post = nullptr;
 };
 
 namespace {
@@ -168,7 +182,7 @@ cudaError_t enqueue_eval(winds_wake_batch *b, const double *dom, const double *s
   if (e == cudaSuccess)
     e = launch_wake_filaments(cd, b->ncases, b->max_fil, P<const int>(b->step_d), step_add, dom,
                               shed, trail, lold_s, lold_t, have_old, b->prm.stretch, lnew_s, lnew_t,
-                              rc_s, rc_t, b->model, b->dcut, pf, bb, s);
+                              rc_s, rc_t, nullptr, nullptr, b->model, b->dcut, pf, bb, s);
   if (e == cudaSuccess)
     e = launch_wake_targets(cd, b->ncases, b->max_nodes, dom, P<double4>(b->tp_raw),
                             P<int>(b->tgroup), bb, s);
@@ -216,7 +230,7 @@ cudaError_t enqueue_eval(winds_wake_batch *b, const double *dom, const double *s
   return e;
 }
 
-cudaError_t enqueue_step(winds_wake_batch *b, int &launches) {
+cudaError_t enqueue_pre(winds_wake_batch *b, int &launches) {
   cudaStream_t s = b->stream;
   const WakeCase *cd = P<const WakeCase>(b->cases_d);
   const int *step = P<const int>(b->step_d);
@@ -263,6 +277,21 @@ cudaError_t enqueue_step(winds_wake_batch *b, int &launches) {
                               P<const double>(b->wind), P<double>(b->dom_new), s);
     ++launches;
   }
+  return e;
+}
+
+// End of step: (with lifting lines) Γ of the converged bound circulation,
+// then the new positions and histories.
+cudaError_t enqueue_post(winds_wake_batch *b, int &launches) {
+  cudaStream_t s = b->stream;
+  const WakeCase *cd = P<const WakeCase>(b->cases_d);
+  cudaError_t e = cudaSuccess;
+  if (b->kj) {
+    e = launch_wake_bookkeep(cd, b->ncases, b->max_cols, P<const double>(b->bound),
+                             P<const double>(b->trail_prev), P<double>(b->shed_cur),
+                             P<double>(b->trail_cur), s);
+    ++launches;
+  }
   const int keep_hist = b->prm.integrator == WINDS_INTEG_AB2 || b->prm.integrator == WINDS_INTEG_AB4;
   if (e == cudaSuccess)
     e = launch_wake_commit(cd, b->ncases, b->max_slots, P<int>(b->step_d), P<double>(b->dom),
@@ -273,6 +302,124 @@ cudaError_t enqueue_step(winds_wake_batch *b, int &launches) {
                            P<const double>(b->len_t), s);
   ++launches;
   return e;
+}
+
+cudaError_t enqueue_step(winds_wake_batch *b, int &launches) {
+  launches = 0;
+  cudaError_t e = enqueue_pre(b, launches);
+  int l2 = 0;
+  if (e == cudaSuccess) e = enqueue_post(b, l2);
+  launches += l2;
+  return e;
+}
+
+// One Kutta-Joukowski iteration of every active case: Γ from the bound
+// iterate, filaments with the step's cores, induced velocity at the lifting
+// lines, station update and per-case convergence.
+cudaError_t enqueue_kj_iter(winds_wake_batch *b, int &launches) {
+  cudaStream_t s = b->stream;
+  const WakeCase *cd = P<const WakeCase>(b->cases_d);
+  const KJCase *kd = P<const KJCase>(b->kjc_d);
+  PackedFilaments pf{P<float4>(b->fa), P<float4>(b->fb), P<float4>(b->fc), P<float>(b->fd),
+                     P<double4>(b->ra), P<double4>(b->rb)};
+  BBox *bb = P<BBox>(b->bbox);
+  cudaError_t e = launch_wake_bookkeep(cd, b->ncases, b->max_cols, P<const double>(b->bound),
+                                       P<const double>(b->trail_prev), P<double>(b->shed_cur),
+                                       P<double>(b->trail_cur), s);
+  if (e == cudaSuccess)
+    e = launch_wake_filaments(cd, b->ncases, b->max_fil, P<const int>(b->step_d), 0,
+                              P<const double>(b->dom), P<const double>(b->shed_cur),
+                              P<const double>(b->trail_cur), nullptr, nullptr, 0, 0, nullptr,
+                              nullptr, nullptr, nullptr, P<const double>(b->rc_s),
+                              P<const double>(b->rc_t), b->model, b->dcut, pf, bb, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(b->ctr.p, 0, sizeof(unsigned), s);
+  F32cArgs a;
+  a.fa = pf.fa;
+  a.fb = pf.fb;
+  a.fc = pf.fc;
+  a.fd = pf.fd;
+  a.ra = pf.ra;
+  a.rb = pf.rb;
+  a.tp = P<const double4>(b->tp_ll);
+  a.groups = P<const Group>(b->kj_groups);
+  a.tiles = P<const Tile>(b->kj_tiles);
+  a.items = P<const Item>(b->kj_items);
+  a.n_items = b->kj_nitems;
+  a.tile_cap = b->kj_tile_cap;
+  a.part = P<double>(b->kj_part);
+  a.work_ctr = P<unsigned>(b->ctr);
+  a.err = P<unsigned>(b->err);
+  a.near_ctr = P<unsigned long long>(b->nearctr);
+  a.bbox = bb;
+  a.model = b->model;
+  a.d = b->dcut;
+  a.n = b->nidx;
+  a.co = b->prm.co;
+  a.wait_limit_ns = default_wait_limit_ns();
+  if (e == cudaSuccess)
+    e = b->prec == WINDS_PREC_F64 ? launch_f64(a, b->kj_grid, s)
+                                  : launch_f32c(a, b->model, b->kj_T, b->kj_KF, b->kj_grid, s);
+  if (e == cudaSuccess)
+    e = launch_reduce(P<const Tile>(b->kj_tiles), b->kj_ntiles, P<const Group>(b->kj_groups),
+                      P<const double>(b->kj_part), P<const int>(b->perm_ll), b->kj_tile_cap, s);
+  if (e == cudaSuccess)
+    e = launch_kj_update(cd, kd, b->ncases, b->max_st, P<const int>(b->step_d),
+                         P<const double>(b->uindb), P<const double>(b->bxn), P<const double>(b->byn),
+                         P<const double>(b->bzn), P<const double>(b->vblade),
+                         P<const double>(b->chord), P<const int>(b->foil), P<const int>(b->foil_off),
+                         P<const double>(b->aoa_t), P<const double>(b->cl_t), P<const double>(b->cd_t),
+                         b->kjp.relax, P<double>(b->bound), P<const int>(b->conv),
+                         P<unsigned long long>(b->res_max), P<int>(b->diverged), P<double>(b->cl_o),
+                         P<double>(b->cd_o), P<double>(b->aoa_o), s);
+  if (e == cudaSuccess)
+    e = launch_kj_check(b->ncases, b->kjp.tol, P<int>(b->conv), P<int>(b->iters),
+                        P<unsigned long long>(b->res_max), P<double>(b->res_last), P<int>(b->active), s);
+  launches = 8;
+  return e;
+}
+
+// Lifting-line targets and the per-step reset of the iteration state.
+cudaError_t enqueue_kj_begin(winds_wake_batch *b) {
+  cudaStream_t s = b->stream;
+  cudaError_t e = launch_bbox_init(P<BBox>(b->bbox), s);
+  if (e == cudaSuccess)
+    e = launch_kj_targets(P<const WakeCase>(b->cases_d), P<const KJCase>(b->kjc_d), b->ncases,
+                          b->max_st, P<const int>(b->step_d), P<const double>(b->ll),
+                          P<double4>(b->tp_ll), P<BBox>(b->bbox), s);
+  for (DevBuf *x : {&b->conv, &b->iters, &b->diverged, &b->res_max})
+    if (e == cudaSuccess) e = cudaMemsetAsync(x->p, 0, b->ncases * 8, s);
+  return e;
+}
+
+int run_kj(winds_wake_batch *b, bool use_graph) {
+  cudaError_t e = enqueue_kj_begin(b);
+  if (e != cudaSuccess) return cuda_fail(e, "kj begin");
+  if (use_graph && !b->exec_kj) {
+    int l = 0;
+    e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+    cudaError_t e2 = e == cudaSuccess ? enqueue_kj_iter(b, l) : e;
+    e = cudaStreamEndCapture(b->stream, &b->g_kj);
+    if (e2 != cudaSuccess) e = e2;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec_kj, b->g_kj, 0);
+    if (e != cudaSuccess) return cuda_fail(e, "kj capture");
+  }
+  b->kj_evals = 0;
+  int active = 1;
+  for (int it = 0; it < b->kjp.maxiter && active; ++it) {
+    int l = 0;
+    e = use_graph ? cudaGraphLaunch(b->exec_kj, b->stream) : enqueue_kj_iter(b, l);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(&active, b->active.p, sizeof(int), cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "kj iteration");
+    ++b->kj_evals;
+  }
+  std::vector<int> div(b->ncases);
+  e = cudaMemcpy(div.data(), b->diverged.p, b->ncases * sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "kj flags");
+  for (int k = 0; k < b->ncases; ++k)
+    if (div[k]) return fail(WINDS_BS_ERR_DIVERGED, "case %d: Diverging soln!!! (Cl is NaN)", k);
+  return WINDS_BS_OK;
 }
 
 }  // namespace
@@ -428,6 +575,19 @@ int winds_wake_create(const winds_wake_case *cases, int ncases, const winds_wake
   return WINDS_BS_OK;
 }
 
+// Error word of the direct-sum kernels (bounded waits that ran out).
+static int device_error_word(winds_wake_batch *b) {
+  unsigned word = 0;
+  cudaError_t e = cudaMemcpy(&word, b->err.p, sizeof(word), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "error word read");
+  if (word) {
+    cudaMemset(b->err.p, 0, sizeof(unsigned));
+    return fail(word & kErrWaitTimeout ? WINDS_BS_ERR_TIMEOUT : WINDS_BS_ERR_CUDA,
+                "device reported error word 0x%x", word);
+  }
+  return WINDS_BS_OK;
+}
+
 int winds_wake_step(winds_wake_batch *b, int nsteps, int use_graph) {
   if (!b || nsteps < 0) return fail(WINDS_BS_ERR_ARG, "bad step arguments");
   if (b->steps_done + nsteps >= b->min_nsteps)
@@ -435,6 +595,43 @@ int winds_wake_step(winds_wake_batch *b, int nsteps, int use_graph) {
                 b->min_nsteps - 1, b->steps_done, nsteps);
   cudaSetDevice(b->dev);
   cudaError_t e = cudaSuccess;
+  if (b->kj) {
+    // pre-commit part, the iteration (host loop on a device convergence flag), commit
+    for (int k = 0; k < nsteps; ++k) {
+      if (use_graph && !b->exec_pre) {
+        int l1 = 0, l2 = 0;
+        e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+        cudaError_t e2 = e == cudaSuccess ? enqueue_pre(b, l1) : e;
+        e = cudaStreamEndCapture(b->stream, &b->g_pre);
+        if (e2 != cudaSuccess) e = e2;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec_pre, b->g_pre, 0);
+        if (e == cudaSuccess) e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+        e2 = e == cudaSuccess ? enqueue_post(b, l2) : e;
+        if (e == cudaSuccess) e = cudaStreamEndCapture(b->stream, &b->g_post);
+        if (e2 != cudaSuccess) e = e2;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec_post, b->g_post, 0);
+        b->launches = l1 + l2;
+        if (e != cudaSuccess) return cuda_fail(e, "wake step capture");
+      }
+      if (k == 0) cudaEventRecord(b->ev0, b->stream);
+      int l = 0;
+      e = use_graph ? cudaGraphLaunch(b->exec_pre, b->stream) : enqueue_pre(b, l);
+      if (e != cudaSuccess) return cuda_fail(e, "wake step");
+      int rc = run_kj(b, use_graph != 0);
+      if (!rc) rc = device_error_word(b);
+      if (rc) return rc;
+      int l2 = 0;
+      e = use_graph ? cudaGraphLaunch(b->exec_post, b->stream) : enqueue_post(b, l2);
+      if (!use_graph) b->launches = l + l2;
+      if (e != cudaSuccess) return cuda_fail(e, "wake step commit");
+    }
+    b->timed_steps = nsteps;
+    if (nsteps > 0) cudaEventRecord(b->ev1, b->stream);
+    b->steps_done += nsteps;
+    e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "wake step sync");
+    return device_error_word(b);
+  }
   if (use_graph && !b->exec && nsteps > 0) {
     // capture one step (launches nothing) before the timed steps
     e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
@@ -462,14 +659,7 @@ int winds_wake_step(winds_wake_batch *b, int nsteps, int use_graph) {
   b->steps_done += nsteps;
   e = cudaStreamSynchronize(b->stream);
   if (e != cudaSuccess) return cuda_fail(e, "wake step sync");
-  unsigned word = 0;
-  cudaMemcpy(&word, b->err.p, sizeof(word), cudaMemcpyDeviceToHost);
-  if (word) {
-    cudaMemset(b->err.p, 0, sizeof(unsigned));
-    return fail(word & kErrWaitTimeout ? WINDS_BS_ERR_TIMEOUT : WINDS_BS_ERR_CUDA,
-                "device reported error word 0x%x", word);
-  }
-  return WINDS_BS_OK;
+  return device_error_word(b);
 }
 
 int winds_wake_get_state(winds_wake_batch *b, int icase, double *dom, double *bound, double *shed,
@@ -521,12 +711,182 @@ int winds_wake_stats(winds_wake_batch *b, double *step_ms, long long *interactio
   return WINDS_BS_OK;
 }
 
+int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_kj_params *prm) {
+  if (!b || !kj || !prm || !(prm->relax > 0) || !(prm->tol >= 0) || prm->maxiter < 1)
+    return fail(WINDS_BS_ERR_ARG, "bad lifting-line arguments");
+  if (b->ncases > 1024) return fail(WINDS_BS_ERR_ARG, "at most 1024 cases with lifting lines");
+  cudaSetDevice(b->dev);
+  cudaStream_t s = b->stream;
+  b->kjp = *prm;
+  b->kjc.clear();
+  long long fr = 0, tt = 0, st = 0, tab = 0;
+  std::vector<int> foil_off, foils;
+  std::vector<double> aoa, cl, cd, chord;
+  b->max_st = 0;
+  for (int k = 0; k < b->ncases; ++k) {
+    const WakeCase &c = b->cases[k];
+    const winds_kj_case &h = kj[k];
+    const int ns = c.nst - 1;
+    if (!h.ll || !h.bxn || !h.byn || !h.bzn || !h.vblade || !h.chord || !h.foil || h.n_foils < 1 ||
+        !h.foil_points || !h.aoa || !h.cl || !h.cd)
+      return fail(WINDS_BS_ERR_ARG, "case %d: null lifting-line array", k);
+    KJCase q;
+    q.frame_off = fr;
+    q.t_off = tt;
+    q.station_off = st;
+    q.foil_base = (int)foil_off.size();
+    q.n_foils = h.n_foils;
+    long long o = 0;
+    for (int f = 0; f < h.n_foils; ++f) {
+      if (h.foil_points[f] < 2) return fail(WINDS_BS_ERR_ARG, "case %d: airfoil %d has < 2 points", k, f);
+      foil_off.push_back((int)(tab + o));
+      o += h.foil_points[f];
+    }
+    foil_off.push_back((int)(tab + o));
+    for (long long j = 0; j < o; ++j) {
+      aoa.push_back(h.aoa[j]);
+      cl.push_back(h.cl[j]);
+      cd.push_back(h.cd[j]);
+    }
+    for (int i = 0; i < ns; ++i) {
+      if (h.foil[i] < 0 || h.foil[i] >= h.n_foils)
+        return fail(WINDS_BS_ERR_ARG, "case %d: station %d uses airfoil %d of %d", k, i, h.foil[i], h.n_foils);
+      foils.push_back(h.foil[i]);
+      chord.push_back(h.chord[i]);
+    }
+    tab += o;
+    fr += (long long)ns * 3 * c.nsteps * c.nb;
+    tt += (long long)ns * c.nb;
+    st += ns;
+    b->max_st = std::max(b->max_st, ns * c.nb);
+    b->kjc.push_back(q);
+  }
+  b->frames_n = fr, b->n_ll = tt, b->stations_n = st;
+  int rc;
+  for (DevBuf *x : {&b->ll, &b->bxn, &b->byn, &b->bzn, &b->vblade})
+    if ((rc = x->ensure(fr * sizeof(double), s))) return rc;
+  if ((rc = b->kjc_d.ensure(b->ncases * sizeof(KJCase), s)) ||
+      (rc = b->chord.ensure(st * sizeof(double), s)) || (rc = b->foil.ensure(st * sizeof(int), s)) ||
+      (rc = b->foil_off.ensure(foil_off.size() * sizeof(int), s)) ||
+      (rc = b->aoa_t.ensure(tab * sizeof(double), s)) || (rc = b->cl_t.ensure(tab * sizeof(double), s)) ||
+      (rc = b->cd_t.ensure(tab * sizeof(double), s)) || (rc = b->tp_ll.ensure(tt * sizeof(double4), s)) ||
+      (rc = b->perm_ll.ensure(tt * sizeof(int), s)) || (rc = b->uindb.ensure(tt * 3 * sizeof(double), s)))
+    return rc;
+  for (DevBuf *x : {&b->conv, &b->iters, &b->diverged, &b->res_max, &b->res_last, &b->active})
+    if ((rc = x->ensure(std::max(b->ncases, 1) * 8 + 8, s))) return rc;
+  for (DevBuf *x : {&b->cl_o, &b->cd_o, &b->aoa_o})
+    if ((rc = x->ensure(b->bound_n * sizeof(double), s))) return rc;
+  cudaError_t e = cudaMemcpy(b->kjc_d.p, b->kjc.data(), b->ncases * sizeof(KJCase), cudaMemcpyHostToDevice);
+  for (int k = 0; k < b->ncases && e == cudaSuccess; ++k) {
+    const WakeCase &c = b->cases[k];
+    const long long n = (long long)(c.nst - 1) * 3 * c.nsteps * c.nb;
+    const long long off = b->kjc[k].frame_off;
+    const double *src[5] = {kj[k].ll, kj[k].bxn, kj[k].byn, kj[k].bzn, kj[k].vblade};
+    DevBuf *dst[5] = {&b->ll, &b->bxn, &b->byn, &b->bzn, &b->vblade};
+    for (int a = 0; a < 5 && e == cudaSuccess; ++a)
+      e = cudaMemcpy(P<double>(*dst[a]) + off, src[a], n * sizeof(double), cudaMemcpyHostToDevice);
+  }
+  std::vector<int> ident(std::max<long long>(tt, 1));
+  for (long long i = 0; i < tt; ++i) ident[i] = (int)i;
+  if (e == cudaSuccess) e = cudaMemcpy(b->chord.p, chord.data(), st * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->foil.p, foils.data(), st * sizeof(int), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->foil_off.p, foil_off.data(), foil_off.size() * sizeof(int), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->aoa_t.p, aoa.data(), tab * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->cl_t.p, cl.data(), tab * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->cd_t.p, cd.data(), tab * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->perm_ll.p, ident.data(), tt * sizeof(int), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(e, "lifting-line upload");
+  // plan: each case's lifting-line points against its filaments
+  std::vector<GroupSpec> gs;
+  for (int k = 0; k < b->ncases; ++k) {
+    const WakeCase &c = b->cases[k];
+    GroupSpec g;
+    g.out = P<double>(b->uindb) + 3 * b->kjc[k].t_off;
+    g.t_begin = b->kjc[k].t_off;
+    g.t_count = (long long)(c.nst - 1) * c.nb;
+    g.ns_p = c.nst - 1;
+    g.f_begin = (int)c.fil_off;
+    g.f_end = (int)(c.fil_off + c.fil_pad);
+    g.accumulate = 0;
+    gs.push_back(g);
+  }
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->dev);
+  int resident, quantum;
+  if (b->prec == WINDS_PREC_F64) {
+    b->kj_tile_cap = f64_threads();
+    resident = f64_occupancy() * sms;
+    quantum = f64_tile();
+  } else {
+    b->kj_tile_cap = f32c_threads() * b->kj_T;
+    resident = f32c_occupancy(b->model, b->kj_T, b->kj_KF) * sms;
+    quantum = kFilamentPad;
+  }
+  Plan pl;
+  build_plan(pl, gs, b->kj_tile_cap, resident, 4.0, quantum);
+  b->kj_ntiles = (int)pl.tiles.size();
+  b->kj_nitems = (int)pl.items.size();
+  b->kj_grid = std::max(1, std::min(b->kj_nitems, resident));
+  if ((rc = b->kj_groups.ensure(pl.groups.size() * sizeof(Group), s)) ||
+      (rc = b->kj_tiles.ensure(pl.tiles.size() * sizeof(Tile), s)) ||
+      (rc = b->kj_items.ensure(pl.items.size() * sizeof(Item), s)) ||
+      (rc = b->kj_part.ensure((size_t)b->kj_nitems * 3 * b->kj_tile_cap * sizeof(double), s)))
+    return rc;
+  if ((e = cudaMemcpy(b->kj_groups.p, pl.groups.data(), pl.groups.size() * sizeof(Group), cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMemcpy(b->kj_tiles.p, pl.tiles.data(), pl.tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMemcpy(b->kj_items.p, pl.items.data(), pl.items.size() * sizeof(Item), cudaMemcpyHostToDevice)) != cudaSuccess)
+    return cuda_fail(e, "lifting-line plan upload");
+  // graphs captured without the iteration must be rebuilt
+  if (b->exec) {
+    cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+  }
+  b->kj = true;
+  return WINDS_BS_OK;
+}
+
+int winds_wake_kj_stats(winds_wake_batch *b, int *iterations, double *residual,
+                        long long *ll_evaluations) {
+  if (!b || !b->kj) return fail(WINDS_BS_ERR_ARG, "no lifting lines attached");
+  cudaSetDevice(b->dev);
+  cudaStreamSynchronize(b->stream);
+  cudaError_t e = cudaSuccess;
+  if (iterations) e = cudaMemcpy(iterations, b->iters.p, b->ncases * sizeof(int), cudaMemcpyDeviceToHost);
+  if (residual && e == cudaSuccess)
+    e = cudaMemcpy(residual, b->res_last.p, b->ncases * sizeof(double), cudaMemcpyDeviceToHost);
+  if (ll_evaluations) *ll_evaluations = b->kj_evals;
+  return e == cudaSuccess ? WINDS_BS_OK : cuda_fail(e, "kj stats");
+}
+
+int winds_wake_get_perf(winds_wake_batch *b, int icase, double *cl, double *cd, double *aoa) {
+  if (!b || !b->kj || icase < 0 || icase >= b->ncases) return fail(WINDS_BS_ERR_ARG, "bad arguments");
+  cudaSetDevice(b->dev);
+  cudaStreamSynchronize(b->stream);
+  const WakeCase &c = b->cases[icase];
+  const size_t n = (size_t)(c.nst - 1) * c.nb;
+  cudaError_t e = cudaSuccess;
+  if (cl) e = cudaMemcpy(cl, P<double>(b->cl_o) + c.bound_off, n * sizeof(double), cudaMemcpyDeviceToHost);
+  if (cd && e == cudaSuccess) e = cudaMemcpy(cd, P<double>(b->cd_o) + c.bound_off, n * sizeof(double), cudaMemcpyDeviceToHost);
+  if (aoa && e == cudaSuccess) e = cudaMemcpy(aoa, P<double>(b->aoa_o) + c.bound_off, n * sizeof(double), cudaMemcpyDeviceToHost);
+  return e == cudaSuccess ? WINDS_BS_OK : cuda_fail(e, "perf read");
+}
+
 void winds_wake_destroy(winds_wake_batch *b) {
   if (!b) return;
   cudaSetDevice(b->dev);
   if (b->stream) cudaStreamSynchronize(b->stream);
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
+  for (cudaGraphExec_t x : {b->exec_pre, b->exec_kj, b->exec_post})
+    if (x) cudaGraphExecDestroy(x);
+  for (cudaGraph_t x : {b->g_pre, b->g_kj, b->g_post})
+    if (x) cudaGraphDestroy(x);
+  for (DevBuf *x : {&b->kjc_d, &b->ll, &b->bxn, &b->byn, &b->bzn, &b->vblade, &b->chord, &b->foil,
+                    &b->foil_off, &b->aoa_t, &b->cl_t, &b->cd_t, &b->tp_ll, &b->perm_ll, &b->uindb,
+                    &b->kj_groups, &b->kj_tiles, &b->kj_items, &b->kj_part, &b->conv, &b->iters,
+                    &b->res_max, &b->res_last, &b->active, &b->diverged, &b->cl_o, &b->cd_o,
+                    &b->aoa_o})
+    x->release();
   for (DevBuf *x : {&b->cases_d, &b->step_d, &b->dom, &b->dom_pred, &b->dom_new, &b->vel, &b->h1,
                     &b->h2, &b->h3, &b->uind, &b->uind_pred, &b->bound, &b->trail_prev,
                     &b->shed_cur, &b->trail_cur, &b->shed_next, &b->trail_next, &b->rc_s,

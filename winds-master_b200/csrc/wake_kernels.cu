@@ -90,8 +90,8 @@ __global__ void wake_filaments(const WakeCase *cases, const int *step, int step_
                                const double *dom, const double *shed, const double *trail,
                                const double *len_old_s, const double *len_old_t, int have_old,
                                int stretch, double *len_s, double *len_t, double *rc_s,
-                               double *rc_t, int model, double dcut, PackedFilaments pf,
-                               BBox *bb) {
+                               double *rc_t, const double *rc_in_s, const double *rc_in_t,
+                               int model, double dcut, PackedFilaments pf, BBox *bb) {
   const WakeCase c = cases[blockIdx.y];
   const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
@@ -118,6 +118,7 @@ __global__ void wake_filaments(const WakeCase *cases, const int *step, int step_
       g = shed[slot];
       age = j * c.dt;
       lold = len_old_s, lnew = len_s, rcout = rc_s;
+      if (rc_in_s) rcout = nullptr;
     } else {  // trailing: dom(:, j+1) -> dom(:, j)
       const long long k = f - nsh;
       i = (int)(k % c.nst);
@@ -132,18 +133,25 @@ __global__ void wake_filaments(const WakeCase *cases, const int *step, int step_
       g = trail[slot];
       age = (j + 0.5) * c.dt;
       lold = len_old_t, lnew = len_t, rcout = rc_t;
+      if (rc_in_t) rcout = nullptr;
     }
-    const double dx = x2 - x1, dy = y2 - y1, dz = z2 - z1;
-    const double L = sqrt(dx * dx + dy * dy + dz * dz);  // |L| (FilamentLength.m:43)
-    double rc = core_sq(c, g, c.core_mode == 0 ? t_abs : age);
-    if (stretch && have_old && j >= 1 && j <= m - 2) {
-      // filamentmod.m:29-41: lengths square-rooted again, same column index
-      const double a = sqrt(L), o = sqrt(lold[slot]);
-      const double strain = (a - o) / o;
-      rc = rc * (1.0 / (1.0 + strain));
+    const double *rc_in = f < nsh ? rc_in_s : rc_in_t;
+    double rc;
+    if (rc_in) {  // cores held fixed (the Kutta-Joukowski loop keeps the step's vcore)
+      rc = rc_in[slot];
+    } else {
+      const double dx = x2 - x1, dy = y2 - y1, dz = z2 - z1;
+      const double L = sqrt(dx * dx + dy * dy + dz * dz);  // |L| (FilamentLength.m:43)
+      rc = core_sq(c, g, c.core_mode == 0 ? t_abs : age);
+      if (stretch && have_old && j >= 1 && j <= m - 2) {
+        // filamentmod.m:29-41: lengths square-rooted again, same column index
+        const double a = sqrt(L), o = sqrt(lold[slot]);
+        const double strain = (a - o) / o;
+        rc = rc * (1.0 / (1.0 + strain));
+      }
+      lnew[slot] = L;
+      if (rcout) rcout[slot] = rc;
     }
-    lnew[slot] = L;
-    if (rcout) rcout[slot] = rc;
     pack_filament(c.fil_off + f, x1, y1, z1, x2, y2, z2, g, rc, model, dcut, pf.fa, pf.fb, pf.fc,
                   pf.fd, pf.ra, pf.rb);
     lo[0] = (float)fmin(x1, x2), lo[1] = (float)fmin(y1, y2), lo[2] = (float)fmin(z1, z2);
@@ -288,11 +296,12 @@ cudaError_t launch_wake_filaments(const WakeCase *cases, int ncases, long long m
                                   const double *shed, const double *trail,
                                   const double *len_old_s, const double *len_old_t, int have_old,
                                   int stretch, double *len_s, double *len_t, double *rc_s,
-                                  double *rc_t, int model, double dcut,
-                                  const PackedFilaments &pf, BBox *bb, cudaStream_t s) {
+                                  double *rc_t, const double *rc_in_s, const double *rc_in_t,
+                                  int model, double dcut, const PackedFilaments &pf, BBox *bb,
+                                  cudaStream_t s) {
   wake_filaments<<<case_grid(max_fil_pad, ncases, 256), 256, 0, s>>>(
       cases, step, step_add, dom, shed, trail, len_old_s, len_old_t, have_old, stretch, len_s,
-      len_t, rc_s, rc_t, model, dcut, pf, bb);
+      len_t, rc_s, rc_t, rc_in_s, rc_in_t, model, dcut, pf, bb);
   return cudaGetLastError();
 }
 

@@ -23,8 +23,9 @@ cudaError_t launch_wake_filaments(const WakeCase *cases, int ncases, long long m
                                   const double *shed, const double *trail,
                                   const double *len_old_s, const double *len_old_t, int have_old,
                                   int stretch, double *len_s, double *len_t, double *rc_s,
-                                  double *rc_t, int model, double dcut,
-                                  const PackedFilaments &pf, BBox *bb, cudaStream_t s);
+                                  double *rc_t, const double *rc_in_s, const double *rc_in_t,
+                                  int model, double dcut, const PackedFilaments &pf, BBox *bb,
+                                  cudaStream_t s);
 cudaError_t launch_wake_targets(const WakeCase *cases, int ncases, long long max_nodes,
                                 const double *dom, double4 *tp, int *tgroup, BBox *bb,
                                 cudaStream_t s);

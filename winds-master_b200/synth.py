@@ -320,3 +320,67 @@ def batch_cases(n: int, seed: int = 0, steps_range=(60, 720), nodes_range=(17, 4
                              yaw_deg=float(rng.uniform(*yaw_range)),
                              shear=float(rng.uniform(*shear_range)), seed=seed * 1000 + k))
     return out
+
+
+# ----------------------------------------------------------- lifting line (KJ)
+def synthetic_polar(step_deg: float = 0.25):
+    """Airfoil table on [-180, 180] deg: Cl = 2 pi sin(a) cos(a) up to the
+    12 deg stall, then 1.2 sin(2a) (continued on both signs); Cd = 0.008 +
+    0.6 sin^2(a)."""
+    a = np.arange(-180.0, 180.0 + step_deg / 2, step_deg)
+    r = np.radians(a)
+    cl = np.where(np.abs(a) <= 12.0, 2 * np.pi * np.sin(r) * np.cos(r), 1.2 * np.sin(2 * r))
+    cd = 0.008 + 0.6 * np.sin(r) ** 2
+    return a, cl, cd
+
+
+def make_kj_case(case: RotorCase, nsteps: int, t0: float = 0.0, pitch_deg: float = 0.0) -> dict:
+    """Lifting-line inputs of ``core/KuttaJoukowski.m:173-298`` for every step:
+    ``ll`` (pos.bound: quarter-chord midpoints), blade-frame unit vectors
+    ``bxn`` (chord, leading to trailing edge), ``byn``, ``bzn`` (radial), the
+    blade-frame velocity ``vblade`` (wind minus blade motion, vel.blade),
+    chord, one airfoil for every station (``synthetic_polar``)."""
+    nst, nb, ns = case.nst, case.nb, case.ns
+    r, chord_n, twist_n = blade_geometry(case)
+    rm = 0.5 * (r[1:] + r[:-1])
+    s = (rm - case.r_root) / (case.R - case.r_root)
+    chord = 3.5 + (1.4 - 3.5) * s
+    th = np.radians(13.0 * (1.0 - s) + pitch_deg)
+    yaw = np.radians(case.yaw_deg)
+
+    def rot(v):  # yaw about z, v [..., 3]
+        x, y, z = v[..., 0], v[..., 1], v[..., 2]
+        return np.stack([x * np.cos(yaw) - y * np.sin(yaw), x * np.sin(yaw) + y * np.cos(yaw), z], axis=-1)
+
+    shape = (ns, 3, nsteps, nb)
+    out = {k: np.zeros(shape) for k in ("ll", "bxn", "byn", "bzn", "vblade")}
+    for st in range(nsteps):
+        t = t0 + st * case.dt
+        q, _ = blade_nodes(case, t, pitch_deg)
+        out["ll"][:, :, st, :] = 0.5 * (q[1:] + q[:-1])
+        psi = 2.0 * np.pi * np.arange(nb) / nb + case.omega * t            # [nb]
+        rhat = np.stack([np.zeros(nb), np.cos(psi), np.sin(psi)], axis=-1)  # [nb, 3]
+        that = np.stack([np.zeros(nb), -np.sin(psi), np.cos(psi)], axis=-1)
+        xhat = np.array([1.0, 0.0, 0.0])
+        ct, sn = np.cos(th)[:, None, None], np.sin(th)[:, None, None]
+        d = -ct * that[None] + sn * xhat[None, None]                          # chord LE->TE
+        n = sn * that[None] + ct * xhat[None, None]
+        bx, by, bz = rot(d), rot(-n), rot(np.broadcast_to(rhat[None], d.shape))
+        # relative wind at the station: freestream (with shear) minus blade velocity
+        pts = out["ll"][:, :, st, :].transpose(0, 2, 1)                      # [ns, nb, 3]
+        h = np.maximum(case.hub_height + pts[..., 2], 1.0) / case.hub_height
+        w = np.zeros_like(pts)
+        w[..., 0] = case.U * h ** case.shear
+        vb = rot(case.omega * rm[:, None, None] * that[None])                # blade velocity
+        wr = w - vb
+        out["bxn"][:, :, st, :] = bx.transpose(0, 2, 1)
+        out["byn"][:, :, st, :] = by.transpose(0, 2, 1)
+        out["bzn"][:, :, st, :] = bz.transpose(0, 2, 1)
+        out["vblade"][:, :, st, :] = np.stack([(wr * bx).sum(-1), (wr * by).sum(-1),
+                                               (wr * bz).sum(-1)], axis=1)
+    a, cl, cd = synthetic_polar()
+    f = np.asfortranarray
+    res = {k: f(v) for k, v in out.items()}
+    res.update(chord=chord, foil=np.zeros(ns, dtype=np.int32), foil_points=np.array([a.size], dtype=np.int32),
+               aoa=a, cl=cl, cd=cd, twist_deg=np.degrees(th), r_over_R=rm / case.R)
+    return res

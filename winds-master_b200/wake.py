@@ -27,6 +27,17 @@ class WakeCaseC(C.Structure):
                 ("dom", C.c_void_p), ("bound", C.c_void_p), ("trail_gamma", C.c_void_p)]
 
 
+class KJCaseC(C.Structure):
+    _fields_ = [("ll", C.c_void_p), ("bxn", C.c_void_p), ("byn", C.c_void_p), ("bzn", C.c_void_p),
+                ("vblade", C.c_void_p), ("chord", C.c_void_p), ("foil", C.c_void_p),
+                ("n_foils", C.c_int), ("foil_points", C.c_void_p), ("aoa", C.c_void_p),
+                ("cl", C.c_void_p), ("cd", C.c_void_p)]
+
+
+class KJParamsC(C.Structure):
+    _fields_ = [("relax", C.c_double), ("tol", C.c_double), ("maxiter", C.c_int)]
+
+
 class WakeParamsC(C.Structure):
     _fields_ = [("integrator", C.c_int), ("core_model", C.c_int), ("d", C.c_double),
                 ("co", C.c_double), ("precision", C.c_int), ("pcc_double_add", C.c_int),
@@ -44,6 +55,9 @@ def _bind():
         L.winds_wake_stats.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_longlong),
                                        C.POINTER(C.c_int)]
         L.winds_wake_destroy.argtypes = [C.c_void_p]
+        L.winds_wake_set_kj.argtypes = [C.c_void_p, C.POINTER(KJCaseC), C.POINTER(KJParamsC)]
+        L.winds_wake_kj_stats.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_longlong)]
+        L.winds_wake_get_perf.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
         L._wake_bound = True
     return L
 
@@ -91,6 +105,42 @@ class WakeBatch:
     def set_bound(self, i, bound):
         b = np.asfortranarray(bound, dtype=np.float64)
         _check(_bind().winds_wake_set_bound(self.h, i, b.ctypes.data))
+
+    def set_kj(self, kjs, relax=0.25, tol=1e-6, maxiter=30):
+        """Attaches one lifting line per case (dicts as :func:`synth.make_kj_case`
+        returns them): every later step runs the Kutta-Joukowski iteration."""
+        arr = (KJCaseC * len(kjs))()
+        for k, j in enumerate(kjs):
+            a = arr[k]
+            for f in ("ll", "bxn", "byn", "bzn", "vblade", "chord", "aoa", "cl", "cd"):
+                x = np.asfortranarray(j[f], dtype=np.float64)
+                self._keep.append(x)
+                setattr(a, f, x.ctypes.data)
+            for f in ("foil", "foil_points"):
+                x = np.ascontiguousarray(j[f], dtype=np.int32)
+                self._keep.append(x)
+                setattr(a, f, x.ctypes.data)
+            a.n_foils = len(j["foil_points"])
+        p = KJParamsC(float(relax), float(tol), int(maxiter))
+        _check(_bind().winds_wake_set_kj(self.h, arr, C.byref(p)))
+
+    def kj_stats(self):
+        """(iterations [ncases], residual [ncases], lifting-line evaluations)
+        of the last step."""
+        n = len(self.cases)
+        it = np.zeros(n, dtype=np.int32)
+        res = np.zeros(n)
+        ev = C.c_longlong()
+        _check(_bind().winds_wake_kj_stats(self.h, it.ctypes.data, res.ctypes.data, C.byref(ev)))
+        return it, res, ev.value
+
+    def perf(self, i):
+        """Cl, Cd, AoA [ns, nb] of case ``i`` from the last iteration."""
+        c = self.cases[i]
+        shp = (c["nst"] - 1, c["nb"])
+        cl, cd, aoa = (np.zeros(shp, order="F") for _ in range(3))
+        _check(_bind().winds_wake_get_perf(self.h, i, cl.ctypes.data, cd.ctypes.data, aoa.ctypes.data))
+        return cl, cd, aoa
 
     def stats(self):
         ms, n, l = C.c_double(), C.c_longlong(), C.c_int()
