@@ -165,31 +165,36 @@ __device__ __forceinline__ void bbox_accumulate(const float lo[3], const float h
 
 // ------------------------------------------------------- filament packing
 // Writes filament f in the packed layout (see bs_types.h): FP32 hi/lo x1,
-// |L|^2, near-singular radius Rn^2 = max(|L|^2, 9 rc^2), L, gamma/4pi and the
-// core term, plus the FP64 copy. A NaN/Inf ubar is zeroed by the reference
-// (core/BiotSavart.m:111); with finite endpoints that happens exactly when
-// gamma (or, Vatistas, rc; or, cut-off, d*|L|^2) is not finite, so such
-// filaments get gamma/4pi = 0 and contribute nothing.
+// |L|^2, near-singular radius Rn^2 = max(|L|^2, 9 rc^2), L, the core term and
+// K L (K = gamma/4pi), plus the FP64 copy. A NaN/Inf ubar is zeroed by the
+// reference (core/BiotSavart.m:111); with finite endpoints that happens
+// exactly when gamma (or, Vatistas, rc; or, cut-off, d*|L|^2) is not finite,
+// so such filaments get K = 0 and contribute nothing.
+//
+// Vatistas n=2 in FP32: with c = K L x r1, the core factor
+// |L x r1|^2 / sqrt(|L x r1|^4 + (rc^2 |L|^2)^2) equals |c|^2 / sqrt(|c|^4 + D)
+// for D = (K^2 rc^2 |L|^2)^2, so the kernel never multiplies by K.
 __device__ __forceinline__ void pack_filament(long long f, double x1, double y1, double z1,
                                               double x2, double y2, double z2, double g, double r,
                                               int model, double dcut, float4 *fa, float4 *fb,
-                                              float4 *fc, float *fd, double4 *ra, double4 *rb) {
+                                              float4 *fc, float4 *fd, double4 *ra, double4 *rb) {
   ra[f] = make_double4(x1, y1, z1, g);
   rb[f] = make_double4(x2, y2, z2, r);
   const double Lx = x2 - x1, Ly = y2 - y1, Lz = z2 - z1;
   const double L2 = Lx * Lx + Ly * Ly + Lz * Lz;
   double K = g / k4Pi;
+  if (!isfinite(g)) K = 0.0;
   double D;
   if (model == kCoreVatistas) {
-    D = (r * L2) * (r * L2);
     if (!isfinite(r)) K = 0.0;
-    if (!(D >= 1e-30)) D = 1e-30;
+    const double s = K * K * r * L2;
+    D = s * s;
+    if (!(D >= 1e-30)) D = 1e-30;  // also K = 0: the factor stays finite, K L = 0
     if (D > 1e30) D = 1e30;
   } else {
     D = dcut * L2;
     if (!isfinite(D)) K = 0.0, D = 0.0;
   }
-  if (!isfinite(g)) K = 0.0;
   // Near-singular region: r1.r2 < Rn^2, a ball around the midpoint of radius
   // sqrt(|L|^2/4 + Rn^2) that contains every point within 3 core radii.
   double Rn2 = L2;
@@ -199,18 +204,18 @@ __device__ __forceinline__ void pack_filament(long long f, double x1, double y1,
   fa[f] = make_float4(hx, hy, hz, (float)L2);
   fb[f] = make_float4((float)(x1 - (double)hx), (float)(y1 - (double)hy), (float)(z1 - (double)hz),
                       (float)Rn2);
-  fc[f] = make_float4((float)Lx, (float)Ly, (float)Lz, (float)K);
-  fd[f] = (float)D;
+  fc[f] = make_float4((float)Lx, (float)Ly, (float)Lz, (float)D);
+  fd[f] = make_float4((float)(K * Lx), (float)(K * Ly), (float)(K * Lz), 0.f);
 }
 
 // Inert filament (far away, zero length, zero circulation) for padding.
 __device__ __forceinline__ void pack_inert(long long f, float4 *fa, float4 *fb, float4 *fc,
-                                           float *fd, double4 *ra, double4 *rb) {
+                                           float4 *fd, double4 *ra, double4 *rb) {
   const double far = 1e18;
   fa[f] = make_float4((float)far, (float)far, (float)far, 0.f);
   fb[f] = make_float4(0.f, 0.f, 0.f, 0.f);
-  fc[f] = make_float4(0.f, 0.f, 0.f, 0.f);
-  fd[f] = 1.f;
+  fc[f] = make_float4(0.f, 0.f, 0.f, 1.f);
+  fd[f] = make_float4(0.f, 0.f, 0.f, 0.f);
   ra[f] = make_double4(far, far, far, 0.0);
   rb[f] = make_double4(far, far, far, 0.0);
 }

@@ -39,7 +39,7 @@ __global__ void bs_bbox_init(BBox *bb) {
 __global__ void bs_pack_filaments(const double *__restrict__ F1, const double *__restrict__ F2,
                                   const double *__restrict__ gam, const double *__restrict__ rc,
                                   long long d0, long long nf, long long off, int model, double dcut,
-                                  float4 *fa, float4 *fb, float4 *fc, float *fd, double4 *ra,
+                                  float4 *fa, float4 *fb, float4 *fc, float4 *fd, double4 *ra,
                                   double4 *rb, BBox *bb) {
   const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
@@ -58,7 +58,7 @@ __global__ void bs_pack_filaments(const double *__restrict__ F1, const double *_
 
 // Inert filaments filling [from, to): far away, zero length, zero circulation.
 __global__ void bs_pad_filaments(long long from, long long to, float4 *fa, float4 *fb, float4 *fc,
-                                 float *fd, double4 *ra, double4 *rb) {
+                                 float4 *fd, double4 *ra, double4 *rb) {
   const long long f = from + (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= to) return;
   pack_inert(f, fa, fb, fc, fd, ra, rb);
@@ -138,7 +138,7 @@ constexpr uint64_t kDefaultWaitNs = 2000000000ull;  // 2 s per tile: far above a
 
 template <int KF>
 struct StageSmem {
-  static constexpr int kBytes = KF * 52;  // fa, fb, fc: 16 B each; fd: 4 B
+  static constexpr int kBytes = KF * 64;  // fa, fb, fc, fd: 16 B each
   static constexpr int kStages = KF >= 128 ? 3 : kStagesMax;  // filament stages in flight
 };
 
@@ -168,7 +168,7 @@ __device__ __forceinline__ void issue_stage(const F32cArgs &a, unsigned char *st
   bulk_g2s(stage, a.fa + f0, KF * 16, bar);
   bulk_g2s(stage + KF * 16, a.fb + f0, KF * 16, bar);
   bulk_g2s(stage + KF * 32, a.fc + f0, KF * 16, bar);
-  bulk_g2s(stage + KF * 48, a.fd + f0, KF * 4, bar);
+  bulk_g2s(stage + KF * 48, a.fd + f0, KF * 16, bar);
 }
 
 // Thread 0 hands global tile g (filaments f0 .. f0+KF) to the copy engine
@@ -196,18 +196,20 @@ __device__ __forceinline__ bool try_produce(const F32cArgs &a, unsigned char *sm
 }
 
 // One target-filament interaction in FP32, accumulated into (ax, ay, az).
-// With NEAR it also tests r1.r2 < Rn^2: such pairs are skipped and recorded
-// in `bits` (they are redone in FP64 after the tile).
+// (Mx, My, Mz) = K L with K = gamma/4pi; D is the packed core term. With NEAR
+// it also tests r1.r2 < Rn^2: such pairs are skipped and recorded in `bits`
+// (they are redone in FP64 after the tile).
 template <int MODEL, bool CO, bool NEAR>
 __device__ __forceinline__ void interact(float px, float py, float pz, float xrx, float xry,
                                          float xrz, float Lx, float Ly, float Lz, float L2,
-                                         float K, float Dv, float Rn2, float co2, float &ax,
-                                         float &ay, float &az, unsigned &bits, unsigned bit) {
+                                         float Mx, float My, float Mz, float Dv, float Rn2,
+                                         float co2, float &ax, float &ay, float &az,
+                                         unsigned &bits, unsigned bit) {
   const float rx = px - xrx, ry = py - xry, rz = pz - xrz;  // r1 = P - x1
-  // r1 x r2 = L x r1 (no cancellation for far or collinear points)
-  const float cxv = Ly * rz - Lz * ry;
-  const float cyv = Lz * rx - Lx * rz;
-  const float czv = Lx * ry - Ly * rx;
+  // K (r1 x r2) = K L x r1 (no cancellation for far or collinear points)
+  const float cxv = My * rz - Mz * ry;
+  const float cyv = Mz * rx - Mx * rz;
+  const float czv = Mx * ry - My * rx;
   const float r1s = rx * rx + ry * ry + rz * rz;
   const float Ld = Lx * rx + Ly * ry + Lz * rz;
   const float dot = r1s - Ld;          // r1 . r2
@@ -217,14 +219,14 @@ __device__ __forceinline__ void interact(float px, float py, float pz, float xrx
   const float e = fmaf(dot, gg, 1.f);  // 1 + cos(theta) >= 1 for far pairs
   float ub;
   if (MODEL == kCoreVatistas) {
-    // Cnu / (r1 r2 (r1 r2 + r1.r2)) with h^2 = |c|^2/|L|^2 and rc^4 folded:
-    // Cnu = |c|^2 / sqrt(|c|^4 + (rc^2 |L|^2)^2)
+    // Cnu / (r1 r2 (r1 r2 + r1.r2)) with h^2 = |L x r1|^2/|L|^2 and rc^4 folded:
+    // Cnu = |c|^2 / sqrt(|c|^4 + D), c = K L x r1, D = (K^2 rc^2 |L|^2)^2
     const float c2 = cxv * cxv + cyv * cyv + czv * czv;
     const float q = fmaf(c2, c2, Dv);
-    ub = K * ((i1 + i2) * gg) * c2 * rsqrt_approx((e * e) * q);
+    ub = ((i1 + i2) * gg) * c2 * rsqrt_approx((e * e) * q);
   } else {
     // (r1+r2)/(r1r2(r1r2+r1.r2) + d|L|^2) = (i1+i2) gg / (e + d|L|^2 gg^2)
-    ub = K * ((i1 + i2) * gg) * rcp_approx(fmaf(Dv, gg * gg, e));
+    ub = ((i1 + i2) * gg) * rcp_approx(fmaf(Dv, gg * gg, e));
   }
   bool skip = false;
   if (NEAR) {
@@ -248,7 +250,7 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, con
                                           uint64_t *empty, float *s_k, unsigned *s_nb,
                                           unsigned &gt, float (&px)[T], float (&py)[T],
                                           float (&pz)[T], float cx, float cy, float cz,
-                                          float S2, unsigned &near_cnt) {
+                                          float S2, const float *ws, unsigned &near_cnt) {
   const int tid = threadIdx.x;
   const int ntiles = (it.f_end - it.f_begin) / KF;
   const float co2 = (float)(a.co * a.co);
@@ -288,35 +290,82 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, con
     const float4 *sA = reinterpret_cast<const float4 *>(stage);
     const float4 *sB = reinterpret_cast<const float4 *>(stage + KF * 16);
     const float4 *sC = reinterpret_cast<const float4 *>(stage + KF * 32);
-    const float *sD = reinterpret_cast<const float *>(stage + KF * 48);
+    const float4 *sD = reinterpret_cast<const float4 *>(stage + KF * 48);
     if (timed_out) {
       ok = false;
       break;
     }
-    // Hot loop: filaments in groups of 4; the near-singular bits of a group
-    // (bit 8*j + t: filament 4*kk+j, target t) go to shared memory as one word.
+    // Hot loop: filaments in groups of 4. A warp-level screen (one filament
+    // per lane, every 32 filaments) sends groups that are far from all of the
+    // warp's targets down the plain path; the others test every pair and put
+    // their near-singular bits (bit 8*j + t: filament 4*kk+j, target t) in
+    // shared memory as one word. `careful` has bit g for every such group g.
+    unsigned careful = 0u;
 #pragma unroll 1
-    for (int kk = 0; kk < KF; kk += 4) {
-      unsigned nbits = 0;
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int k = kk + j;
-        const float4 A = sA[k];
-        const float4 B = sB[k];
-        const float4 C = sC[k];
-        const float Dv = sD[k];
-        // x1 relative to this thread's centre, from its hi/lo split
-        const float xrx = (A.x - cx) + B.x, xry = (A.y - cy) + B.y, xrz = (A.z - cz) + B.z;
-        // near-singular threshold, raised for threads whose targets spread far
-        // from their centre (the FP32 differences lose ~eps * spread / |r1|)
-        const float L2 = A.w, Rn2 = fmaxf(B.w, S2);
-        const float Lx = C.x, Ly = C.y, Lz = C.z, K = C.w;
-#pragma unroll
-        for (int t = 0; t < T; ++t)
-          interact<MODEL, CO, true>(px[t], py[t], pz[t], xrx, xry, xrz, Lx, Ly, Lz, L2, K, Dv,
-                                    Rn2, co2, ax[t], ay[t], az[t], nbits, 1u << (8 * j + t));
+    for (int w = 0; w < KF / 32; ++w) {
+      unsigned m;
+      if (CO) {
+        m = 0xffffffffu;
+      } else {
+        const int k = 32 * w + lane;
+        const float4 A = sA[k], B = sB[k], C = sC[k];
+        // the warp's target ball (centre, radius, largest S2), kept in shared
+        // memory so it holds no registers across the hot loop
+        const float wcx = ws[0], wcy = ws[1], wcz = ws[2], wr = ws[3], rn_floor = ws[4];
+        const float big = fabsf(wcx) + fabsf(wcy) + fabsf(wcz);
+        const float mx = (A.x - wcx) + fmaf(0.5f, C.x, B.x);
+        const float my = (A.y - wcy) + fmaf(0.5f, C.y, B.y);
+        const float mz = (A.z - wcz) + fmaf(0.5f, C.z, B.z);
+        const float d2 = mx * mx + my * my + mz * mz;
+        const float reach = sqrtf(fmaf(0.25f, A.w, fmaxf(B.w, rn_floor)));
+        const float slack =
+            1e-5f * (big + fabsf(A.x) + fabsf(A.y) + fabsf(A.z)) + 1e-3f * (reach + wr);
+        const float lim = wr + reach + slack;
+        m = __ballot_sync(0xffffffffu, !(d2 > lim * lim));
       }
-      s_nb[(kk / 4) * kThreads + tid] = nbits;
+#pragma unroll 1
+      for (int g = 0; g < 8; ++g) {
+        const int kk = 32 * w + 4 * g;
+        if (((m >> (4 * g)) & 0xfu) == 0u) {
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const int k = kk + j;
+            const float4 A = sA[k];
+            const float4 B = sB[k];
+            const float4 C = sC[k];
+            const float4 M = sD[k];
+            const float xrx = (A.x - cx) + B.x, xry = (A.y - cy) + B.y, xrz = (A.z - cz) + B.z;
+            unsigned unused = 0;
+#pragma unroll
+            for (int t = 0; t < T; ++t)
+              interact<MODEL, false, false>(px[t], py[t], pz[t], xrx, xry, xrz, C.x, C.y, C.z,
+                                            A.w, M.x, M.y, M.z, C.w, 0.f, co2, ax[t], ay[t],
+                                            az[t], unused, 0u);
+          }
+        } else {
+          careful |= 1u << (8 * w + g);
+          unsigned nbits = 0;
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const int k = kk + j;
+            const float4 A = sA[k];
+            const float4 B = sB[k];
+            const float4 C = sC[k];
+            const float4 M = sD[k];
+            // x1 relative to this thread's centre, from its hi/lo split
+            const float xrx = (A.x - cx) + B.x, xry = (A.y - cy) + B.y, xrz = (A.z - cz) + B.z;
+            // near-singular threshold, raised for threads whose targets spread
+            // far from their centre (the FP32 differences lose ~eps * spread / |r1|)
+            const float Rn2 = fmaxf(B.w, S2);
+#pragma unroll
+            for (int t = 0; t < T; ++t)
+              interact<MODEL, CO, true>(px[t], py[t], pz[t], xrx, xry, xrz, C.x, C.y, C.z, A.w,
+                                        M.x, M.y, M.z, C.w, Rn2, co2, ax[t], ay[t], az[t], nbits,
+                                        1u << (8 * j + t));
+          }
+          s_nb[(kk / 4) * kThreads + tid] = nbits;
+        }
+      }
     }
     // This warp is done with the stage: release it to the producer.
     __syncwarp();
@@ -338,8 +387,11 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, con
     }
     // Near-singular pairs of this tile, each lane its own: the reference formula
     // in FP64, added to the Kahan state as an exact hi + lo pair.
+    unsigned cg = careful;
 #pragma unroll 1
-    for (int w = 0; w < KF / 4; ++w) {
+    while (cg) {
+      const int w = __ffs(cg) - 1;
+      cg &= cg - 1u;
       unsigned bits = s_nb[w * kThreads + tid];
       while (bits) {
         const int b = __ffs(bits) - 1;
@@ -389,12 +441,14 @@ struct MinBlocks {
 
 template <int T, int KF, int MODEL>
 __global__ void __launch_bounds__(kThreads, MinBlocks<T>::value) bs_f32c(const F32cArgs a) {
+  static_assert(KF % 32 == 0 && KF / 4 <= 32, "one screen word per 32 filaments, one bit per group");
   extern __shared__ __align__(128) unsigned char smem[];
   float *s_k = reinterpret_cast<float *>(smem + StageSmem<KF>::kStages * StageSmem<KF>::kBytes);
   unsigned *s_nb = reinterpret_cast<unsigned *>(s_k + 6 * kThreads * T);
   uint64_t *full = reinterpret_cast<uint64_t *>(s_nb + (KF / 4) * kThreads);
   uint64_t *empty = full + StageSmem<KF>::kStages;
   __shared__ int s_item;
+  __shared__ float s_ws[kThreads / 32][8];
   const int tid = threadIdx.x;
   if (tid == 0) {
     for (int s = 0; s < StageSmem<KF>::kStages; ++s) {
@@ -439,13 +493,43 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<T>::value) bs_f32c(const F
       for (int c = 0; c < 6; ++c) s_k[c * kThreads * T + tid * T + t] = 0.f;
     }
     const float S2 = 0.09f * spread2;  // pairs closer than 0.3 x spread go to FP64
+    // The warp's targets lie in the ball (wc, wr) around lane 0's centre. As
+    // r1.r2 = |P - m|^2 - |L|^2/4 (m the filament midpoint), a filament whose
+    // midpoint is farther than wr + sqrt(|L|^2/4 + Rn^2) from wc has
+    // r1.r2 >= Rn^2 for every target of the warp; rn_floor is the warp's
+    // largest per-thread threshold S2.
+    const float wcx = __shfl_sync(0xffffffffu, cx, 0);
+    const float wcy = __shfl_sync(0xffffffffu, cy, 0);
+    const float wcz = __shfl_sync(0xffffffffu, cz, 0);
+    float wr2 = 0.f;
+#pragma unroll
+    for (int t = 0; t < T; ++t) {
+      const float dx = (cx - wcx) + px[t], dy = (cy - wcy) + py[t], dz = (cz - wcz) + pz[t];
+      wr2 = fmaxf(wr2, dx * dx + dy * dy + dz * dz);
+    }
+    float rn_floor = S2;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      wr2 = fmaxf(wr2, __shfl_xor_sync(0xffffffffu, wr2, o));
+      rn_floor = fmaxf(rn_floor, __shfl_xor_sync(0xffffffffu, rn_floor, o));
+    }
+    float *ws = s_ws[tid >> 5];
+    if ((tid & 31) == 0) {
+      ws[0] = wcx;
+      ws[1] = wcy;
+      ws[2] = wcz;
+      ws[3] = sqrtf(wr2);
+      ws[4] = rn_floor;
+    }
+    __syncwarp();
     bool ok;
     if (co_on)
       ok = f32c_item<T, KF, MODEL, true>(a, it, tl, smem, full, empty, s_k, s_nb, gt, px, py, pz,
-                                         cx, cy, cz, S2, near_cnt);
+                                         cx, cy, cz, S2, ws, near_cnt);
     else
       ok = f32c_item<T, KF, MODEL, false>(a, it, tl, smem, full, empty, s_k, s_nb, gt, px, py,
-                                          pz, cx, cy, cz, S2, near_cnt);
+                                          pz, cx, cy, cz, S2, ws, near_cnt);
+    __syncwarp();
     if (!ok) return;
     double *part = a.part + (size_t)item_id * 3 * a.tile_cap;
 #pragma unroll

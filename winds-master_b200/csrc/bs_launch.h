@@ -8,8 +8,7 @@
 namespace winds {
 
 struct PackedFilaments {
-  float4 *fa, *fb, *fc;
-  float *fd;
+  float4 *fa, *fb, *fc, *fd;
   double4 *ra, *rb;
 };
 

@@ -4,8 +4,11 @@
 //   packed filaments, padded to the filament tile (KF) with inert entries
 //     fa[f] = (x1_hi.x, x1_hi.y, x1_hi.z, |L|^2)   float4
 //     fb[f] = (x1_lo.x, x1_lo.y, x1_lo.z, Rn^2)    float4  (x1 = hi + lo exactly to ~2^-48)
-//     fc[f] = (L.x, L.y, L.z, gamma/4pi)           float4  (L = x2 - x1)
-//     fd[f] = (rc^2 |L|^2)^2 (Vatistas) or d |L|^2 (cut-off)   float
+//     fc[f] = (L.x, L.y, L.z, D)                   float4  (L = x2 - x1)
+//     fd[f] = (K L.x, K L.y, K L.z, 0)             float4  (K = gamma/4pi)
+//   with D = (K^2 rc^2 |L|^2)^2 (Vatistas: the core term scaled like |K L x r1|^4,
+//   so K cancels from the core factor and enters only through K L) or d |L|^2
+//   (cut-off)
 //   raw FP64 filaments for near-singular terms and the FP64 path
 //     ra[f] = (x1, y1, z1, gamma)  rb[f] = (x2, y2, z2, rc^2)   double4
 //   targets  tp[t] = (x, y, z, 0) double4, sorted by (group, Morton code of the
@@ -58,7 +61,7 @@ struct BBox {           // ordered-int keys of float bounds (see float_key)
 
 struct F32cArgs {
   const float4 *fa, *fb, *fc;
-  const float *fd;
+  const float4 *fd;
   const double4 *ra, *rb;
   const double4 *tp;
   const Group *groups;

@@ -281,7 +281,7 @@ int pack_inputs(Context *c, const winds_bs_family *fams, int nfam,
   for (const TargetSpec &t : tsets) nt += t.count;
   int rc;
   if ((rc = c->fa.ensure(nfp * sizeof(float4), s)) || (rc = c->fb.ensure(nfp * sizeof(float4), s)) ||
-      (rc = c->fc.ensure(nfp * sizeof(float4), s)) || (rc = c->fd.ensure(nfp * sizeof(float), s)) ||
+      (rc = c->fc.ensure(nfp * sizeof(float4), s)) || (rc = c->fd.ensure(nfp * sizeof(float4), s)) ||
       (rc = c->ra.ensure(nfp * sizeof(double4), s)) ||
       (rc = c->rb.ensure(nfp * sizeof(double4), s)) ||
       (rc = c->tp.ensure(std::max<long long>(nt, 1) * sizeof(double4), s)) ||
@@ -297,7 +297,7 @@ int pack_inputs(Context *c, const winds_bs_family *fams, int nfam,
     return fail(WINDS_BS_ERR_CUDA, "target sort size query failed");
   if ((rc = c->sort_tmp.ensure(sort_bytes + 256, s))) return rc;
   PackedFilaments pf{(float4 *)c->fa.p, (float4 *)c->fb.p, (float4 *)c->fc.p,
-                     (float *)c->fd.p, (double4 *)c->ra.p, (double4 *)c->rb.p};
+                     (float4 *)c->fd.p, (double4 *)c->ra.p, (double4 *)c->rb.p};
   cudaError_t e = launch_bbox_init((BBox *)c->bbox.p, s);
   c->launches += 1;
   long long off = 0;
@@ -409,7 +409,7 @@ int run_direct_sum(Context *c, const std::vector<GroupSpec> &gs, int model, doub
   a.fa = (const float4 *)c->fa.p;
   a.fb = (const float4 *)c->fb.p;
   a.fc = (const float4 *)c->fc.p;
-  a.fd = (const float *)c->fd.p;
+  a.fd = (const float4 *)c->fd.p;
   a.ra = (const double4 *)c->ra.p;
   a.rb = (const double4 *)c->rb.p;
   a.tp = (const double4 *)c->tp.p;

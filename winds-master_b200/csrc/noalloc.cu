@@ -189,7 +189,7 @@ extern "C" int winds_bs_eval_device_noalloc(const winds_bs_family *fams, int nfa
   unsigned *err = cv.take<unsigned>(4);
   unsigned long long *nearc = cv.take<unsigned long long>(1);
   PackedFilaments pf{cv.take<float4>(nfp), cv.take<float4>(nfp), cv.take<float4>(nfp),
-                     cv.take<float>(nfp), cv.take<double4>(nfp), cv.take<double4>(nfp)};
+                     cv.take<float4>(nfp), cv.take<double4>(nfp), cv.take<double4>(nfp)};
   double4 *tp = cv.take<double4>(nt);
   double4 *tp_raw = cv.take<double4>(nt);
   int *tgroup = cv.take<int>(nt);

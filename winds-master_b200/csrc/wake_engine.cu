@@ -98,7 +98,7 @@ int alloc_all(winds_wake_batch *b) {
     return rc;
   const long long nf = b->fil_pad, nt = std::max<long long>(b->nodes, 1);
   if ((rc = b->fa.ensure(nf * sizeof(float4), s)) || (rc = b->fb.ensure(nf * sizeof(float4), s)) ||
-      (rc = b->fc.ensure(nf * sizeof(float4), s)) || (rc = b->fd.ensure(nf * sizeof(float), s)) ||
+      (rc = b->fc.ensure(nf * sizeof(float4), s)) || (rc = b->fd.ensure(nf * sizeof(float4), s)) ||
       (rc = b->ra.ensure(nf * sizeof(double4), s)) || (rc = b->rb.ensure(nf * sizeof(double4), s)) ||
       (rc = b->tp.ensure(nt * sizeof(double4), s)) ||
       (rc = b->tp_raw.ensure(nt * sizeof(double4), s)) ||
@@ -175,7 +175,7 @@ cudaError_t enqueue_eval(winds_wake_batch *b, const double *dom, const double *s
                          double *rc_s, double *rc_t, DevBuf &groups, int &launches) {
   cudaStream_t s = b->stream;
   const WakeCase *cd = P<const WakeCase>(b->cases_d);
-  PackedFilaments pf{P<float4>(b->fa), P<float4>(b->fb), P<float4>(b->fc), P<float>(b->fd),
+  PackedFilaments pf{P<float4>(b->fa), P<float4>(b->fb), P<float4>(b->fc), P<float4>(b->fd),
                      P<double4>(b->ra), P<double4>(b->rb)};
   BBox *bb = P<BBox>(b->bbox);
   cudaError_t e = launch_bbox_init(bb, s);
@@ -320,7 +320,7 @@ cudaError_t enqueue_kj_iter(winds_wake_batch *b, int &launches) {
   cudaStream_t s = b->stream;
   const WakeCase *cd = P<const WakeCase>(b->cases_d);
   const KJCase *kd = P<const KJCase>(b->kjc_d);
-  PackedFilaments pf{P<float4>(b->fa), P<float4>(b->fb), P<float4>(b->fc), P<float>(b->fd),
+  PackedFilaments pf{P<float4>(b->fa), P<float4>(b->fb), P<float4>(b->fc), P<float4>(b->fd),
                      P<double4>(b->ra), P<double4>(b->rb)};
   BBox *bb = P<BBox>(b->bbox);
   cudaError_t e = launch_wake_bookkeep(cd, b->ncases, b->max_cols, P<const double>(b->bound),
