@@ -117,6 +117,12 @@ typedef struct {
   const double *aoa;       /* concatenated tables: AoA (deg, ascending), Cl, Cd        */
   const double *cl;
   const double *cd;
+  /* Station inputs of the bound-circulation MLP (optional; all four needed by
+   * winds_wake_set_mlp): */
+  const double *r_over_R;     /* [ns] station radius / rotor radius               */
+  const double *chord_over_R; /* [ns] chord / rotor radius                        */
+  const double *twist;        /* [ns] local pitch (twist + blade pitch), rad      */
+  const double *azimuth;      /* [nsteps,nb] blade azimuth per step, rad          */
 } winds_kj_case;
 
 typedef struct {
@@ -136,6 +142,28 @@ int winds_wake_kj_stats(winds_wake_batch *b, int *iterations, double *residual,
 
 /* Cl, Cd and AoA [ns,nb] of one case from the last iteration of the last step. */
 int winds_wake_get_perf(winds_wake_batch *b, int icase, double *cl, double *cd, double *aoa);
+
+/* Starts every later step's iteration from the MLP's prediction instead of
+ * the previous step's bound circulation (winds_mlp.h; NULL restores the
+ * previous-step start). Features per station, in this order: r/R, chord/R,
+ * twist, sin(azimuth), cos(azimuth), the local inflow in the blade frame
+ * (3 components: vblade at the step plus the previous step's induced
+ * velocity at the lifting line, transformed as kj() does), previous bound
+ * circulation, its change over the previous step; the start value is
+ * Gamma_prev + out_scale * network(features). The network must have 10 inputs
+ * and live on the batch's device; the iteration and its tolerance are
+ * unchanged. No reference counterpart (WInDS.m:131 always starts from the
+ * previous step). */
+struct winds_mlp;
+int winds_wake_set_mlp(winds_wake_batch *b, struct winds_mlp *m);
+
+/* The start value [ns,nb] of the last step's iteration for one case. */
+int winds_wake_get_kj_guess(winds_wake_batch *b, int icase, double *guess);
+
+/* The MLP features [ns*nb][10] (rows i + ns*b) of one case at the last step,
+ * computed whenever the lifting lines carry the station inputs (training
+ * pairs: these rows with the converged bound circulation). */
+int winds_wake_get_kj_features(winds_wake_batch *b, int icase, float *x);
 
 void winds_wake_destroy(winds_wake_batch *b);
 

@@ -1,0 +1,65 @@
+"""GPU tests of the MLP start value of the Kutta-Joukowski iteration
+(winds_wake_set_mlp): device features and start value against the host path,
+and what the trained network gains over the previous-step start."""
+from __future__ import annotations
+
+import importlib
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _mods():
+    gi = importlib.import_module("winds-master_b200.gamma_init")
+    mlp = importlib.import_module("winds-master_b200.mlp")
+    wake = importlib.import_module("winds-master_b200.wake")
+    synth = importlib.import_module("winds-master_b200.synth")
+    return gi, mlp, wake, synth
+
+
+def test_features_and_start_value_match_host(wb):
+    gi, mlp, wake, synth = _mods()
+    pts = gi.operating_points(3, seed=7, nst=13, wake_steps=10)
+    cases, kjs = gi.build(pts, 4)
+    b = wake.WakeBatch(cases, integrator="pcc")
+    b.set_kj(kjs, relax=0.3, tol=1e-6, maxiter=100)
+    m = mlp.Mlp(gi.N_FEATURES, seed=3)
+    m.set_scaling(np.zeros(10, np.float32), np.full(10, 0.2, np.float32), 0.7)
+    b.set_mlp(m)
+    prev = [b.bound(k) for k in range(3)]
+    b.step(1)
+    for k in range(3):
+        x = b.kj_features(k)
+        # step 0: no previous induced velocity, no previous change
+        xh = synth.kj_features(kjs[k], 0, prev[k])
+        np.testing.assert_allclose(x, xh, rtol=2e-6, atol=1e-6)
+        g = b.kj_guess(k)
+        gh = prev[k].ravel(order="F") + float(np.float32(0.7)) * m.forward(x).astype(np.float64)
+        np.testing.assert_allclose(g.ravel(order="F"), gh, rtol=1e-12, atol=1e-9)
+    # later steps carry the change of the converged circulation
+    prev1 = [b.bound(k) for k in range(3)]
+    b.step(1)
+    for k in range(3):
+        x = b.kj_features(k)
+        np.testing.assert_allclose(x[:, 8], prev1[k].ravel(order="F"), rtol=1e-6, atol=1e-5)
+        np.testing.assert_allclose(x[:, 9], (prev1[k] - prev[k]).ravel(order="F"), rtol=1e-5, atol=1e-4)
+    b.close()
+    m.close()
+
+
+def test_trained_start_value_saves_iterations(wb):
+    """Trained on plain-solver pairs (~4.5e5) of the attached-flow operating
+    points among 400 candidates, the network's start value needs fewer
+    iterations on held-out attached points at the same tolerance and leaves
+    the converged circulation unchanged (the fixed point is unique there)."""
+    gi, *_ = _mods()
+    r = gi.study(n_train=400, n_test=120, epochs=60)
+    assert r["pairs"] > 300000 and r["test_points"] >= 10
+    assert r["loss_last"] < 0.1 * r["loss_first"]
+    assert r["converged_plain"] == 1.0 and r["converged_mlp"] == 1.0
+    assert r["saved_steady"] > 0.03, r
+    assert r["cases_improved"] >= 0.6 * r["test_points"], r
+    assert r["bound_rel_diff_max"] <= 2e-3, r
+    r["model"].close()

@@ -5,6 +5,8 @@
 //                airfoil tables (:262-269), Γ = ½|V|c Cl (:277), relaxed update
 //                (:281), relative residual in FP64 (:290), per station
 //   kj_check     per case: converged when max |residual| <= tol (:45)
+//   kj_features, kj_apply_guess   inputs and result of the bound-circulation
+//                MLP that replaces the previous-step start value (WInDS.m:131)
 #include <cmath>
 
 #include "bs_device.cuh"
@@ -86,6 +88,53 @@ __global__ void kj_update(const WakeCase *cases, const KJCase *kc, const int *st
   atomicMax(&res_max[ci], (unsigned long long)__double_as_longlong(r));
 }
 
+// The inflow features are the station's total inflow in the blade frame at
+// this step with the induced velocity of the previous step's last iteration
+// (uindb, zero before the first step): vblade + [bxn; byn; bzn] uindb, the
+// velocity the first iteration of kj() would see (core/KuttaJoukowski.m:241-249).
+__global__ void kj_features(const WakeCase *cases, const KJCase *kc, const int *step,
+                            const double *bound, const double *bound_last,
+                            const double *vblade, const double *bxn,
+                            const double *byn, const double *bzn, const double *uindb,
+                            const double *st_r, const double *st_c, const double *st_tw,
+                            const double *azim, float *x) {
+  const WakeCase c = cases[blockIdx.y];
+  const KJCase k = kc[blockIdx.y];
+  const int ns = c.nst - 1;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ns * c.nb) return;
+  const int i = t % ns, b = t / ns;
+  const int s = *step;
+  const long long fo = k.frame_off + i + (long long)ns * (3 * (s + (long long)c.nsteps * b));
+  const long long st = k.station_off + i;
+  const double az = azim[k.az_off + s + (long long)c.nsteps * b];
+  float *f = x + (k.t_off + t) * kKJFeatures;
+  f[0] = (float)st_r[st];
+  f[1] = (float)st_c[st];
+  f[2] = (float)st_tw[st];
+  f[3] = (float)sin(az);
+  f[4] = (float)cos(az);
+  const double *u = uindb + 3 * k.t_off + i + (long long)ns * 3 * b;
+  const double *fr[3] = {bxn, byn, bzn};
+  for (int a = 0; a < 3; ++a)
+    f[5 + a] = (float)(vblade[fo + a * ns] +
+                       (fr[a][fo] * u[0] + fr[a][fo + ns] * u[ns] + fr[a][fo + 2 * ns] * u[2 * ns]));
+  const long long q = c.bound_off + i + (long long)ns * b;
+  f[8] = (float)bound[q];
+  f[9] = (float)(bound[q] - bound_last[q]);
+}
+
+__global__ void kj_apply_guess(const WakeCase *cases, const KJCase *kc, const float *y,
+                               float out_scale, double *bound) {
+  const WakeCase c = cases[blockIdx.y];
+  const KJCase k = kc[blockIdx.y];
+  const int ns = c.nst - 1;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ns * c.nb) return;
+  const int i = t % ns, b = t / ns;
+  bound[c.bound_off + i + (long long)ns * b] += (double)out_scale * (double)y[k.t_off + t];
+}
+
 // One thread per case: a case converged in this iteration stops updating.
 __global__ void kj_check(int ncases, double tol, int *converged, int *iters,
                          unsigned long long *res_max, double *res_last, int *active) {
@@ -118,6 +167,24 @@ cudaError_t launch_kj_update(const WakeCase *cases, const KJCase *kc, int ncases
   kj_update<<<dim3((max_st + 127) / 128, ncases), 128, 0, s>>>(
       cases, kc, step, uindb, bxn, byn, bzn, vblade, chord, foil, foil_off, aoa_t, cl_t, cd_t,
       relax, bound, converged, res_max, diverged, cl_out, cd_out, aoa_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_kj_features(const WakeCase *cases, const KJCase *kc, int ncases, int max_st,
+                               const int *step, const double *bound, const double *bound_last,
+                               const double *vblade, const double *bxn, const double *byn,
+                               const double *bzn, const double *uindb, const double *st_r,
+                               const double *st_c, const double *st_tw, const double *azim,
+                               float *x, cudaStream_t s) {
+  kj_features<<<dim3((max_st + 127) / 128, ncases), 128, 0, s>>>(
+      cases, kc, step, bound, bound_last, vblade, bxn, byn, bzn, uindb, st_r, st_c, st_tw, azim,
+      x);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_kj_apply_guess(const WakeCase *cases, const KJCase *kc, int ncases, int max_st,
+                                  const float *y, float out_scale, double *bound, cudaStream_t s) {
+  kj_apply_guess<<<dim3((max_st + 127) / 128, ncases), 128, 0, s>>>(cases, kc, y, out_scale, bound);
   return cudaGetLastError();
 }
 

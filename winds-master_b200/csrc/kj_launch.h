@@ -12,9 +12,18 @@ struct KJCase {
   long long frame_off;    // ns*3*nsteps*nb per case: ll, bxn, byn, bzn, vblade
   long long t_off;        // first lifting-line target (ns*nb per case)
   long long station_off;  // first station (ns per case): chord, foil
+  long long az_off;       // nsteps*nb per case: blade azimuth (MLP features)
   int foil_base;          // this case's first entry in the foil offset table
   int n_foils;
 };
+
+// Features of the bound-circulation MLP per lifting-line point (row t_off + t):
+// r/R, chord/R, twist, sin and cos of the blade azimuth, the three
+// blade-frame components of the local inflow (vblade at the step plus the
+// previous step's induced velocity at the lifting line), the current bound
+// circulation (the previous step's converged value) and its change over the
+// previous step.
+constexpr int kKJFeatures = 10;
 
 cudaError_t launch_kj_targets(const WakeCase *cases, const KJCase *kc, int ncases, int max_st,
                               const int *step, const double *ll, double4 *tp, BBox *bb,
@@ -27,6 +36,15 @@ cudaError_t launch_kj_update(const WakeCase *cases, const KJCase *kc, int ncases
                              double relax, double *bound, const int *converged,
                              unsigned long long *res_max, int *diverged, double *cl_out,
                              double *cd_out, double *aoa_out, cudaStream_t s);
+cudaError_t launch_kj_features(const WakeCase *cases, const KJCase *kc, int ncases, int max_st,
+                               const int *step, const double *bound, const double *bound_last,
+                               const double *vblade, const double *bxn, const double *byn,
+                               const double *bzn, const double *uindb, const double *st_r,
+                               const double *st_c, const double *st_tw, const double *azim,
+                               float *x, cudaStream_t s);
+// bound += out_scale * y (row order of the lifting-line targets)
+cudaError_t launch_kj_apply_guess(const WakeCase *cases, const KJCase *kc, int ncases, int max_st,
+                                  const float *y, float out_scale, double *bound, cudaStream_t s);
 cudaError_t launch_kj_check(int ncases, double tol, int *converged, int *iters,
                             unsigned long long *res_max, double *res_last, int *active,
                             cudaStream_t s);

@@ -18,6 +18,8 @@
 #include "bs_launch.h"
 #include "engine.h"
 #include "kj_launch.h"
+#include "mlp_engine.h"
+#include "mlp_launch.h"
 #include "wake_launch.h"
 #include "winds_wake.h"
 
@@ -64,6 +66,11 @@ struct winds_wake_batch {
   DevBuf conv, iters, res_max, res_last, active, diverged, cl_o, cd_o, aoa_o;
   int kj_ntiles = 0, kj_nitems = 0, kj_grid = 0, kj_tile_cap = 0, kj_T = 2, kj_KF = 64;
   long long kj_evals = 0;
+  // bound-circulation MLP start value
+  bool mlp_inputs = false;      // every case gave the station arrays
+  DevBuf st_r, st_c, st_tw, azim, guess, feat, bound_last;
+  winds_mlp *mlp = nullptr;
+  MlpWork mw;
   cudaGraphExec_t exec_pre = nullptr, exec_kj = nullptr, exec_post = nullptr;
   cudaGraph_t g_pre = nullptr, g_kj = nullptr, g_post = nullptr;
 };
@@ -388,6 +395,34 @@ cudaError_t enqueue_kj_begin(winds_wake_batch *b) {
                           P<double4>(b->tp_ll), P<BBox>(b->bbox), s);
   for (DevBuf *x : {&b->conv, &b->iters, &b->diverged, &b->res_max})
     if (e == cudaSuccess) e = cudaMemsetAsync(x->p, 0, b->ncases * 8, s);
+  const WakeCase *cd = P<const WakeCase>(b->cases_d);
+  const KJCase *kd = P<const KJCase>(b->kjc_d);
+  if (e == cudaSuccess && b->mlp_inputs)
+    e = launch_kj_features(cd, kd, b->ncases, b->max_st, P<const int>(b->step_d),
+                           P<const double>(b->bound), P<const double>(b->bound_last),
+                           P<const double>(b->vblade), P<const double>(b->bxn), P<const double>(b->byn),
+                           P<const double>(b->bzn), P<const double>(b->uindb),
+                           P<const double>(b->st_r), P<const double>(b->st_c),
+                           P<const double>(b->st_tw), P<const double>(b->azim), P<float>(b->feat),
+                           s);
+  // the previous step's converged value, for the next step's change feature
+  if (e == cudaSuccess && b->mlp_inputs)
+    e = cudaMemcpyAsync(b->bound_last.p, b->bound.p, b->bound_n * sizeof(double),
+                        cudaMemcpyDeviceToDevice, s);
+  if (e == cudaSuccess && b->mlp) {
+    // start value Gamma_prev + out_scale * network(features)
+    e = launch_mlp_prep(P<float>(b->feat), b->n_ll, kKJFeatures, mlp_shift_dev(b->mlp),
+                        mlp_scale_dev(b->mlp), P<__nv_bfloat16>(b->mw.X), s);
+    if (e == cudaSuccess &&
+        mlp_forward(b->mlp, P<__nv_bfloat16>(b->mw.X), b->n_ll, b->mw, P<float>(b->mw.y), s))
+      e = cudaErrorLaunchFailure;
+    if (e == cudaSuccess)
+      e = launch_kj_apply_guess(cd, kd, b->ncases, b->max_st, P<const float>(b->mw.y),
+                                mlp_out_scale(b->mlp), P<double>(b->bound), s);
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b->guess.p, b->bound.p, b->bound_n * sizeof(double),
+                        cudaMemcpyDeviceToDevice, s);
   return e;
 }
 
@@ -419,6 +454,16 @@ int run_kj(winds_wake_batch *b, bool use_graph) {
   if (e != cudaSuccess) return cuda_fail(e, "kj flags");
   for (int k = 0; k < b->ncases; ++k)
     if (div[k]) return fail(WINDS_BS_ERR_DIVERGED, "case %d: Diverging soln!!! (Cl is NaN)", k);
+  if (b->mlp) {
+    unsigned word = 0;
+    e = cudaMemcpy(&word, mlp_err_word(b->mlp), sizeof(word), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "mlp error word");
+    if (word) {
+      cudaMemset(mlp_err_word(b->mlp), 0, sizeof(unsigned));
+      return fail(word & kErrWaitTimeout ? WINDS_BS_ERR_TIMEOUT : WINDS_BS_ERR_CUDA,
+                  "mlp kernels reported error word 0x%x", word);
+    }
+  }
   return WINDS_BS_OK;
 }
 
@@ -719,7 +764,8 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
   cudaStream_t s = b->stream;
   b->kjp = *prm;
   b->kjc.clear();
-  long long fr = 0, tt = 0, st = 0, tab = 0;
+  long long fr = 0, tt = 0, st = 0, tab = 0, az = 0;
+  bool all_inputs = true;
   std::vector<int> foil_off, foils;
   std::vector<double> aoa, cl, cd, chord;
   b->max_st = 0;
@@ -734,6 +780,8 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
     q.frame_off = fr;
     q.t_off = tt;
     q.station_off = st;
+    q.az_off = az;
+    if (!h.r_over_R || !h.chord_over_R || !h.twist || !h.azimuth) all_inputs = false;
     q.foil_base = (int)foil_off.size();
     q.n_foils = h.n_foils;
     long long o = 0;
@@ -755,6 +803,7 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
       chord.push_back(h.chord[i]);
     }
     tab += o;
+    az += (long long)c.nsteps * c.nb;
     fr += (long long)ns * 3 * c.nsteps * c.nb;
     tt += (long long)ns * c.nb;
     st += ns;
@@ -774,8 +823,36 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
     return rc;
   for (DevBuf *x : {&b->conv, &b->iters, &b->diverged, &b->res_max, &b->res_last, &b->active})
     if ((rc = x->ensure(std::max(b->ncases, 1) * 8 + 8, s))) return rc;
-  for (DevBuf *x : {&b->cl_o, &b->cd_o, &b->aoa_o})
+  for (DevBuf *x : {&b->cl_o, &b->cd_o, &b->aoa_o, &b->guess, &b->bound_last})
     if ((rc = x->ensure(b->bound_n * sizeof(double), s))) return rc;
+  // no change before the first step
+  if (cudaError_t e0 = cudaMemcpy(b->bound_last.p, b->bound.p, b->bound_n * sizeof(double),
+                                  cudaMemcpyDeviceToDevice);
+      e0 != cudaSuccess)
+    return cuda_fail(e0, "bound copy");
+  b->mlp_inputs = all_inputs;
+  // no induced velocity at the lifting line before the first step
+  if (cudaError_t e0 = cudaMemset(b->uindb.p, 0, tt * 3 * sizeof(double)); e0 != cudaSuccess)
+    return cuda_fail(e0, "lifting-line reset");
+  if (all_inputs) {
+    if ((rc = b->feat.ensure(std::max<long long>(tt, 1) * kKJFeatures * sizeof(float), s))) return rc;
+    if ((rc = b->st_r.ensure(st * sizeof(double), s)) || (rc = b->st_c.ensure(st * sizeof(double), s)) ||
+        (rc = b->st_tw.ensure(st * sizeof(double), s)) || (rc = b->azim.ensure(az * sizeof(double), s)))
+      return rc;
+    for (int k = 0; k < b->ncases; ++k) {
+      const WakeCase &c = b->cases[k];
+      const size_t ns = (size_t)(c.nst - 1);
+      const size_t so = (size_t)b->kjc[k].station_off, ao = (size_t)b->kjc[k].az_off;
+      cudaError_t e2 = cudaMemcpy(P<double>(b->st_r) + so, kj[k].r_over_R, ns * 8, cudaMemcpyHostToDevice);
+      if (e2 == cudaSuccess) e2 = cudaMemcpy(P<double>(b->st_c) + so, kj[k].chord_over_R, ns * 8, cudaMemcpyHostToDevice);
+      if (e2 == cudaSuccess) e2 = cudaMemcpy(P<double>(b->st_tw) + so, kj[k].twist, ns * 8, cudaMemcpyHostToDevice);
+      if (e2 == cudaSuccess)
+        e2 = cudaMemcpy(P<double>(b->azim) + ao, kj[k].azimuth, (size_t)c.nsteps * c.nb * 8, cudaMemcpyHostToDevice);
+      if (e2 != cudaSuccess) return cuda_fail(e2, "mlp station upload");
+    }
+  } else {
+    b->mlp = nullptr;
+  }
   cudaError_t e = cudaMemcpy(b->kjc_d.p, b->kjc.data(), b->ncases * sizeof(KJCase), cudaMemcpyHostToDevice);
   for (int k = 0; k < b->ncases && e == cudaSuccess; ++k) {
     const WakeCase &c = b->cases[k];
@@ -845,6 +922,48 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
   return WINDS_BS_OK;
 }
 
+int winds_wake_set_mlp(winds_wake_batch *b, winds_mlp *m) {
+  if (!b || !b->kj) return fail(WINDS_BS_ERR_ARG, "attach lifting lines before the MLP");
+  if (!m) {
+    b->mlp = nullptr;
+    return WINDS_BS_OK;
+  }
+  if (!b->mlp_inputs)
+    return fail(WINDS_BS_ERR_ARG, "every lifting line needs r_over_R, chord_over_R, twist, azimuth");
+  if (mlp_n_in(m) != kKJFeatures)
+    return fail(WINDS_BS_ERR_ARG, "the MLP has %d inputs, the start value uses %d", mlp_n_in(m),
+                kKJFeatures);
+  if (mlp_device(m) != b->dev) return fail(WINDS_BS_ERR_ARG, "MLP and batch on different devices");
+  cudaSetDevice(b->dev);
+  int rc = b->mw.ensure(std::max<long long>(b->n_ll, 1), false, b->stream);
+  if (rc) return rc;
+  b->mlp = m;
+  return WINDS_BS_OK;
+}
+
+int winds_wake_get_kj_features(winds_wake_batch *b, int icase, float *x) {
+  if (!b || !b->kj || !b->mlp_inputs || icase < 0 || icase >= b->ncases || !x)
+    return fail(WINDS_BS_ERR_ARG, "no lifting-line features");
+  cudaSetDevice(b->dev);
+  cudaStreamSynchronize(b->stream);
+  const WakeCase &c = b->cases[icase];
+  cudaError_t e = cudaMemcpy(x, P<float>(b->feat) + b->kjc[icase].t_off * kKJFeatures,
+                             (size_t)(c.nst - 1) * c.nb * kKJFeatures * sizeof(float),
+                             cudaMemcpyDeviceToHost);
+  return e == cudaSuccess ? WINDS_BS_OK : cuda_fail(e, "feature read");
+}
+
+int winds_wake_get_kj_guess(winds_wake_batch *b, int icase, double *guess) {
+  if (!b || !b->kj || icase < 0 || icase >= b->ncases || !guess)
+    return fail(WINDS_BS_ERR_ARG, "bad arguments");
+  cudaSetDevice(b->dev);
+  cudaStreamSynchronize(b->stream);
+  const WakeCase &c = b->cases[icase];
+  cudaError_t e = cudaMemcpy(guess, P<double>(b->guess) + c.bound_off,
+                             (size_t)(c.nst - 1) * c.nb * sizeof(double), cudaMemcpyDeviceToHost);
+  return e == cudaSuccess ? WINDS_BS_OK : cuda_fail(e, "guess read");
+}
+
 int winds_wake_kj_stats(winds_wake_batch *b, int *iterations, double *residual,
                         long long *ll_evaluations) {
   if (!b || !b->kj) return fail(WINDS_BS_ERR_ARG, "no lifting lines attached");
@@ -885,8 +1004,10 @@ void winds_wake_destroy(winds_wake_batch *b) {
                     &b->foil_off, &b->aoa_t, &b->cl_t, &b->cd_t, &b->tp_ll, &b->perm_ll, &b->uindb,
                     &b->kj_groups, &b->kj_tiles, &b->kj_items, &b->kj_part, &b->conv, &b->iters,
                     &b->res_max, &b->res_last, &b->active, &b->diverged, &b->cl_o, &b->cd_o,
-                    &b->aoa_o})
+                    &b->aoa_o, &b->st_r, &b->st_c, &b->st_tw, &b->azim, &b->guess, &b->feat,
+                    &b->bound_last})
     x->release();
+  b->mw.release();
   for (DevBuf *x : {&b->cases_d, &b->step_d, &b->dom, &b->dom_pred, &b->dom_new, &b->vel, &b->h1,
                     &b->h2, &b->h3, &b->uind, &b->uind_pred, &b->bound, &b->trail_prev,
                     &b->shed_cur, &b->trail_cur, &b->shed_next, &b->trail_next, &b->rc_s,

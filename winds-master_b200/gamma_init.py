@@ -1,0 +1,186 @@
+"""The learned start value of the Kutta-Joukowski iteration.
+
+The plain solver (the batched device time step with the lifting-line fixed
+point of ``core/KuttaJoukowski.m:42-49``, started from the previous step's
+bound circulation as ``WInDS.m:131`` does) generates pairs (station state,
+converged bound circulation); the MLP of ``winds_mlp.h`` learns the change
+``Gamma_conv - Gamma_prev`` from the state and then starts each step's
+iteration at ``Gamma_prev + out_scale * network(state)``. The iteration still
+runs to the same tolerance, so converged results are unchanged and only
+iterations (each one two Biot-Savart calls in the reference: shed and
+trailing filaments onto the lifting line) are saved.
+
+Operating points: 3 blades, R = 63 m, 41 span nodes, 10 deg per step, wind
+speed U in [5, 25] m/s, blade pitch in [0, 15] deg, yaw in [0, 30] deg and
+tip-speed ratio in [5, 9] (rotor speed TSR U / R), drawn from a seed;
+synthetic blade and polar (chord 3.5 -> 1.4 m, twist 13 -> 0 deg, Cl =
+2 pi sin a cos a to the 12 deg stall, then 1.2 sin 2a; Cd = 0.008 +
+0.6 sin^2 a) with cylindrical root sections (Cl = 0) inside r/R < 0.2.
+
+Features (device-computed, ``winds_wake_get_kj_features``): r/R, chord/R,
+twist, sin and cos of the azimuth, the local inflow in the blade frame
+(kinematic inflow plus the previous step's induced velocity at the lifting
+line), the previous bound circulation and its change over the previous step.
+Training pairs come only from (case, step) whose plain iteration converged.
+"""
+from __future__ import annotations
+
+import dataclasses
+import time
+
+import numpy as np
+
+from . import synth
+from .mlp import Mlp
+from .wake import WakeBatch
+
+N_FEATURES = 10
+
+
+@dataclasses.dataclass
+class OperatingPoint:
+    case: synth.RotorCase
+    pitch_deg: float
+
+
+ROOT_CUT = 0.2
+
+
+def operating_points(n: int, seed: int, nst: int = 41, wake_steps: int = 36,
+                     dpsi_deg: float = 10.0, U=(5.0, 25.0), pitch=(0.0, 15.0), yaw=(0.0, 30.0),
+                     tsr=(5.0, 9.0), shear: float = 0.0):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for k in range(n):
+        u = float(rng.uniform(*U))
+        omega = float(rng.uniform(*tsr)) * u / 63.0
+        c = synth.RotorCase(nst=nst, nsteps=wake_steps, dpsi_deg=dpsi_deg, U=u,
+                            omega_rpm=omega * 60.0 / (2.0 * np.pi),
+                            yaw_deg=float(rng.uniform(*yaw)), shear=shear,
+                            seed=seed * 10007 + k, jitter=0.0)
+        out.append(OperatingPoint(c, float(rng.uniform(*pitch))))
+    return out
+
+
+def build(points, run_steps: int):
+    """Wake and lifting-line inputs of every point for ``run_steps`` steps."""
+    cases, kjs = [], []
+    for p in points:
+        cases.append(synth.make_wake_case(p.case, nsteps=run_steps + 1, pitch_deg=p.pitch_deg))
+        kjs.append(synth.make_kj_case(p.case, nsteps=run_steps + 1, pitch_deg=p.pitch_deg,
+                                      root_cut=ROOT_CUT))
+    return cases, kjs
+
+
+def run(points, run_steps: int, relax=0.3, tol=1e-6, maxiter=100, mlp=None, precision="f32c",
+        record=False, graph=True):
+    """Runs every point for ``run_steps`` pcc steps with the lifting line.
+    Returns per-step, per-case iterations, the lifting-line evaluations per
+    step (the batch iterates until its slowest case converged), the bound
+    circulation after every step and, with ``record``, the training pairs."""
+    cases, kjs = build(points, run_steps)
+    b = WakeBatch(cases, integrator="pcc", precision=precision)
+    b.set_kj(kjs, relax=relax, tol=tol, maxiter=maxiter)
+    if mlp is not None:
+        b.set_mlp(mlp)
+    n = len(points)
+    lifting = [kj["foil"] == 0 for kj in kjs]  # stations with the lifting polar
+    aoa_max = np.zeros(n)
+    iters = np.zeros((run_steps, n), dtype=np.int64)
+    evals = np.zeros(run_steps, dtype=np.int64)
+    bounds = []
+    X, dG, tag = [], [], []
+    t0 = time.perf_counter()
+    for s in range(run_steps):
+        b.step(1, graph=graph)
+        it, _, ev = b.kj_stats()
+        iters[s] = it
+        evals[s] = ev
+        conv = [b.bound(k) for k in range(n)]
+        for k in range(n):
+            aoa = b.perf(k)[2]
+            aoa_max[k] = max(aoa_max[k], float(np.nanmax(np.abs(aoa[lifting[k]]))))
+        if record:
+            for k in range(n):
+                if it[k] < maxiter:  # converged pairs only
+                    x = b.kj_features(k)
+                    X.append(x)
+                    dG.append(conv[k].ravel(order="F") - x[:, 8].astype(np.float64))
+                    tag.append(np.full((x.shape[0], 2), (s, k), dtype=np.int32))
+        bounds.append(conv)
+    wall = time.perf_counter() - t0
+    b.close()
+    out = dict(iters=iters, evals=evals, bounds=bounds, wall_s=wall, aoa_max=aoa_max)
+    if record:
+        out["X"] = np.concatenate(X).astype(np.float32) if X else np.zeros((0, N_FEATURES), np.float32)
+        out["dG"] = np.concatenate(dG).astype(np.float32) if dG else np.zeros(0, np.float32)
+        out["step_case"] = np.concatenate(tag) if tag else np.zeros((0, 2), np.int32)
+    return out
+
+
+def attached(points, run_steps=12, stall_deg=12.0, **kw):
+    """The points whose plain solution keeps every lifting station below
+    stall (|AoA| < stall_deg): there the fixed point is unique, so the start
+    value changes iterations but not the converged circulation. (The
+    synthetic polar drops from 1.28 to 0.49 at 12 deg; a station past it can
+    have two fixed points, and any change of start value may select the
+    other one.)"""
+    r = run(points, run_steps, **kw)
+    return [p for p, a in zip(points, r["aoa_max"]) if a < stall_deg]
+
+
+def train(X, dG, epochs=30, batch=4096, lr=2e-3, seed=0, weight_decay=0.0):
+    """An MLP fitted to dG (the change of the converged bound circulation)
+    from the features X, with standardised inputs and target; Adam with the
+    learning rate stepped down (x1, x1/4, x1/16) over three equal phases."""
+    shift = X.mean(0)
+    sd = X.std(0)
+    scale = np.where(sd > 0, 1.0 / np.maximum(sd, 1e-12), 1.0).astype(np.float32)
+    out_scale = float(max(dG.std(), 1e-12))
+    m = Mlp(N_FEATURES, seed=seed)
+    m.set_scaling(shift.astype(np.float32), scale, out_scale)
+    losses = []
+    per = [epochs - 2 * (epochs // 3), epochs // 3, epochs // 3]
+    for k, (ep, f) in enumerate(zip(per, (1.0, 0.25, 0.0625))):
+        if ep > 0:
+            losses.append(m.train(X, dG / out_scale, epochs=ep, batch=batch, lr=lr * f,
+                                  seed=seed + 1 + k, weight_decay=weight_decay))
+    return m, np.concatenate(losses) if losses else np.zeros(0)
+
+
+def study(n_train: int = 400, n_test: int = 120, train_steps: int = 42, test_steps: int = 30,
+          skip: int = 4, epochs: int = 60, relax: float = 0.3, tol: float = 1e-6,
+          maxiter: int = 200, seed: int = 1, precision: str = "f32c"):
+    """Trains the start value on the attached-flow points among ``n_train``
+    seeded candidates (pairs from steps >= ``skip``, past the start-up
+    transient of the synthetic initial circulation) and compares the
+    iteration with and without it on the attached points among ``n_test``
+    other candidates. Returns a dict of the measurements."""
+    t0 = time.perf_counter()
+    kw = dict(relax=relax, tol=tol, maxiter=maxiter, precision=precision)
+    train_pts = attached(operating_points(n_train, seed=seed), **kw)
+    d = run(train_pts, train_steps, record=True, **kw)
+    keep = d["step_case"][:, 0] >= skip
+    t1 = time.perf_counter()
+    m, losses = train(d["X"][keep], d["dG"][keep], epochs=epochs, seed=seed)
+    t2 = time.perf_counter()
+    test_pts = attached(operating_points(n_test, seed=seed + 1), **kw)
+    a = run(test_pts, test_steps, **kw)
+    b = run(test_pts, test_steps, mlp=m, **kw)
+    ia, ib = a["iters"], b["iters"]
+    rel = [float(np.abs(np.asarray(x) - np.asarray(y)).max() / (np.abs(np.asarray(x)).max() + 1.0))
+           for x, y in zip(a["bounds"][-1], b["bounds"][-1])]
+    ms, nsteps = m.train_stats()
+    return dict(
+        model=m, train_points=len(train_pts), test_points=len(test_pts),
+        pairs=int(keep.sum()), loss_first=float(losses[0]), loss_last=float(losses[-1]),
+        data_s=t1 - t0, train_s=t2 - t1, train_device_ms=ms, adam_steps=nsteps,
+        iters_plain=int(ia.sum()), iters_mlp=int(ib.sum()),
+        iters_plain_steady=int(ia[skip:].sum()), iters_mlp_steady=int(ib[skip:].sum()),
+        evals_plain=int(a["evals"].sum()), evals_mlp=int(b["evals"].sum()),
+        converged_plain=float((ia < maxiter).mean()), converged_mlp=float((ib < maxiter).mean()),
+        saved=1.0 - ib.sum() / max(ia.sum(), 1), saved_steady=1.0 - ib[skip:].sum() / max(ia[skip:].sum(), 1),
+        cases_improved=int((ib.sum(0) < ia.sum(0)).sum()),
+        bound_rel_diff_max=max(rel) if rel else 0.0,
+        bound_rel_diff_median=float(np.median(rel)) if rel else 0.0,
+        wall_plain_s=a["wall_s"], wall_mlp_s=b["wall_s"])

@@ -259,7 +259,7 @@ def blade_nodes(case: RotorCase, t: float, pitch_deg: float = 0.0):
 
 
 def make_wake_case(case: RotorCase, nsteps: int, t0: float = 0.0, jitter: float = 0.0,
-                   a1: float = 0.0) -> dict:
+                   a1: float = 0.0, pitch_deg: float = 0.0) -> dict:
     """Initial state, kinematics and wind of one rotor for the device time step.
 
     The wake keeps ``na = case.nsteps + 1`` age columns: column 0 the
@@ -272,13 +272,13 @@ def make_wake_case(case: RotorCase, nsteps: int, t0: float = 0.0, jitter: float 
     quarter = np.zeros((nst, 3, nsteps, nb))
     trailing = np.zeros((nst, 3, nsteps, nb))
     for s in range(nsteps):
-        quarter[:, :, s, :], trailing[:, :, s, :] = blade_nodes(case, t0 + s * dt)
+        quarter[:, :, s, :], trailing[:, :, s, :] = blade_nodes(case, t0 + s * dt, pitch_deg)
     dom = np.zeros((nst, 3, na, nb))
-    q0, te0 = blade_nodes(case, t0)
+    q0, te0 = blade_nodes(case, t0, pitch_deg)
     dom[:, :, 0, :], dom[:, :, 1, :] = q0, te0
     for j in range(2, na):
         age = (j - 1) * dt
-        _, te = blade_nodes(case, t0 - age)
+        _, te = blade_nodes(case, t0 - age, pitch_deg)
         height = case.hub_height + te[:, 2, :]
         speed = case.U * np.power(np.maximum(height, 1.0) / case.hub_height, case.shear)
         te[:, 0, :] += speed * age
@@ -334,7 +334,8 @@ def synthetic_polar(step_deg: float = 0.25):
     return a, cl, cd
 
 
-def make_kj_case(case: RotorCase, nsteps: int, t0: float = 0.0, pitch_deg: float = 0.0) -> dict:
+def make_kj_case(case: RotorCase, nsteps: int, t0: float = 0.0, pitch_deg: float = 0.0,
+                 root_cut: float = 0.0) -> dict:
     """Lifting-line inputs of ``core/KuttaJoukowski.m:173-298`` for every step:
     ``ll`` (pos.bound: quarter-chord midpoints), blade-frame unit vectors
     ``bxn`` (chord, leading to trailing edge), ``byn``, ``bzn`` (radial), the
@@ -379,8 +380,40 @@ def make_kj_case(case: RotorCase, nsteps: int, t0: float = 0.0, pitch_deg: float
         out["vblade"][:, :, st, :] = np.stack([(wr * bx).sum(-1), (wr * by).sum(-1),
                                                (wr * bz).sum(-1)], axis=1)
     a, cl, cd = synthetic_polar()
+    foil = np.zeros(ns, dtype=np.int32)
+    foil_points = [a.size]
+    if root_cut > 0:
+        # cylindrical root sections (no lift, Cd 0.5) inside r/R < root_cut
+        foil[rm / case.R < root_cut] = 1
+        ac = np.array([-180.0, 180.0])
+        a, cl, cd = np.concatenate([a, ac]), np.concatenate([cl, [0.0, 0.0]]), np.concatenate([cd, [0.5, 0.5]])
+        foil_points.append(2)
     f = np.asfortranarray
     res = {k: f(v) for k, v in out.items()}
-    res.update(chord=chord, foil=np.zeros(ns, dtype=np.int32), foil_points=np.array([a.size], dtype=np.int32),
-               aoa=a, cl=cl, cd=cd, twist_deg=np.degrees(th), r_over_R=rm / case.R)
+    steps = t0 + case.dt * np.arange(nsteps)
+    azimuth = 2.0 * np.pi * np.arange(nb)[None, :] / nb + case.omega * steps[:, None]  # [nsteps, nb]
+    res.update(chord=chord, foil=foil, foil_points=np.array(foil_points, dtype=np.int32),
+               aoa=a, cl=cl, cd=cd, twist_deg=np.degrees(th), r_over_R=rm / case.R,
+               chord_over_R=chord / case.R, twist=th.copy(), azimuth=f(azimuth))
     return res
+
+
+def kj_features(kj: dict, s: int, bound, bound_last=None, uind=None) -> np.ndarray:
+    """Inputs of the bound-circulation MLP at step ``s`` (rows i + ns*b), the
+    device's feature order, as float32: r/R, chord/R, twist, sin/cos azimuth,
+    local inflow in the blade frame (vblade plus ``uind`` [ns,3,nb], the
+    previous step's induced velocity at the lifting line, rotated with
+    bxn/byn/bzn; zero when None), bound circulation and its change since
+    ``bound_last`` (zero when None)."""
+    ns, _, _, nb = kj["vblade"].shape
+    az = kj["azimuth"][s]                                   # [nb]
+    vb = kj["vblade"][:, :, s, :].copy()                    # [ns, 3, nb]
+    if uind is not None:
+        for a, key in enumerate(("bxn", "byn", "bzn")):
+            vb[:, a, :] += (kj[key][:, :, s, :] * uind).sum(1)
+    bound = np.asarray(bound, dtype=np.float64)
+    d = bound - (np.asarray(bound_last) if bound_last is not None else bound)
+    cols = [np.repeat(kj["r_over_R"][:, None], nb, 1), np.repeat(kj["chord_over_R"][:, None], nb, 1),
+            np.repeat(kj["twist"][:, None], nb, 1), np.repeat(np.sin(az)[None, :], ns, 0),
+            np.repeat(np.cos(az)[None, :], ns, 0), vb[:, 0], vb[:, 1], vb[:, 2], bound, d]
+    return np.stack([c.ravel(order="F") for c in cols], axis=1).astype(np.float32)

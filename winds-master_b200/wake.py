@@ -31,7 +31,8 @@ class KJCaseC(C.Structure):
     _fields_ = [("ll", C.c_void_p), ("bxn", C.c_void_p), ("byn", C.c_void_p), ("bzn", C.c_void_p),
                 ("vblade", C.c_void_p), ("chord", C.c_void_p), ("foil", C.c_void_p),
                 ("n_foils", C.c_int), ("foil_points", C.c_void_p), ("aoa", C.c_void_p),
-                ("cl", C.c_void_p), ("cd", C.c_void_p)]
+                ("cl", C.c_void_p), ("cd", C.c_void_p), ("r_over_R", C.c_void_p),
+                ("chord_over_R", C.c_void_p), ("twist", C.c_void_p), ("azimuth", C.c_void_p)]
 
 
 class KJParamsC(C.Structure):
@@ -58,6 +59,9 @@ def _bind():
         L.winds_wake_set_kj.argtypes = [C.c_void_p, C.POINTER(KJCaseC), C.POINTER(KJParamsC)]
         L.winds_wake_kj_stats.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_longlong)]
         L.winds_wake_get_perf.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.winds_wake_set_mlp.argtypes = [C.c_void_p, C.c_void_p]
+        L.winds_wake_get_kj_guess.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        L.winds_wake_get_kj_features.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         L._wake_bound = True
     return L
 
@@ -102,6 +106,14 @@ class WakeBatch:
         _check(_bind().winds_wake_get_state(self.h, i, *[out[k].ctypes.data for k in ks]))
         return out
 
+    def bound(self, i):
+        """Bound circulation [ns, nb] of case ``i``."""
+        c = self.cases[i]
+        g = np.zeros((c["nst"] - 1, c["nb"]), order="F")
+        _check(_bind().winds_wake_get_state(self.h, i, None, g.ctypes.data, None, None, None, None,
+                                            None))
+        return g
+
     def set_bound(self, i, bound):
         b = np.asfortranarray(bound, dtype=np.float64)
         _check(_bind().winds_wake_set_bound(self.h, i, b.ctypes.data))
@@ -121,8 +133,33 @@ class WakeBatch:
                 self._keep.append(x)
                 setattr(a, f, x.ctypes.data)
             a.n_foils = len(j["foil_points"])
+            for f in ("r_over_R", "chord_over_R", "twist", "azimuth"):  # MLP inputs, optional
+                if f in j:
+                    x = np.asfortranarray(j[f], dtype=np.float64)
+                    self._keep.append(x)
+                    setattr(a, f, x.ctypes.data)
         p = KJParamsC(float(relax), float(tol), int(maxiter))
         _check(_bind().winds_wake_set_kj(self.h, arr, C.byref(p)))
+
+    def set_mlp(self, mlp):
+        """Start every later step's iteration from ``mlp``'s prediction
+        (``None``: from the previous step's bound circulation)."""
+        _check(_bind().winds_wake_set_mlp(self.h, mlp.h if mlp is not None else None))
+        self._mlp = mlp  # the network must outlive its use
+
+    def kj_guess(self, i):
+        """Start value [ns, nb] of case ``i``'s last iteration."""
+        c = self.cases[i]
+        g = np.zeros((c["nst"] - 1, c["nb"]), order="F")
+        _check(_bind().winds_wake_get_kj_guess(self.h, i, g.ctypes.data))
+        return g
+
+    def kj_features(self, i):
+        """MLP features [ns*nb, 10] of case ``i`` at the last step."""
+        c = self.cases[i]
+        x = np.zeros(((c["nst"] - 1) * c["nb"], 10), dtype=np.float32)
+        _check(_bind().winds_wake_get_kj_features(self.h, i, x.ctypes.data))
+        return x
 
     def kj_stats(self):
         """(iterations [ncases], residual [ncases], lifting-line evaluations)
