@@ -123,6 +123,12 @@ typedef struct {
   const double *chord_over_R; /* [ns] chord / rotor radius                        */
   const double *twist;        /* [ns] local pitch (twist + blade pitch), rad      */
   const double *azimuth;      /* [nsteps,nb] blade azimuth per step, rad          */
+  /* Rotor loads (optional; with twist, enables winds_wake_get_loads):
+   * postproc/perform.m:18-62 per step. */
+  const double *r_station;    /* [ns] station radius (blade.RNodes), m             */
+  const double *dr_station;   /* [ns] station width (blade.DRNodes), m             */
+  const double *rpm;          /* [nsteps] rotor speed (fastout.RotSpeed), rpm      */
+  double rho;                 /* air density (const.rho), kg/m^3                  */
 } winds_kj_case;
 
 typedef struct {
@@ -156,6 +162,11 @@ int winds_wake_get_perf(winds_wake_batch *b, int icase, double *cl, double *cd, 
  * previous step). */
 struct winds_mlp;
 int winds_wake_set_mlp(winds_wake_batch *b, struct winds_mlp *m);
+
+/* Rotor thrust (N), torque (N m) and power (W) of every case at the last step
+ * (arrays of ncases; any may be NULL), from the converged Cl, Cd and AoA as
+ * postproc/perform.m computes them. */
+int winds_wake_get_loads(winds_wake_batch *b, double *thrust, double *torque, double *power);
 
 /* The start value [ns,nb] of the last step's iteration for one case. */
 int winds_wake_get_kj_guess(winds_wake_batch *b, int icase, double *guess);

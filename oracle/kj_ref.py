@@ -85,3 +85,9 @@ class KJWakeRef(wake_ref.WakeRef):
                        self.relax, self.tol, self.maxiter, self.d, self.co)
         self.bound, self.kj_iters, self.kj_res, self.cl, self.cd, self.aoa = out
         self.shed, self.trail = wake_ref.bookkeeping(self.bound, self.trail_prev)
+        kj = self.kj
+        if "r_station" in kj:  # rotor loads of the step (postproc/perform.m)
+            import perform_ref
+            self.T, self.Q, self.P, _ = perform_ref.loads(
+                self.cl, self.cd, self.aoa, kj["vblade"][:, :, s, :], np.degrees(kj["twist"]),
+                kj["chord"], kj["r_station"], kj["dr_station"], kj["rpm"][s], kj["rho"])

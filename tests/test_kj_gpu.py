@@ -39,6 +39,7 @@ def test_kj_step_matches_oracle(wb, synth, prec):
     for step in range(3):
         batch.step(1)
         iters, res, nev = batch.kj_stats()
+        T, Q, P = batch.loads()
         for k, r in enumerate(refs):
             r.step()
             st = batch.state(k)
@@ -58,6 +59,15 @@ def test_kj_step_matches_oracle(wb, synth, prec):
                 assert abs(int(iters[k]) - r.kj_iters) <= 1, (step, k, iters[k], r.kj_iters)
                 np.testing.assert_allclose(st["bound"], r.bound, rtol=0, atol=5 * tol * scale)
                 np.testing.assert_allclose(aoa, r.aoa, rtol=0, atol=1e-3)
+            # rotor loads of the step (postproc/perform.m) at the run tolerance
+            import perform_ref
+            Td, Qd, Pd, _ = perform_ref.loads(cl, cd, aoa, cases[k][1]["vblade"][:, :, step, :],
+                                             np.degrees(cases[k][1]["twist"]), cases[k][1]["chord"],
+                                             cases[k][1]["r_station"], cases[k][1]["dr_station"],
+                                             cases[k][1]["rpm"][step], cases[k][1]["rho"])
+            # the device formula on the device's own Cl, Cd, AoA: same arithmetic
+            assert abs(T[k] - Td) <= 1e-9 * abs(Td) and abs(P[k] - Pd) <= 1e-9 * abs(Pd)
+            assert abs(T[k] - r.T) <= 1e-4 * abs(r.T) and abs(P[k] - r.P) <= 1e-4 * abs(r.P), (T[k], r.T, P[k], r.P)
             # the step's Γ is re-formed from the converged bound (kj(), :285-288)
             np.testing.assert_allclose(st["shed"][:, 0], st["bound"], rtol=0, atol=0)
             # carrying the state on: compare on the oracle's own trajectory

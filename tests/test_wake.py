@@ -102,3 +102,31 @@ def test_kj_oracle_fixed_point(synth):
                foil_points=np.array([2], dtype=np.int32))
     with pytest.raises(kj_ref.KJDiverged):
         kj_ref.kj_solve(bad, 0, c["dom"], ref.trail_prev, ref.rcs, ref.rct, ref.bound)
+
+
+def test_perform_oracle_rotation_and_totals():
+    """perform.m's 'zzz' DCMRot sequence [-90, twist, pitch] equals one z
+    rotation by twist + pitch - 90 (core/DCMRot.m:27-45); totals sum every
+    station and blade; a station with zero Cl and Cd carries no load."""
+    import perform_ref
+
+    def dcm(seq_deg):  # DCMRot: A <- R A for each rotation, y = A x
+        A = np.eye(3)
+        for t in seq_deg:
+            A = perform_ref.rz(t) @ A
+        return A
+
+    for tw, pitch in ((5.0, 2.0), (-3.0, 17.5), (13.0, 0.0)):
+        np.testing.assert_allclose(dcm([-90.0, tw, pitch]), perform_ref.rz(tw + pitch - 90.0), atol=1e-15)
+    rng = np.random.default_rng(0)
+    ns, nb = 5, 3
+    vb = rng.normal(0, 1, (ns, 3, nb)) + np.array([[[-9.0], [-40.0], [0.0]]])
+    cl, cd, aoa = rng.uniform(0.2, 1.2, (ns, nb)), rng.uniform(0.01, 0.05, (ns, nb)), rng.uniform(2, 10, (ns, nb))
+    th = rng.uniform(0, 10, ns)
+    chord, r, dr = np.full(ns, 2.0), np.linspace(10, 60, ns), np.full(ns, 10.0)
+    T, Q, P, dT = perform_ref.loads(cl, cd, aoa, vb, th, chord, r, dr, 12.1, 1.225)
+    assert abs(T - dT.sum()) < 1e-9 * abs(T)
+    assert abs(P - np.pi / 30 * 12.1 * Q) < 1e-9 * abs(P)
+    cl[2, 1] = cd[2, 1] = 0.0
+    _, _, _, dT0 = perform_ref.loads(cl, cd, aoa, vb, th, chord, r, dr, 12.1, 1.225)
+    assert dT0[2, 1] == 0.0

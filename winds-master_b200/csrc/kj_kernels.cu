@@ -7,6 +7,7 @@
 //   kj_check     per case: converged when max |residual| <= tol (:45)
 //   kj_features, kj_apply_guess   inputs and result of the bound-circulation
 //                MLP that replaces the previous-step start value (WInDS.m:131)
+//   kj_loads     rotor thrust, torque and power (postproc/perform.m:18-62)
 #include <cmath>
 
 #include "bs_device.cuh"
@@ -135,6 +136,69 @@ __global__ void kj_apply_guess(const WakeCase *cases, const KJCase *kc, const fl
   bound[c.bound_off + i + (long long)ns * b] += (double)out_scale * (double)y[k.t_off + t];
 }
 
+// Spanwise loads of one station (postproc/perform.m:20-55): the blade-frame
+// velocity to the rotor frame, velX = -Rz(theta - 90 deg) vblade with theta =
+// twist + pitch (DCMRot with the 'zzz' sequence [-90, twist, pitch]); inflow
+// angle phi = aoa - theta; a/a' = TSR / tan(phi); a and a'; normal and
+// tangential coefficients; dT, dQ, dP.
+__global__ void kj_dloads(const WakeCase *cases, const KJCase *kc, const int *step,
+                          const double *vblade, const double *cl, const double *cd,
+                          const double *aoa, const double *st_tw, const double *chord,
+                          const double *st_rr, const double *st_dr, const double *rpm,
+                          double *dl) {
+  const WakeCase c = cases[blockIdx.y];
+  const KJCase k = kc[blockIdx.y];
+  const int ns = c.nst - 1;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ns * c.nb) return;
+  const int i = t % ns, b = t / ns;
+  const int s = *step;
+  const long long fo = k.frame_off + i + (long long)ns * (3 * (s + (long long)c.nsteps * b));
+  const long long st = k.station_off + i;
+  const long long q = c.bound_off + i + (long long)ns * b;
+  const double th = st_tw[st] * (180.0 / kPi);  // deg
+  const double rot = (th - 90.0) * (kPi / 180.0);
+  const double cr = cos(rot), sr = sin(rot);
+  const double u0 = vblade[fo], u1 = vblade[fo + ns];
+  const double v1 = -(cr * u0 - sr * u1);
+  const double v2 = -(sr * u0 + cr * u1);
+  const double tsr = v2 / v1;
+  const double phi = aoa[q] - th;
+  const double pr = phi * (kPi / 180.0);
+  const double tp = tan(pr);
+  const double aap = tsr / tp;
+  const double a = aap * (v1 - tp * v2) / (aap * v1 + tp * v2);
+  const double ap = a / aap;
+  const double cz = cl[q] * cos(pr) + cd[q] * sin(pr);
+  const double cx = cl[q] * sin(pr) - cd[q] * cos(pr);
+  const double w1 = v1 * (1.0 - a), w2 = v2 * (1.0 + ap);
+  const double w = w1 * w1 + w2 * w2;
+  const double dT = 0.5 * k.rho * chord[st] * cz * w * st_dr[st];
+  const double dQ = 0.5 * k.rho * chord[st] * cx * w * st_rr[st] * st_dr[st];
+  double *o = dl + 3 * (k.t_off + t);
+  o[0] = dT;
+  o[1] = dQ;
+  o[2] = (kPi / 30.0) * rpm[k.rpm_off + s] * dQ;
+}
+
+// Rotor totals, summed over stations and then blades as sum(sum(dT,1),4).
+__global__ void kj_sum_loads(const WakeCase *cases, const KJCase *kc, int ncases,
+                             const double *dl, double *out) {
+  const int ci = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ci >= ncases) return;
+  const WakeCase c = cases[ci];
+  const KJCase k = kc[ci];
+  const int ns = c.nst - 1;
+  double tot[3] = {0.0, 0.0, 0.0};
+  for (int b = 0; b < c.nb; ++b) {
+    double sb[3] = {0.0, 0.0, 0.0};
+    for (int i = 0; i < ns; ++i)
+      for (int a = 0; a < 3; ++a) sb[a] += dl[3 * (k.t_off + i + (long long)ns * b) + a];
+    for (int a = 0; a < 3; ++a) tot[a] += sb[a];
+  }
+  for (int a = 0; a < 3; ++a) out[3 * ci + a] = tot[a];
+}
+
 // One thread per case: a case converged in this iteration stops updating.
 __global__ void kj_check(int ncases, double tol, int *converged, int *iters,
                          unsigned long long *res_max, double *res_last, int *active) {
@@ -185,6 +249,19 @@ cudaError_t launch_kj_features(const WakeCase *cases, const KJCase *kc, int ncas
 cudaError_t launch_kj_apply_guess(const WakeCase *cases, const KJCase *kc, int ncases, int max_st,
                                   const float *y, float out_scale, double *bound, cudaStream_t s) {
   kj_apply_guess<<<dim3((max_st + 127) / 128, ncases), 128, 0, s>>>(cases, kc, y, out_scale, bound);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_kj_loads(const WakeCase *cases, const KJCase *kc, int ncases, int max_st,
+                            const int *step, const double *vblade, const double *cl,
+                            const double *cd, const double *aoa, const double *st_tw,
+                            const double *chord, const double *st_rr, const double *st_dr,
+                            const double *rpm, double *dl, double *out, cudaStream_t s) {
+  kj_dloads<<<dim3((max_st + 127) / 128, ncases), 128, 0, s>>>(
+      cases, kc, step, vblade, cl, cd, aoa, st_tw, chord, st_rr, st_dr, rpm, dl);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  kj_sum_loads<<<(ncases + 127) / 128, 128, 0, s>>>(cases, kc, ncases, dl, out);
   return cudaGetLastError();
 }
 

@@ -13,6 +13,8 @@ struct KJCase {
   long long t_off;        // first lifting-line target (ns*nb per case)
   long long station_off;  // first station (ns per case): chord, foil
   long long az_off;       // nsteps*nb per case: blade azimuth (MLP features)
+  long long rpm_off;      // nsteps per case: rotor speed (loads)
+  double rho;             // air density (loads)
   int foil_base;          // this case's first entry in the foil offset table
   int n_foils;
 };
@@ -45,6 +47,14 @@ cudaError_t launch_kj_features(const WakeCase *cases, const KJCase *kc, int ncas
 // bound += out_scale * y (row order of the lifting-line targets)
 cudaError_t launch_kj_apply_guess(const WakeCase *cases, const KJCase *kc, int ncases, int max_st,
                                   const float *y, float out_scale, double *bound, cudaStream_t s);
+// Rotor thrust, torque and power of every case at the step
+// (postproc/perform.m:18-62): out[3*case + {0,1,2}] = T, Q, P; dl [rows][3]
+// holds the spanwise terms.
+cudaError_t launch_kj_loads(const WakeCase *cases, const KJCase *kc, int ncases, int max_st,
+                            const int *step, const double *vblade, const double *cl,
+                            const double *cd, const double *aoa, const double *st_tw,
+                            const double *chord, const double *st_rr, const double *st_dr,
+                            const double *rpm, double *dl, double *out, cudaStream_t s);
 cudaError_t launch_kj_check(int ncases, double tol, int *converged, int *iters,
                             unsigned long long *res_max, double *res_last, int *active,
                             cudaStream_t s);

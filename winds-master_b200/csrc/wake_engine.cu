@@ -68,6 +68,8 @@ struct winds_wake_batch {
   long long kj_evals = 0;
   // bound-circulation MLP start value
   bool mlp_inputs = false;      // every case gave the station arrays
+  bool loads = false;           // every case gave the loads inputs
+  DevBuf st_rr, st_dr, rpm, dl, loads_out;
   DevBuf st_r, st_c, st_tw, azim, guess, feat, bound_last;
   winds_mlp *mlp = nullptr;
   MlpWork mw;
@@ -298,6 +300,16 @@ cudaError_t enqueue_post(winds_wake_batch *b, int &launches) {
                              P<const double>(b->trail_prev), P<double>(b->shed_cur),
                              P<double>(b->trail_cur), s);
     ++launches;
+    if (e == cudaSuccess && b->loads) {
+      e = launch_kj_loads(cd, P<const KJCase>(b->kjc_d), b->ncases, b->max_st,
+                          P<const int>(b->step_d), P<const double>(b->vblade),
+                          P<const double>(b->cl_o), P<const double>(b->cd_o),
+                          P<const double>(b->aoa_o), P<const double>(b->st_tw),
+                          P<const double>(b->chord), P<const double>(b->st_rr),
+                          P<const double>(b->st_dr), P<const double>(b->rpm), P<double>(b->dl),
+                          P<double>(b->loads_out), s);
+      launches += 2;
+    }
   }
   const int keep_hist = b->prm.integrator == WINDS_INTEG_AB2 || b->prm.integrator == WINDS_INTEG_AB4;
   if (e == cudaSuccess)
@@ -761,11 +773,17 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
     return fail(WINDS_BS_ERR_ARG, "bad lifting-line arguments");
   if (b->ncases > 1024) return fail(WINDS_BS_ERR_ARG, "at most 1024 cases with lifting lines");
   cudaSetDevice(b->dev);
+  cudaStreamSynchronize(b->stream);
+  // graphs captured for an earlier attachment describe other buffers
+  for (cudaGraphExec_t *x : {&b->exec_pre, &b->exec_kj, &b->exec_post})
+    if (*x) cudaGraphExecDestroy(*x), *x = nullptr;
+  for (cudaGraph_t *x : {&b->g_pre, &b->g_kj, &b->g_post})
+    if (*x) cudaGraphDestroy(*x), *x = nullptr;
   cudaStream_t s = b->stream;
   b->kjp = *prm;
   b->kjc.clear();
-  long long fr = 0, tt = 0, st = 0, tab = 0, az = 0;
-  bool all_inputs = true;
+  long long fr = 0, tt = 0, st = 0, tab = 0, az = 0, rp = 0;
+  bool all_inputs = true, have_twist = true, all_loads = true;
   std::vector<int> foil_off, foils;
   std::vector<double> aoa, cl, cd, chord;
   b->max_st = 0;
@@ -782,6 +800,10 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
     q.station_off = st;
     q.az_off = az;
     if (!h.r_over_R || !h.chord_over_R || !h.twist || !h.azimuth) all_inputs = false;
+    if (!h.twist) have_twist = false;
+    if (!h.r_station || !h.dr_station || !h.rpm || !(h.rho > 0)) all_loads = false;
+    q.rpm_off = rp;
+    q.rho = h.rho;
     q.foil_base = (int)foil_off.size();
     q.n_foils = h.n_foils;
     long long o = 0;
@@ -804,6 +826,7 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
     }
     tab += o;
     az += (long long)c.nsteps * c.nb;
+    rp += c.nsteps;
     fr += (long long)ns * 3 * c.nsteps * c.nb;
     tt += (long long)ns * c.nb;
     st += ns;
@@ -830,14 +853,42 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
                                   cudaMemcpyDeviceToDevice);
       e0 != cudaSuccess)
     return cuda_fail(e0, "bound copy");
+  all_loads = all_loads && have_twist;
   b->mlp_inputs = all_inputs;
+  b->loads = all_loads;
+  if (have_twist) {
+    if ((rc = b->st_tw.ensure(st * sizeof(double), s))) return rc;
+    for (int k = 0; k < b->ncases; ++k) {
+      cudaError_t e2 = cudaMemcpy(P<double>(b->st_tw) + b->kjc[k].station_off, kj[k].twist,
+                                  (size_t)(b->cases[k].nst - 1) * 8, cudaMemcpyHostToDevice);
+      if (e2 != cudaSuccess) return cuda_fail(e2, "twist upload");
+    }
+  }
+  if (all_loads) {
+    if ((rc = b->st_rr.ensure(st * sizeof(double), s)) || (rc = b->st_dr.ensure(st * sizeof(double), s)) ||
+        (rc = b->rpm.ensure(rp * sizeof(double), s)) ||
+        (rc = b->dl.ensure(std::max<long long>(tt, 1) * 3 * sizeof(double), s)) ||
+        (rc = b->loads_out.ensure(std::max(b->ncases, 1) * 3 * sizeof(double), s)))
+      return rc;
+    for (int k = 0; k < b->ncases; ++k) {
+      const size_t ns = (size_t)(b->cases[k].nst - 1), so = (size_t)b->kjc[k].station_off;
+      cudaError_t e2 = cudaMemcpy(P<double>(b->st_rr) + so, kj[k].r_station, ns * 8, cudaMemcpyHostToDevice);
+      if (e2 == cudaSuccess) e2 = cudaMemcpy(P<double>(b->st_dr) + so, kj[k].dr_station, ns * 8, cudaMemcpyHostToDevice);
+      if (e2 == cudaSuccess)
+        e2 = cudaMemcpy(P<double>(b->rpm) + b->kjc[k].rpm_off, kj[k].rpm,
+                        (size_t)b->cases[k].nsteps * 8, cudaMemcpyHostToDevice);
+      if (e2 != cudaSuccess) return cuda_fail(e2, "loads upload");
+    }
+    if (cudaError_t e0 = cudaMemset(b->loads_out.p, 0, b->ncases * 3 * sizeof(double)); e0 != cudaSuccess)
+      return cuda_fail(e0, "loads reset");
+  }
   // no induced velocity at the lifting line before the first step
   if (cudaError_t e0 = cudaMemset(b->uindb.p, 0, tt * 3 * sizeof(double)); e0 != cudaSuccess)
     return cuda_fail(e0, "lifting-line reset");
   if (all_inputs) {
     if ((rc = b->feat.ensure(std::max<long long>(tt, 1) * kKJFeatures * sizeof(float), s))) return rc;
     if ((rc = b->st_r.ensure(st * sizeof(double), s)) || (rc = b->st_c.ensure(st * sizeof(double), s)) ||
-        (rc = b->st_tw.ensure(st * sizeof(double), s)) || (rc = b->azim.ensure(az * sizeof(double), s)))
+        (rc = b->azim.ensure(az * sizeof(double), s)))
       return rc;
     for (int k = 0; k < b->ncases; ++k) {
       const WakeCase &c = b->cases[k];
@@ -845,7 +896,6 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
       const size_t so = (size_t)b->kjc[k].station_off, ao = (size_t)b->kjc[k].az_off;
       cudaError_t e2 = cudaMemcpy(P<double>(b->st_r) + so, kj[k].r_over_R, ns * 8, cudaMemcpyHostToDevice);
       if (e2 == cudaSuccess) e2 = cudaMemcpy(P<double>(b->st_c) + so, kj[k].chord_over_R, ns * 8, cudaMemcpyHostToDevice);
-      if (e2 == cudaSuccess) e2 = cudaMemcpy(P<double>(b->st_tw) + so, kj[k].twist, ns * 8, cudaMemcpyHostToDevice);
       if (e2 == cudaSuccess)
         e2 = cudaMemcpy(P<double>(b->azim) + ao, kj[k].azimuth, (size_t)c.nsteps * c.nb * 8, cudaMemcpyHostToDevice);
       if (e2 != cudaSuccess) return cuda_fail(e2, "mlp station upload");
@@ -953,6 +1003,21 @@ int winds_wake_get_kj_features(winds_wake_batch *b, int icase, float *x) {
   return e == cudaSuccess ? WINDS_BS_OK : cuda_fail(e, "feature read");
 }
 
+int winds_wake_get_loads(winds_wake_batch *b, double *thrust, double *torque, double *power) {
+  if (!b || !b->kj || !b->loads) return fail(WINDS_BS_ERR_ARG, "no loads inputs attached");
+  cudaSetDevice(b->dev);
+  cudaStreamSynchronize(b->stream);
+  std::vector<double> h((size_t)b->ncases * 3);
+  cudaError_t e = cudaMemcpy(h.data(), b->loads_out.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "loads read");
+  for (int k = 0; k < b->ncases; ++k) {
+    if (thrust) thrust[k] = h[3 * k];
+    if (torque) torque[k] = h[3 * k + 1];
+    if (power) power[k] = h[3 * k + 2];
+  }
+  return WINDS_BS_OK;
+}
+
 int winds_wake_get_kj_guess(winds_wake_batch *b, int icase, double *guess) {
   if (!b || !b->kj || icase < 0 || icase >= b->ncases || !guess)
     return fail(WINDS_BS_ERR_ARG, "bad arguments");
@@ -1005,7 +1070,7 @@ void winds_wake_destroy(winds_wake_batch *b) {
                     &b->kj_groups, &b->kj_tiles, &b->kj_items, &b->kj_part, &b->conv, &b->iters,
                     &b->res_max, &b->res_last, &b->active, &b->diverged, &b->cl_o, &b->cd_o,
                     &b->aoa_o, &b->st_r, &b->st_c, &b->st_tw, &b->azim, &b->guess, &b->feat,
-                    &b->bound_last})
+                    &b->bound_last, &b->st_rr, &b->st_dr, &b->rpm, &b->dl, &b->loads_out})
     x->release();
   b->mw.release();
   for (DevBuf *x : {&b->cases_d, &b->step_d, &b->dom, &b->dom_pred, &b->dom_new, &b->vel, &b->h1,

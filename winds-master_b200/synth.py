@@ -29,6 +29,7 @@ import math
 import numpy as np
 
 ALPHA_RL = 1.25643  # Ramasamy-Leishman alpha, core/constants.m:22
+RHO = 1.225  # air density, kg/m^3
 
 
 @dataclasses.dataclass
@@ -394,7 +395,9 @@ def make_kj_case(case: RotorCase, nsteps: int, t0: float = 0.0, pitch_deg: float
     azimuth = 2.0 * np.pi * np.arange(nb)[None, :] / nb + case.omega * steps[:, None]  # [nsteps, nb]
     res.update(chord=chord, foil=foil, foil_points=np.array(foil_points, dtype=np.int32),
                aoa=a, cl=cl, cd=cd, twist_deg=np.degrees(th), r_over_R=rm / case.R,
-               chord_over_R=chord / case.R, twist=th.copy(), azimuth=f(azimuth))
+               chord_over_R=chord / case.R, twist=th.copy(), azimuth=f(azimuth),
+               r_station=rm.copy(), dr_station=np.diff(r), rpm=np.full(nsteps, case.omega_rpm),
+               rho=RHO)
     return res
 
 

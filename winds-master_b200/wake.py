@@ -32,7 +32,9 @@ class KJCaseC(C.Structure):
                 ("vblade", C.c_void_p), ("chord", C.c_void_p), ("foil", C.c_void_p),
                 ("n_foils", C.c_int), ("foil_points", C.c_void_p), ("aoa", C.c_void_p),
                 ("cl", C.c_void_p), ("cd", C.c_void_p), ("r_over_R", C.c_void_p),
-                ("chord_over_R", C.c_void_p), ("twist", C.c_void_p), ("azimuth", C.c_void_p)]
+                ("chord_over_R", C.c_void_p), ("twist", C.c_void_p), ("azimuth", C.c_void_p),
+                ("r_station", C.c_void_p), ("dr_station", C.c_void_p), ("rpm", C.c_void_p),
+                ("rho", C.c_double)]
 
 
 class KJParamsC(C.Structure):
@@ -62,6 +64,7 @@ def _bind():
         L.winds_wake_set_mlp.argtypes = [C.c_void_p, C.c_void_p]
         L.winds_wake_get_kj_guess.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         L.winds_wake_get_kj_features.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        L.winds_wake_get_loads.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L._wake_bound = True
     return L
 
@@ -133,11 +136,13 @@ class WakeBatch:
                 self._keep.append(x)
                 setattr(a, f, x.ctypes.data)
             a.n_foils = len(j["foil_points"])
-            for f in ("r_over_R", "chord_over_R", "twist", "azimuth"):  # MLP inputs, optional
+            # MLP and loads inputs, optional
+            for f in ("r_over_R", "chord_over_R", "twist", "azimuth", "r_station", "dr_station", "rpm"):
                 if f in j:
                     x = np.asfortranarray(j[f], dtype=np.float64)
                     self._keep.append(x)
                     setattr(a, f, x.ctypes.data)
+            a.rho = float(j.get("rho", 0.0))
         p = KJParamsC(float(relax), float(tol), int(maxiter))
         _check(_bind().winds_wake_set_kj(self.h, arr, C.byref(p)))
 
@@ -153,6 +158,14 @@ class WakeBatch:
         g = np.zeros((c["nst"] - 1, c["nb"]), order="F")
         _check(_bind().winds_wake_get_kj_guess(self.h, i, g.ctypes.data))
         return g
+
+    def loads(self):
+        """Rotor thrust (N), torque (N m), power (W) of every case at the last
+        step (postproc/perform.m)."""
+        n = len(self.cases)
+        T, Q, P = np.zeros(n), np.zeros(n), np.zeros(n)
+        _check(_bind().winds_wake_get_loads(self.h, T.ctypes.data, Q.ctypes.data, P.ctypes.data))
+        return T, Q, P
 
     def kj_features(self, i):
         """MLP features [ns*nb, 10] of case ``i`` at the last step."""
