@@ -51,7 +51,11 @@ def parse():
     ap.add_argument("--wake-steps", type=int, default=3,
                     help="timed pcc steps of the 64-case batched wake (0: skip)")
     ap.add_argument("--quick", action="store_true",
-                    help="timed loop only (no FP64 comparison, e2e or CPU baseline)")
+                    help="timed loop only (no FP64 comparison, e2e, CPU baseline or studies)")
+    ap.add_argument("--no-studies", action="store_true",
+                    help="skip the start-value study and the end-to-end run")
+    ap.add_argument("--e2e-steps", type=int, default=3,
+                    help="pcc steps of the 16-case end-to-end run (each path)")
     return ap.parse_args()
 
 
@@ -130,6 +134,20 @@ def workload(seed, kind="large"):
     P = np.asfortranarray(pts.reshape(-1, 3, 1, 1))
     nf = sum(f[0].shape[0] * f[0].shape[2] * f[0].shape[3] for f in fams)
     return w, fams, P, nf, P.shape[0]
+
+
+def profiled_traffic(interactions):
+    """DRAM bytes per launch of bs_f32c from the committed ncu summary
+    (dram__bytes_read.sum + dram__bytes_write.sum of one captured launch),
+    scaled to this launch by interactions; None without a summary."""
+    path = os.path.join(ROOT, "profiles", "bs_f32c_large.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("traffic_bytes_per_launch:"):
+            b, n = line.split(":", 1)[1].split()[:2]
+            return float(b) * interactions / float(n)
+    return None
 
 
 def cpu_rate(fams, P, n_targets, seed=0):
@@ -212,6 +230,81 @@ def wake_bench(args, seed=2, ncases=64):
             "plain_fp64_steps_per_s": 1000.0 / plain_ms,
             "speedup_vs_plain_fp64": plain_ms / ms,
             "nodes": int(sum(c["nst"] * c["na"] * c["nb"] for c in cases))}
+
+
+# ------------------------------------------------------------------ start value
+def kj_mlp_bench():
+    """Learned Kutta-Joukowski start value: pairs from the plain solver on the
+    attached-flow points among 800 seeded operating points (U 5-25 m/s, pitch
+    0-15 deg, yaw 0-30 deg, TSR 5-9, 10 deg steps), trained on the GPU, then
+    iterations with and without it at tol 1e-6 on held-out points."""
+    gi = importlib.import_module("winds-master_b200.gamma_init")
+    r = gi.study(n_train=800, n_test=120, epochs=60)
+    r.pop("model").close()
+    return {k: (round(v, 6) if isinstance(v, float) else v) for k, v in r.items()}
+
+
+# ------------------------------------------------------------------ end to end
+def e2e_run_bench(steps, ncases=16, ages=1440, seed=5):
+    """16 rotor cases, 3 blades x 41 nodes, wake truncated at 1440 steps of
+    1 deg, U = 11.4 m/s, shear 0.2, yaw 0-30 deg, pcc with the lifting-line
+    iteration (tol 1e-6) and rotor loads every step: the FP32-compensated
+    batch with graph replay and the MLP start value (trained here on
+    plain-solver pairs of the same conditions with 120-step wakes) against the
+    plain FP64 path (FP64 direct sum, previous-step start, no graphs).
+    Thrust and power histories are compared step by step."""
+    synth = importlib.import_module("winds-master_b200.synth")
+    wake = importlib.import_module("winds-master_b200.wake")
+    gi = importlib.import_module("winds-master_b200.gamma_init")
+    rng = np.random.Generator(np.random.PCG64(seed))
+    yaws = rng.uniform(0.0, 30.0, ncases)
+
+    def points(n_ages, yaw_list, s0):
+        return [gi.OperatingPoint(synth.RotorCase(nst=41, nsteps=n_ages, dpsi_deg=1.0, U=11.4,
+                                                  omega_rpm=12.1, yaw_deg=float(y), shear=0.2,
+                                                  seed=s0 + k, jitter=0.0), 0.0)
+                for k, y in enumerate(yaw_list)]
+
+    t0 = time.perf_counter()
+    tr = gi.run(points(120, rng.uniform(0.0, 30.0, 64), 900), 48, record=True, maxiter=200)
+    keep = tr["step_case"][:, 0] >= 4
+    m, _ = gi.train(tr["X"][keep], tr["dG"][keep], epochs=40)
+    train_s = time.perf_counter() - t0
+    pts = points(ages, yaws, 100)
+    cases, kjs = gi.build(pts, steps + 1)
+    out = {}
+    for name, prec, mlp, graph in (("fast", "f32c", m, True), ("plain_fp64", "f64", None, False)):
+        b = wake.WakeBatch(cases, integrator="pcc", precision=prec)
+        b.set_kj(kjs, relax=0.3, tol=1e-6, maxiter=200)
+        if mlp is not None:
+            b.set_mlp(mlp)
+        T, P, its, ms = [], [], [], []
+        for s in range(steps):
+            b.step(1, graph=graph)
+            t_, _, p_ = b.loads()
+            T.append(t_)
+            P.append(p_)
+            its.append(int(b.kj_stats()[0].sum()))
+            ms.append(b.stats()[0])
+        inter = b.stats()[1]
+        b.close()
+        out[name] = dict(T=np.array(T), P=np.array(P), iters=its, ms=ms, inter=inter)
+    m.close()
+    f, p = out["fast"], out["plain_fp64"]
+    relT = np.abs(f["T"] - p["T"]) / np.abs(p["T"])
+    relP = np.abs(f["P"] - p["P"]) / np.maximum(np.abs(p["P"]), 1e-9 * np.abs(p["T"]))
+    fast_ms, plain_ms = statistics.mean(f["ms"]), statistics.mean(p["ms"])
+    return {"cases": ncases, "nodes_per_case": 41 * (ages + 1) * 3,
+            "filaments_per_case": (40 * (ages + 1) + 41 * ages) * 3, "steps": steps,
+            "steps_per_s": 1000.0 / fast_ms, "plain_fp64_steps_per_s": 1000.0 / plain_ms,
+            "speedup_vs_plain_fp64": plain_ms / fast_ms,
+            "interactions_per_step": f["inter"],
+            "kj_iterations_fast": f["iters"], "kj_iterations_plain": p["iters"],
+            "thrust_rel_diff_max": float(relT.max()), "power_rel_diff_max": float(relP.max()),
+            "thrust_history_N": f["T"].sum(1).round(1).tolist(),
+            "power_history_W": f["P"].sum(1).round(1).tolist(),
+            "mlp_training_s": round(train_s, 2), "timing": "CUDA events around each step "
+            "(host waits on the per-iteration convergence flag included)"}
 
 
 # ------------------------------------------------------------------ our arm
@@ -334,11 +427,7 @@ def ours(args):
 
     mean_main = statistics.mean(main_ms)
     achieved = FLOP_PER_INTERACTION * interactions / (mean_main * 1e-3) / 1e12
-    traffic = None
-    tf = os.path.join(ROOT, "profiles", "bs_f32c_traffic.json")
-    if os.path.exists(tf):
-        tj = json.load(open(tf))
-        traffic = tj.get("bytes_per_interaction", 0.0) * interactions
+    traffic = profiled_traffic(interactions)
 
     cpu = None
     if rank == 0 and world == 1 and not args.quick:
@@ -351,6 +440,11 @@ def ours(args):
     wake_line = None
     if rank == 0 and args.wake_steps > 0 and not args.quick:
         wake_line = wake_bench(args)
+    mlp_line = e2e_line_run = None
+    if rank == 0 and not (args.quick or args.no_studies):
+        mlp_line = kj_mlp_bench()
+        if args.e2e_steps > 0:
+            e2e_line_run = e2e_run_bench(args.e2e_steps)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -379,6 +473,8 @@ def ours(args):
             "tiling": dict(zip(("targets_per_thread", "filaments_per_tile", "waves"),
                                wb.get_tuning(core, nt, nf))),
             "wake_batch": wake_line,
+            "kj_start_value": mlp_line,
+            "e2e_run": e2e_line_run,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -47,7 +47,7 @@ struct Plan {
 };
 
 struct TuneChoice {
-  int T = 8;
+  int T = 4;
   int KF = 64;
   double waves = 8.0;
 };
