@@ -164,6 +164,11 @@ __device__ __forceinline__ void bbox_accumulate(const float lo[3], const float h
 }
 
 // ------------------------------------------------------- filament packing
+// Field q of filament f in the pair-record layout (bs_types.h).
+__device__ __forceinline__ float &pk_field(float4 *pk, long long f, int q) {
+  return reinterpret_cast<float *>(pk)[(f >> 1) * 32 + 2 * q + (f & 1)];
+}
+
 // Writes filament f in the packed layout (see bs_types.h): FP32 hi/lo x1,
 // |L|^2, near-singular radius Rn^2 = max(|L|^2, 9 rc^2), L, the core term and
 // K L (K = gamma/4pi), plus the FP64 copy. A NaN/Inf ubar is zeroed by the
@@ -176,8 +181,8 @@ __device__ __forceinline__ void bbox_accumulate(const float lo[3], const float h
 // for D = (K^2 rc^2 |L|^2)^2, so the kernel never multiplies by K.
 __device__ __forceinline__ void pack_filament(long long f, double x1, double y1, double z1,
                                               double x2, double y2, double z2, double g, double r,
-                                              int model, double dcut, float4 *fa, float4 *fb,
-                                              float4 *fc, float4 *fd, double4 *ra, double4 *rb) {
+                                              int model, double dcut, float4 *pk, double4 *ra,
+                                              double4 *rb) {
   ra[f] = make_double4(x1, y1, z1, g);
   rb[f] = make_double4(x2, y2, z2, r);
   const double Lx = x2 - x1, Ly = y2 - y1, Lz = z2 - z1;
@@ -201,21 +206,22 @@ __device__ __forceinline__ void pack_filament(long long f, double x1, double y1,
   if (isfinite(r) && 9.0 * r > Rn2) Rn2 = 9.0 * r;
   if (!(Rn2 > 1e-20)) Rn2 = 1e-20;
   const float hx = (float)x1, hy = (float)y1, hz = (float)z1;
-  fa[f] = make_float4(hx, hy, hz, (float)L2);
-  fb[f] = make_float4((float)(x1 - (double)hx), (float)(y1 - (double)hy), (float)(z1 - (double)hz),
-                      (float)Rn2);
-  fc[f] = make_float4((float)Lx, (float)Ly, (float)Lz, (float)D);
-  fd[f] = make_float4((float)(K * Lx), (float)(K * Ly), (float)(K * Lz), 0.f);
+  const float v[16] = {hx, hy, hz, (float)L2,
+                       (float)(x1 - (double)hx), (float)(y1 - (double)hy),
+                       (float)(z1 - (double)hz), (float)Rn2,
+                       (float)Lx, (float)Ly, (float)Lz, (float)D,
+                       (float)(K * Lx), (float)(K * Ly), (float)(K * Lz), 0.f};
+#pragma unroll
+  for (int q = 0; q < 16; ++q) pk_field(pk, f, q) = v[q];
 }
 
 // Inert filament (far away, zero length, zero circulation) for padding.
-__device__ __forceinline__ void pack_inert(long long f, float4 *fa, float4 *fb, float4 *fc,
-                                           float4 *fd, double4 *ra, double4 *rb) {
+__device__ __forceinline__ void pack_inert(long long f, float4 *pk, double4 *ra, double4 *rb) {
   const double far = 1e18;
-  fa[f] = make_float4((float)far, (float)far, (float)far, 0.f);
-  fb[f] = make_float4(0.f, 0.f, 0.f, 0.f);
-  fc[f] = make_float4(0.f, 0.f, 0.f, 1.f);
-  fd[f] = make_float4(0.f, 0.f, 0.f, 0.f);
+  const float v[16] = {(float)far, (float)far, (float)far, 0.f, 0.f, 0.f, 0.f, 0.f,
+                       0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+  for (int q = 0; q < 16; ++q) pk_field(pk, f, q) = v[q];
   ra[f] = make_double4(far, far, far, 0.0);
   rb[f] = make_double4(far, far, far, 0.0);
 }

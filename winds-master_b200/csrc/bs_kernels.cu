@@ -39,7 +39,7 @@ __global__ void bs_bbox_init(BBox *bb) {
 __global__ void bs_pack_filaments(const double *__restrict__ F1, const double *__restrict__ F2,
                                   const double *__restrict__ gam, const double *__restrict__ rc,
                                   long long d0, long long nf, long long off, int model, double dcut,
-                                  float4 *fa, float4 *fb, float4 *fc, float4 *fd, double4 *ra,
+                                  float4 *pk, double4 *ra,
                                   double4 *rb, BBox *bb) {
   const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
@@ -49,7 +49,7 @@ __global__ void bs_pack_filaments(const double *__restrict__ F1, const double *_
     const double x1 = F1[b], y1 = F1[b + d0], z1 = F1[b + 2 * d0];
     const double x2 = F2[b], y2 = F2[b + d0], z2 = F2[b + 2 * d0];
     const double g = gam[f], r = rc[f];
-    pack_filament(off + f, x1, y1, z1, x2, y2, z2, g, r, model, dcut, fa, fb, fc, fd, ra, rb);
+    pack_filament(off + f, x1, y1, z1, x2, y2, z2, g, r, model, dcut, pk, ra, rb);
     lo[0] = (float)fmin(x1, x2), lo[1] = (float)fmin(y1, y2), lo[2] = (float)fmin(z1, z2);
     hi[0] = (float)fmax(x1, x2), hi[1] = (float)fmax(y1, y2), hi[2] = (float)fmax(z1, z2);
   }
@@ -57,11 +57,11 @@ __global__ void bs_pack_filaments(const double *__restrict__ F1, const double *_
 }
 
 // Inert filaments filling [from, to): far away, zero length, zero circulation.
-__global__ void bs_pad_filaments(long long from, long long to, float4 *fa, float4 *fb, float4 *fc,
-                                 float4 *fd, double4 *ra, double4 *rb) {
+__global__ void bs_pad_filaments(long long from, long long to, float4 *pk, double4 *ra,
+                                 double4 *rb) {
   const long long f = from + (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= to) return;
-  pack_inert(f, fa, fb, fc, fd, ra, rb);
+  pack_inert(f, pk, ra, rb);
 }
 
 __global__ void bs_pack_targets(const double *__restrict__ P, long long ns, long long np,
@@ -138,7 +138,7 @@ constexpr uint64_t kDefaultWaitNs = 2000000000ull;  // 2 s per tile: far above a
 
 template <int KF>
 struct StageSmem {
-  static constexpr int kBytes = KF * 64;  // fa, fb, fc, fd: 16 B each
+  static constexpr int kBytes = KF * 64;  // KF/2 pair records of 128 B
   static constexpr int kStages = KF >= 128 ? 3 : kStagesMax;  // filament stages in flight
 };
 
@@ -165,10 +165,7 @@ template <int KF>
 __device__ __forceinline__ void issue_stage(const F32cArgs &a, unsigned char *stage, uint64_t *bar,
                                             int f0) {
   mbar_arrive_expect_tx(bar, StageSmem<KF>::kBytes);
-  bulk_g2s(stage, a.fa + f0, KF * 16, bar);
-  bulk_g2s(stage + KF * 16, a.fb + f0, KF * 16, bar);
-  bulk_g2s(stage + KF * 32, a.fc + f0, KF * 16, bar);
-  bulk_g2s(stage + KF * 48, a.fd + f0, KF * 16, bar);
+  bulk_g2s(stage, a.pk + (size_t)(f0 / 2) * 8, KF * 64, bar);
 }
 
 // Thread 0 hands global tile g (filaments f0 .. f0+KF) to the copy engine
@@ -195,51 +192,109 @@ __device__ __forceinline__ bool try_produce(const F32cArgs &a, unsigned char *sm
   return true;
 }
 
-// One target-filament interaction in FP32, accumulated into (ax, ay, az).
-// (Mx, My, Mz) = K L with K = gamma/4pi; D is the packed core term. With NEAR
-// it also tests r1.r2 < Rn^2: such pairs are skipped and recorded in `bits`
-// (they are redone in FP64 after the tile).
+// ----------------------------------------------------- packed FP32 arithmetic
+// The direct sum runs on pairs of filaments: every FP32 operation is a packed
+// f32x2 instruction (two independent IEEE operations, round to nearest) on the
+// two filaments of a pair record, so one issue slot does two interactions'
+// worth of arithmetic; the FMA pipe, not instruction issue, bounds the loop.
+__device__ __forceinline__ float2 lo2(const float4 v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(const float4 v) { return make_float2(v.z, v.w); }
+__device__ __forceinline__ float2 neg2(const float2 v) { return make_float2(-v.x, -v.y); }
+__device__ __forceinline__ float2 rsqrt2(const float2 v) {
+  return make_float2(rsqrt_approx(v.x), rsqrt_approx(v.y));
+}
+__device__ __forceinline__ float2 rcp2(const float2 v) {
+  return make_float2(rcp_approx(v.x), rcp_approx(v.y));
+}
+
+// One filament pair of a stage, relative to this thread's centre c.
+struct Fil2 {
+  float2 qx, qy, qz;  // x1 - c (from the hi/lo split)
+  float2 Lx, Ly, Lz, L2, D;
+  float2 Mx, My, Mz;  // K L, K = gamma/4pi
+  float2 Rn2;         // near-singular threshold (careful path)
+};
+
+// Pair record r (8 float4, layout in bs_types.h) into registers.
+__device__ __forceinline__ void load_pair(const float4 *r, float2 ncx, float2 ncy, float2 ncz,
+                                          Fil2 &f) {
+  const float4 a0 = r[0], a1 = r[1], b0 = r[2], b1 = r[3];
+  const float4 l0 = r[4], l1 = r[5], m0 = r[6], m1 = r[7];
+  f.qx = __fadd2_rn(__fadd2_rn(lo2(a0), ncx), lo2(b0));
+  f.qy = __fadd2_rn(__fadd2_rn(hi2(a0), ncy), hi2(b0));
+  f.qz = __fadd2_rn(__fadd2_rn(lo2(a1), ncz), lo2(b1));
+  f.L2 = hi2(a1);
+  f.Rn2 = hi2(b1);
+  f.Lx = lo2(l0);
+  f.Ly = hi2(l0);
+  f.Lz = lo2(l1);
+  f.D = hi2(l1);
+  f.Mx = lo2(m0);
+  f.My = hi2(m0);
+  f.Mz = lo2(m1);
+}
+
+// One target against one filament pair, accumulated into the packed sums
+// (ax, ay, az) (one lane per filament of the pair). (npx, npy, npz) = -(P - c)
+// broadcast to both lanes. With NEAR it also tests r1.r2 < Rn^2 per lane: such
+// terms are zeroed and recorded in `bits` (bit0 for the pair's first
+// filament, bit1 for its second); they are redone in FP64 after the tile.
 template <int MODEL, bool CO, bool NEAR>
-__device__ __forceinline__ void interact(float px, float py, float pz, float xrx, float xry,
-                                         float xrz, float Lx, float Ly, float Lz, float L2,
-                                         float Mx, float My, float Mz, float Dv, float Rn2,
-                                         float co2, float &ax, float &ay, float &az,
-                                         unsigned &bits, unsigned bit) {
-  const float rx = px - xrx, ry = py - xry, rz = pz - xrz;  // r1 = P - x1
-  // K (r1 x r2) = K L x r1 (no cancellation for far or collinear points)
-  const float cxv = My * rz - Mz * ry;
-  const float cyv = Mz * rx - Mx * rz;
-  const float czv = Mx * ry - My * rx;
-  const float r1s = rx * rx + ry * ry + rz * rz;
-  const float Ld = Lx * rx + Ly * ry + Lz * rz;
-  const float dot = r1s - Ld;          // r1 . r2
-  const float r2s = dot + (L2 - Ld);   // |r1 - L|^2
-  const float i1 = rsqrt_approx(r1s), i2 = rsqrt_approx(r2s);
-  const float gg = i1 * i2;
-  const float e = fmaf(dot, gg, 1.f);  // 1 + cos(theta) >= 1 for far pairs
-  float ub;
+__device__ __forceinline__ void interact2(float2 npx, float2 npy, float2 npz, const Fil2 &f,
+                                          float2 Rn2, float co2, float2 &ax, float2 &ay,
+                                          float2 &az, unsigned &bits, unsigned bit0,
+                                          unsigned bit1) {
+  const float2 nx = __fadd2_rn(f.qx, npx);  // x1 - P = -r1
+  const float2 ny = __fadd2_rn(f.qy, npy);
+  const float2 nz = __fadd2_rn(f.qz, npz);
+  float2 r1s = __fmul2_rn(nx, nx);
+  r1s = __ffma2_rn(ny, ny, r1s);
+  r1s = __ffma2_rn(nz, nz, r1s);
+  float2 ld = __fmul2_rn(f.Lx, nx);  // -L.r1
+  ld = __ffma2_rn(f.Ly, ny, ld);
+  ld = __ffma2_rn(f.Lz, nz, ld);
+  const float2 dot = __fadd2_rn(r1s, ld);                   // r1 . r2
+  const float2 r2s = __fadd2_rn(dot, __fadd2_rn(f.L2, ld));  // |r1 - L|^2
+  const float2 i1 = rsqrt2(r1s), i2 = rsqrt2(r2s);
+  const float2 gg = __fmul2_rn(i1, i2);
+  const float2 e = __ffma2_rn(dot, gg, make_float2(1.f, 1.f));  // 1 + cos(theta)
+  // K (r1 x r2) = K L x r1 = (x1 - P) x (K L): no cancellation for far or
+  // collinear points
+  const float2 cx = __ffma2_rn(ny, f.Mz, __fmul2_rn(nz, neg2(f.My)));
+  const float2 cy = __ffma2_rn(nz, f.Mx, __fmul2_rn(nx, neg2(f.Mz)));
+  const float2 cz = __ffma2_rn(nx, f.My, __fmul2_rn(ny, neg2(f.Mx)));
+  float2 ub;
   if (MODEL == kCoreVatistas) {
     // Cnu / (r1 r2 (r1 r2 + r1.r2)) with h^2 = |L x r1|^2/|L|^2 and rc^4 folded:
     // Cnu = |c|^2 / sqrt(|c|^4 + D), c = K L x r1, D = (K^2 rc^2 |L|^2)^2
-    const float c2 = cxv * cxv + cyv * cyv + czv * czv;
-    const float q = fmaf(c2, c2, Dv);
-    ub = ((i1 + i2) * gg) * c2 * rsqrt_approx((e * e) * q);
+    float2 c2 = __fmul2_rn(cx, cx);
+    c2 = __ffma2_rn(cy, cy, c2);
+    c2 = __ffma2_rn(cz, cz, c2);
+    const float2 q = __ffma2_rn(c2, c2, f.D);
+    const float2 w = __fmul2_rn(__fmul2_rn(__fadd2_rn(i1, i2), gg), c2);
+    ub = __fmul2_rn(w, rsqrt2(__fmul2_rn(__fmul2_rn(e, e), q)));
   } else {
     // (r1+r2)/(r1r2(r1r2+r1.r2) + d|L|^2) = (i1+i2) gg / (e + d|L|^2 gg^2)
-    ub = ((i1 + i2) * gg) * rcp_approx(fmaf(Dv, gg * gg, e));
+    ub = __fmul2_rn(__fmul2_rn(__fadd2_rn(i1, i2), gg),
+                    rcp2(__ffma2_rn(f.D, __fmul2_rn(gg, gg), e)));
   }
-  bool skip = false;
   if (NEAR) {
-    const bool nr = dot < Rn2;
-    skip = nr;
-    if (nr) bits |= bit;
+    if (dot.x < Rn2.x) {
+      bits |= bit0;
+      ub.x = 0.f;
+    }
+    if (dot.y < Rn2.y) {
+      bits |= bit1;
+      ub.y = 0.f;
+    }
   }
-  if (CO) skip = skip || (fminf(r1s, r2s) > co2);
-  if (!skip) {
-    ax = fmaf(ub, cxv, ax);
-    ay = fmaf(ub, cyv, ay);
-    az = fmaf(ub, czv, az);
+  if (CO) {
+    if (fminf(r1s.x, r2s.x) > co2) ub.x = 0.f;
+    if (fminf(r1s.y, r2s.y) > co2) ub.y = 0.f;
   }
+  ax = __ffma2_rn(ub, cx, ax);
+  ay = __ffma2_rn(ub, cy, ay);
+  az = __ffma2_rn(ub, cz, az);
 }
 
 // One item: the thread's T targets against filaments [it.f_begin, it.f_end).
@@ -248,8 +303,8 @@ template <int T, int KF, int MODEL, bool CO>
 __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, const Tile &tl,
                                           unsigned char *smem, uint64_t *full,
                                           uint64_t *empty, float *s_k, unsigned *s_nb,
-                                          unsigned &gt, float (&px)[T], float (&py)[T],
-                                          float (&pz)[T], float cx, float cy, float cz,
+                                          unsigned &gt, float2 (&npx)[T], float2 (&npy)[T],
+                                          float2 (&npz)[T], float2 ncx, float2 ncy, float2 ncz,
                                           float S2, const float *ws, unsigned &near_cnt) {
   const int tid = threadIdx.x;
   const int ntiles = (it.f_end - it.f_begin) / KF;
@@ -269,9 +324,9 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, con
         break;
       }
   }
-  float ax[T], ay[T], az[T];
+  float2 ax[T], ay[T], az[T];
 #pragma unroll
-  for (int t = 0; t < T; ++t) ax[t] = ay[t] = az[t] = 0.f;
+  for (int t = 0; t < T; ++t) ax[t] = ay[t] = az[t] = make_float2(0.f, 0.f);
 
   int i = 0;
   for (; ok && i < ntiles; ++i) {
@@ -287,19 +342,18 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, con
     }
     const bool timed_out = !ok || !mbar_wait_bounded(&full[st], par, a.err, a.wait_limit_ns);
     const unsigned char *stage = smem + st * StageSmem<KF>::kBytes;
-    const float4 *sA = reinterpret_cast<const float4 *>(stage);
-    const float4 *sB = reinterpret_cast<const float4 *>(stage + KF * 16);
-    const float4 *sC = reinterpret_cast<const float4 *>(stage + KF * 32);
-    const float4 *sD = reinterpret_cast<const float4 *>(stage + KF * 48);
+    const float4 *sP = reinterpret_cast<const float4 *>(stage);  // KF/2 pair records
+    const float *sF = reinterpret_cast<const float *>(stage);
     if (timed_out) {
       ok = false;
       break;
     }
-    // Hot loop: filaments in groups of 4. A warp-level screen (one filament
-    // per lane, every 32 filaments) sends groups that are far from all of the
-    // warp's targets down the plain path; the others test every pair and put
-    // their near-singular bits (bit 8*j + t: filament 4*kk+j, target t) in
-    // shared memory as one word. `careful` has bit g for every such group g.
+    // Hot loop: filaments in groups of 4 (two pair records). A warp-level
+    // screen (one filament per lane, every 32 filaments) sends groups that are
+    // far from all of the warp's targets down the plain path; the others test
+    // every pair and put their near-singular bits (bit 8*j + t: filament
+    // 4*kk+j, target t) in shared memory as one word. `careful` has bit g for
+    // every such group g.
     unsigned careful = 0u;
 #pragma unroll 1
     for (int w = 0; w < KF / 32; ++w) {
@@ -308,18 +362,19 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, con
         m = 0xffffffffu;
       } else {
         const int k = 32 * w + lane;
-        const float4 A = sA[k], B = sB[k], C = sC[k];
+        const float *f = sF + (k >> 1) * 32 + (k & 1);  // field j of filament k at f[2 j]
         // the warp's target ball (centre, radius, largest S2), kept in shared
         // memory so it holds no registers across the hot loop
         const float wcx = ws[0], wcy = ws[1], wcz = ws[2], wr = ws[3], rn_floor = ws[4];
         const float big = fabsf(wcx) + fabsf(wcy) + fabsf(wcz);
-        const float mx = (A.x - wcx) + fmaf(0.5f, C.x, B.x);
-        const float my = (A.y - wcy) + fmaf(0.5f, C.y, B.y);
-        const float mz = (A.z - wcz) + fmaf(0.5f, C.z, B.z);
+        const float Ax = f[0], Ay = f[2], Az = f[4], L2 = f[6];
+        const float mx = (Ax - wcx) + fmaf(0.5f, f[16], f[8]);
+        const float my = (Ay - wcy) + fmaf(0.5f, f[18], f[10]);
+        const float mz = (Az - wcz) + fmaf(0.5f, f[20], f[12]);
         const float d2 = mx * mx + my * my + mz * mz;
-        const float reach = sqrtf(fmaf(0.25f, A.w, fmaxf(B.w, rn_floor)));
+        const float reach = sqrtf(fmaf(0.25f, L2, fmaxf(f[14], rn_floor)));
         const float slack =
-            1e-5f * (big + fabsf(A.x) + fabsf(A.y) + fabsf(A.z)) + 1e-3f * (reach + wr);
+            1e-5f * (big + fabsf(Ax) + fabsf(Ay) + fabsf(Az)) + 1e-3f * (reach + wr);
         const float lim = wr + reach + slack;
         m = __ballot_sync(0xffffffffu, !(d2 > lim * lim));
       }
@@ -328,40 +383,30 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, con
         const int kk = 32 * w + 4 * g;
         if (((m >> (4 * g)) & 0xfu) == 0u) {
 #pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            const int k = kk + j;
-            const float4 A = sA[k];
-            const float4 B = sB[k];
-            const float4 C = sC[k];
-            const float4 M = sD[k];
-            const float xrx = (A.x - cx) + B.x, xry = (A.y - cy) + B.y, xrz = (A.z - cz) + B.z;
+          for (int j = 0; j < 2; ++j) {
+            Fil2 f;
+            load_pair(sP + (kk / 2 + j) * 8, ncx, ncy, ncz, f);
             unsigned unused = 0;
 #pragma unroll
             for (int t = 0; t < T; ++t)
-              interact<MODEL, false, false>(px[t], py[t], pz[t], xrx, xry, xrz, C.x, C.y, C.z,
-                                            A.w, M.x, M.y, M.z, C.w, 0.f, co2, ax[t], ay[t],
-                                            az[t], unused, 0u);
+              interact2<MODEL, false, false>(npx[t], npy[t], npz[t], f, f.Rn2, co2, ax[t], ay[t],
+                                             az[t], unused, 0u, 0u);
           }
         } else {
           careful |= 1u << (8 * w + g);
           unsigned nbits = 0;
 #pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            const int k = kk + j;
-            const float4 A = sA[k];
-            const float4 B = sB[k];
-            const float4 C = sC[k];
-            const float4 M = sD[k];
-            // x1 relative to this thread's centre, from its hi/lo split
-            const float xrx = (A.x - cx) + B.x, xry = (A.y - cy) + B.y, xrz = (A.z - cz) + B.z;
+          for (int j = 0; j < 2; ++j) {
+            Fil2 f;
+            load_pair(sP + (kk / 2 + j) * 8, ncx, ncy, ncz, f);
             // near-singular threshold, raised for threads whose targets spread
             // far from their centre (the FP32 differences lose ~eps * spread / |r1|)
-            const float Rn2 = fmaxf(B.w, S2);
+            const float2 Rn2 = make_float2(fmaxf(f.Rn2.x, S2), fmaxf(f.Rn2.y, S2));
 #pragma unroll
             for (int t = 0; t < T; ++t)
-              interact<MODEL, CO, true>(px[t], py[t], pz[t], xrx, xry, xrz, C.x, C.y, C.z, A.w,
-                                        M.x, M.y, M.z, C.w, Rn2, co2, ax[t], ay[t], az[t], nbits,
-                                        1u << (8 * j + t));
+              interact2<MODEL, CO, true>(npx[t], npy[t], npz[t], f, Rn2, co2, ax[t], ay[t],
+                                         az[t], nbits, 1u << (8 * (2 * j) + t),
+                                         1u << (8 * (2 * j + 1) + t));
           }
           s_nb[(kk / 4) * kThreads + tid] = nbits;
         }
@@ -380,10 +425,10 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, con
 #pragma unroll
     for (int t = 0; t < T; ++t) {
       const int sl = tid * T + t;
-      kahan_add(s_k[0 * kThreads * T + sl], s_k[1 * kThreads * T + sl], ax[t]);
-      kahan_add(s_k[2 * kThreads * T + sl], s_k[3 * kThreads * T + sl], ay[t]);
-      kahan_add(s_k[4 * kThreads * T + sl], s_k[5 * kThreads * T + sl], az[t]);
-      ax[t] = ay[t] = az[t] = 0.f;
+      kahan_add(s_k[0 * kThreads * T + sl], s_k[1 * kThreads * T + sl], ax[t].x + ax[t].y);
+      kahan_add(s_k[2 * kThreads * T + sl], s_k[3 * kThreads * T + sl], ay[t].x + ay[t].y);
+      kahan_add(s_k[4 * kThreads * T + sl], s_k[5 * kThreads * T + sl], az[t].x + az[t].y);
+      ax[t] = ay[t] = az[t] = make_float2(0.f, 0.f);
     }
     // Near-singular pairs of this tile, each lane its own: the reference formula
     // in FP64, added to the Kahan state as an exact hi + lo pair.
@@ -432,11 +477,12 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, con
   return true;
 }
 
-// Resident CTAs per SM the register allocation is capped for: 6 for T <= 4
-// (80 registers), 4 for T = 8 (128 registers).
+// Resident CTAs per SM the register allocation is capped for: 6 for T = 2
+// (80 registers), 4 for T = 4 (128), 2 for T = 8 (255). The packed loop keeps
+// each target as broadcast pairs and its sums as pairs (12 registers a target).
 template <int T>
 struct MinBlocks {
-  static constexpr int value = T <= 4 ? 6 : 4;
+  static constexpr int value = T <= 2 ? 6 : (T <= 4 ? 4 : 2);
 };
 
 template <int T, int KF, int MODEL>
@@ -493,6 +539,16 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<T>::value) bs_f32c(const F
       for (int c = 0; c < 6; ++c) s_k[c * kThreads * T + tid * T + t] = 0.f;
     }
     const float S2 = 0.09f * spread2;  // pairs closer than 0.3 x spread go to FP64
+    // -(P - c) in both lanes of a packed register, and -c likewise
+    float2 npx[T], npy[T], npz[T];
+#pragma unroll
+    for (int t = 0; t < T; ++t) {
+      npx[t] = make_float2(-px[t], -px[t]);
+      npy[t] = make_float2(-py[t], -py[t]);
+      npz[t] = make_float2(-pz[t], -pz[t]);
+    }
+    const float2 ncx = make_float2(-cx, -cx), ncy = make_float2(-cy, -cy),
+                 ncz = make_float2(-cz, -cz);
     // The warp's targets lie in the ball (wc, wr) around lane 0's centre. As
     // r1.r2 = |P - m|^2 - |L|^2/4 (m the filament midpoint), a filament whose
     // midpoint is farther than wr + sqrt(|L|^2/4 + Rn^2) from wc has
@@ -524,11 +580,11 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<T>::value) bs_f32c(const F
     __syncwarp();
     bool ok;
     if (co_on)
-      ok = f32c_item<T, KF, MODEL, true>(a, it, tl, smem, full, empty, s_k, s_nb, gt, px, py, pz,
-                                         cx, cy, cz, S2, ws, near_cnt);
+      ok = f32c_item<T, KF, MODEL, true>(a, it, tl, smem, full, empty, s_k, s_nb, gt, npx, npy,
+                                         npz, ncx, ncy, ncz, S2, ws, near_cnt);
     else
-      ok = f32c_item<T, KF, MODEL, false>(a, it, tl, smem, full, empty, s_k, s_nb, gt, px, py,
-                                          pz, cx, cy, cz, S2, ws, near_cnt);
+      ok = f32c_item<T, KF, MODEL, false>(a, it, tl, smem, full, empty, s_k, s_nb, gt, npx, npy,
+                                          npz, ncx, ncy, ncz, S2, ws, near_cnt);
     __syncwarp();
     if (!ok) return;
     double *part = a.part + (size_t)item_id * 3 * a.tile_cap;
@@ -771,8 +827,8 @@ cudaError_t launch_pack_filaments(const double *F1, const double *F2, const doub
   if (nf <= 0) return cudaSuccess;
   const int bs = 256;
   const long long grid = (nf + bs - 1) / bs;
-  bs_pack_filaments<<<(unsigned)grid, bs, 0, s>>>(F1, F2, gam, rc, d0, nf, off, model, dcut, pf.fa,
-                                                 pf.fb, pf.fc, pf.fd, pf.ra, pf.rb, bb);
+  bs_pack_filaments<<<(unsigned)grid, bs, 0, s>>>(F1, F2, gam, rc, d0, nf, off, model, dcut, pf.pk,
+                                                 pf.ra, pf.rb, bb);
   return cudaGetLastError();
 }
 
@@ -781,7 +837,7 @@ cudaError_t launch_pad_filaments(long long from, long long to, const PackedFilam
   if (to <= from) return cudaSuccess;
   const int bs = 256;
   const long long grid = (to - from + bs - 1) / bs;
-  bs_pad_filaments<<<(unsigned)grid, bs, 0, s>>>(from, to, pf.fa, pf.fb, pf.fc, pf.fd, pf.ra, pf.rb);
+  bs_pad_filaments<<<(unsigned)grid, bs, 0, s>>>(from, to, pf.pk, pf.ra, pf.rb);
   return cudaGetLastError();
 }
 

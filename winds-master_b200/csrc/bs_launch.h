@@ -8,7 +8,7 @@
 namespace winds {
 
 struct PackedFilaments {
-  float4 *fa, *fb, *fc, *fd;
+  float4 *pk;  // pair records: 4 float4 per filament (layout in bs_types.h)
   double4 *ra, *rb;
 };
 

@@ -1,11 +1,13 @@
 // bs_types.h -- plain structs shared by the host engine and the kernels.
 //
 // HBM layout of one evaluation (all per-context, grow-only buffers):
-//   packed filaments, padded to the filament tile (KF) with inert entries
-//     fa[f] = (x1_hi.x, x1_hi.y, x1_hi.z, |L|^2)   float4
-//     fb[f] = (x1_lo.x, x1_lo.y, x1_lo.z, Rn^2)    float4  (x1 = hi + lo exactly to ~2^-48)
-//     fc[f] = (L.x, L.y, L.z, D)                   float4  (L = x2 - x1)
-//     fd[f] = (K L.x, K L.y, K L.z, 0)             float4  (K = gamma/4pi)
+//   packed filaments, padded to the filament tile (KF) with inert entries, as
+//   pair records: filaments 2j and 2j+1 share 32 floats (8 float4), field q of
+//   filament 2j+h at float 2q+h, so every float4 holds two fields of both:
+//     fields  0-3   x1_hi.x, x1_hi.y, x1_hi.z, |L|^2
+//             4-7   x1_lo.x, x1_lo.y, x1_lo.z, Rn^2   (x1 = hi + lo to ~2^-48)
+//             8-11  L.x, L.y, L.z, D                  (L = x2 - x1)
+//            12-15  K L.x, K L.y, K L.z, 0            (K = gamma/4pi)
 //   with D = (K^2 rc^2 |L|^2)^2 (Vatistas: the core term scaled like |K L x r1|^4,
 //   so K cancels from the core factor and enters only through K L) or d |L|^2
 //   (cut-off)
@@ -60,8 +62,7 @@ struct BBox {           // ordered-int keys of float bounds (see float_key)
 };
 
 struct F32cArgs {
-  const float4 *fa, *fb, *fc;
-  const float4 *fd;
+  const float4 *pk;  // pair records, 8 float4 per two filaments
   const double4 *ra, *rb;
   const double4 *tp;
   const Group *groups;

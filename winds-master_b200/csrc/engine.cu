@@ -162,7 +162,7 @@ void shutdown_all() {
     Context *c = kv.second;
     cudaSetDevice(c->dev);
     cudaStreamSynchronize(c->stream);
-    for (DevBuf *b : {&c->fa, &c->fb, &c->fc, &c->fd, &c->ra, &c->rb, &c->tp, &c->tp_raw,
+    for (DevBuf *b : {&c->pk, &c->ra, &c->rb, &c->tp, &c->tp_raw,
                       &c->tgroup, &c->keys, &c->vals, &c->perm, &c->sort_tmp, &c->groups,
                       &c->tiles, &c->items, &c->part, &c->bbox, &c->ctr, &c->err, &c->nearctr,
                       &c->in_P, &c->in_F, &c->out_u})
@@ -280,8 +280,7 @@ int pack_inputs(Context *c, const winds_bs_family *fams, int nfam,
   long long nt = 0;
   for (const TargetSpec &t : tsets) nt += t.count;
   int rc;
-  if ((rc = c->fa.ensure(nfp * sizeof(float4), s)) || (rc = c->fb.ensure(nfp * sizeof(float4), s)) ||
-      (rc = c->fc.ensure(nfp * sizeof(float4), s)) || (rc = c->fd.ensure(nfp * sizeof(float4), s)) ||
+  if ((rc = c->pk.ensure(nfp * 4 * sizeof(float4), s)) ||
       (rc = c->ra.ensure(nfp * sizeof(double4), s)) ||
       (rc = c->rb.ensure(nfp * sizeof(double4), s)) ||
       (rc = c->tp.ensure(std::max<long long>(nt, 1) * sizeof(double4), s)) ||
@@ -296,8 +295,7 @@ int pack_inputs(Context *c, const winds_bs_family *fams, int nfam,
       cudaSuccess)
     return fail(WINDS_BS_ERR_CUDA, "target sort size query failed");
   if ((rc = c->sort_tmp.ensure(sort_bytes + 256, s))) return rc;
-  PackedFilaments pf{(float4 *)c->fa.p, (float4 *)c->fb.p, (float4 *)c->fc.p,
-                     (float4 *)c->fd.p, (double4 *)c->ra.p, (double4 *)c->rb.p};
+  PackedFilaments pf{(float4 *)c->pk.p, (double4 *)c->ra.p, (double4 *)c->rb.p};
   cudaError_t e = launch_bbox_init((BBox *)c->bbox.p, s);
   c->launches += 1;
   long long off = 0;
@@ -409,10 +407,7 @@ int run_direct_sum(Context *c, const std::vector<GroupSpec> &gs, int model, doub
   const size_t part_bytes = pl.items.size() * 3 * (size_t)tile_cap * sizeof(double);
   if ((rc = c->part.ensure(part_bytes + 16, s))) return rc;
   F32cArgs a;
-  a.fa = (const float4 *)c->fa.p;
-  a.fb = (const float4 *)c->fb.p;
-  a.fc = (const float4 *)c->fc.p;
-  a.fd = (const float4 *)c->fd.p;
+  a.pk = (const float4 *)c->pk.p;
   a.ra = (const double4 *)c->ra.p;
   a.rb = (const double4 *)c->rb.p;
   a.tp = (const double4 *)c->tp.p;

@@ -59,7 +59,7 @@ struct Context {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev_main0 = nullptr, ev_main1 = nullptr, ev_upload = nullptr;
   // packed inputs; targets sorted (tp) from their packed order (tp_raw)
-  DevBuf fa, fb, fc, fd, ra, rb, tp, tp_raw, tgroup, keys, vals, perm, sort_tmp;
+  DevBuf pk, ra, rb, tp, tp_raw, tgroup, keys, vals, perm, sort_tmp;
   // plan tables and partial sums
   DevBuf groups, tiles, items, part;
   // small words

@@ -188,8 +188,7 @@ extern "C" int winds_bs_eval_device_noalloc(const winds_bs_family *fams, int nfa
   unsigned *ctr = cv.take<unsigned>(4);
   unsigned *err = cv.take<unsigned>(4);
   unsigned long long *nearc = cv.take<unsigned long long>(1);
-  PackedFilaments pf{cv.take<float4>(nfp), cv.take<float4>(nfp), cv.take<float4>(nfp),
-                     cv.take<float4>(nfp), cv.take<double4>(nfp), cv.take<double4>(nfp)};
+  PackedFilaments pf{cv.take<float4>(nfp * 4), cv.take<double4>(nfp), cv.take<double4>(nfp)};
   double4 *tp = cv.take<double4>(nt);
   double4 *tp_raw = cv.take<double4>(nt);
   int *tgroup = cv.take<int>(nt);
@@ -237,10 +236,7 @@ extern "C" int winds_bs_eval_device_noalloc(const winds_bs_family *fams, int nfa
 
   // ---- direct sum and reduction
   F32cArgs a;
-  a.fa = pf.fa;
-  a.fb = pf.fb;
-  a.fc = pf.fc;
-  a.fd = pf.fd;
+  a.pk = pf.pk;
   a.ra = pf.ra;
   a.rb = pf.rb;
   a.tp = tp;

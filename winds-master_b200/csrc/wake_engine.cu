@@ -47,7 +47,7 @@ struct winds_wake_batch {
   DevBuf rc_s, rc_t, len_old_s, len_old_t, len_s, len_t, len_ps, len_pt;
   DevBuf quarter, trailing, wind;
   // direct-sum buffers
-  DevBuf fa, fb, fc, fd, ra, rb, tp, tp_raw, tgroup, keys, vals, perm, sort_tmp;
+  DevBuf pk, ra, rb, tp, tp_raw, tgroup, keys, vals, perm, sort_tmp;
   DevBuf groups_main, groups_pred, tiles, items, part, bbox, ctr, err, nearctr;
   size_t sort_bytes = 0;
   int n_tiles = 0, n_items = 0, tile_cap = 0, grid = 0;
@@ -106,8 +106,7 @@ int alloc_all(winds_wake_batch *b) {
       (rc = b->step_d.ensure(4 * sizeof(int), s)))
     return rc;
   const long long nf = b->fil_pad, nt = std::max<long long>(b->nodes, 1);
-  if ((rc = b->fa.ensure(nf * sizeof(float4), s)) || (rc = b->fb.ensure(nf * sizeof(float4), s)) ||
-      (rc = b->fc.ensure(nf * sizeof(float4), s)) || (rc = b->fd.ensure(nf * sizeof(float4), s)) ||
+  if ((rc = b->pk.ensure(nf * 4 * sizeof(float4), s)) ||
       (rc = b->ra.ensure(nf * sizeof(double4), s)) || (rc = b->rb.ensure(nf * sizeof(double4), s)) ||
       (rc = b->tp.ensure(nt * sizeof(double4), s)) ||
       (rc = b->tp_raw.ensure(nt * sizeof(double4), s)) ||
@@ -184,7 +183,7 @@ cudaError_t enqueue_eval(winds_wake_batch *b, const double *dom, const double *s
                          double *rc_s, double *rc_t, DevBuf &groups, int &launches) {
   cudaStream_t s = b->stream;
   const WakeCase *cd = P<const WakeCase>(b->cases_d);
-  PackedFilaments pf{P<float4>(b->fa), P<float4>(b->fb), P<float4>(b->fc), P<float4>(b->fd),
+  PackedFilaments pf{P<float4>(b->pk),
                      P<double4>(b->ra), P<double4>(b->rb)};
   BBox *bb = P<BBox>(b->bbox);
   cudaError_t e = launch_bbox_init(bb, s);
@@ -207,10 +206,7 @@ cudaError_t enqueue_eval(winds_wake_batch *b, const double *dom, const double *s
                               P<double4>(b->tp), s);
   if (e == cudaSuccess) e = cudaMemsetAsync(b->ctr.p, 0, sizeof(unsigned), s);
   F32cArgs a;
-  a.fa = pf.fa;
-  a.fb = pf.fb;
-  a.fc = pf.fc;
-  a.fd = pf.fd;
+  a.pk = pf.pk;
   a.ra = pf.ra;
   a.rb = pf.rb;
   a.tp = P<const double4>(b->tp);
@@ -339,7 +335,7 @@ cudaError_t enqueue_kj_iter(winds_wake_batch *b, int &launches) {
   cudaStream_t s = b->stream;
   const WakeCase *cd = P<const WakeCase>(b->cases_d);
   const KJCase *kd = P<const KJCase>(b->kjc_d);
-  PackedFilaments pf{P<float4>(b->fa), P<float4>(b->fb), P<float4>(b->fc), P<float4>(b->fd),
+  PackedFilaments pf{P<float4>(b->pk),
                      P<double4>(b->ra), P<double4>(b->rb)};
   BBox *bb = P<BBox>(b->bbox);
   cudaError_t e = launch_wake_bookkeep(cd, b->ncases, b->max_cols, P<const double>(b->bound),
@@ -353,10 +349,7 @@ cudaError_t enqueue_kj_iter(winds_wake_batch *b, int &launches) {
                               P<const double>(b->rc_t), b->model, b->dcut, pf, bb, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(b->ctr.p, 0, sizeof(unsigned), s);
   F32cArgs a;
-  a.fa = pf.fa;
-  a.fb = pf.fb;
-  a.fc = pf.fc;
-  a.fd = pf.fd;
+  a.pk = pf.pk;
   a.ra = pf.ra;
   a.rb = pf.rb;
   a.tp = P<const double4>(b->tp_ll);
@@ -1077,8 +1070,7 @@ void winds_wake_destroy(winds_wake_batch *b) {
                     &b->h2, &b->h3, &b->uind, &b->uind_pred, &b->bound, &b->trail_prev,
                     &b->shed_cur, &b->trail_cur, &b->shed_next, &b->trail_next, &b->rc_s,
                     &b->rc_t, &b->len_old_s, &b->len_old_t, &b->len_s, &b->len_t, &b->len_ps,
-                    &b->len_pt, &b->quarter, &b->trailing, &b->wind, &b->fa, &b->fb, &b->fc,
-                    &b->fd, &b->ra, &b->rb, &b->tp, &b->tp_raw, &b->tgroup, &b->keys, &b->vals,
+                    &b->len_pt, &b->quarter, &b->trailing, &b->wind, &b->pk, &b->ra, &b->rb, &b->tp, &b->tp_raw, &b->tgroup, &b->keys, &b->vals,
                     &b->perm, &b->sort_tmp, &b->groups_main, &b->groups_pred, &b->tiles,
                     &b->items, &b->part, &b->bbox, &b->ctr, &b->err, &b->nearctr})
     x->release();

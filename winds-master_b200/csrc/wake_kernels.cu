@@ -152,12 +152,11 @@ __global__ void wake_filaments(const WakeCase *cases, const int *step, int step_
       lnew[slot] = L;
       if (rcout) rcout[slot] = rc;
     }
-    pack_filament(c.fil_off + f, x1, y1, z1, x2, y2, z2, g, rc, model, dcut, pf.fa, pf.fb, pf.fc,
-                  pf.fd, pf.ra, pf.rb);
+    pack_filament(c.fil_off + f, x1, y1, z1, x2, y2, z2, g, rc, model, dcut, pf.pk, pf.ra, pf.rb);
     lo[0] = (float)fmin(x1, x2), lo[1] = (float)fmin(y1, y2), lo[2] = (float)fmin(z1, z2);
     hi[0] = (float)fmax(x1, x2), hi[1] = (float)fmax(y1, y2), hi[2] = (float)fmax(z1, z2);
   } else if (f < c.fil_pad) {
-    pack_inert(c.fil_off + f, pf.fa, pf.fb, pf.fc, pf.fd, pf.ra, pf.rb);
+    pack_inert(c.fil_off + f, pf.pk, pf.ra, pf.rb);
   }
   bbox_accumulate(lo, hi, bb->fmin, bb->fmax);
 }

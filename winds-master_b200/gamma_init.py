@@ -168,19 +168,27 @@ def study(n_train: int = 400, n_test: int = 120, train_steps: int = 42, test_ste
     a = run(test_pts, test_steps, **kw)
     b = run(test_pts, test_steps, mlp=m, **kw)
     ia, ib = a["iters"], b["iters"]
+    # iterations are compared over (step, case) that converged in both runs;
+    # the converged circulation over cases that converged at every step
+    both = (ia < maxiter) & (ib < maxiter)
+    steady = both.copy()
+    steady[:skip] = False
+    ok_case = np.all(both, axis=0)
     rel = [float(np.abs(np.asarray(x) - np.asarray(y)).max() / (np.abs(np.asarray(x)).max() + 1.0))
-           for x, y in zip(a["bounds"][-1], b["bounds"][-1])]
+           for k, (x, y) in enumerate(zip(a["bounds"][-1], b["bounds"][-1])) if ok_case[k]]
     ms, nsteps = m.train_stats()
     return dict(
         model=m, train_points=len(train_pts), test_points=len(test_pts),
         pairs=int(keep.sum()), loss_first=float(losses[0]), loss_last=float(losses[-1]),
         data_s=t1 - t0, train_s=t2 - t1, train_device_ms=ms, adam_steps=nsteps,
-        iters_plain=int(ia.sum()), iters_mlp=int(ib.sum()),
-        iters_plain_steady=int(ia[skip:].sum()), iters_mlp_steady=int(ib[skip:].sum()),
+        iters_plain=int(ia[both].sum()), iters_mlp=int(ib[both].sum()),
+        iters_plain_steady=int(ia[steady].sum()), iters_mlp_steady=int(ib[steady].sum()),
         evals_plain=int(a["evals"].sum()), evals_mlp=int(b["evals"].sum()),
         converged_plain=float((ia < maxiter).mean()), converged_mlp=float((ib < maxiter).mean()),
-        saved=1.0 - ib.sum() / max(ia.sum(), 1), saved_steady=1.0 - ib[skip:].sum() / max(ia[skip:].sum(), 1),
-        cases_improved=int((ib.sum(0) < ia.sum(0)).sum()),
+        saved=1.0 - ib[both].sum() / max(ia[both].sum(), 1),
+        saved_steady=1.0 - ib[steady].sum() / max(ia[steady].sum(), 1),
+        cases_improved=int((np.where(both, ib, 0).sum(0) < np.where(both, ia, 0).sum(0)).sum()),
+        cases_compared=int(ok_case.sum()),
         bound_rel_diff_max=max(rel) if rel else 0.0,
         bound_rel_diff_median=float(np.median(rel)) if rel else 0.0,
         wall_plain_s=a["wall_s"], wall_mlp_s=b["wall_s"])
