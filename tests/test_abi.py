@@ -16,7 +16,7 @@ from conftest import ROOT
 
 def declared_functions():
     names = set()
-    for h in ("winds_bs.h", "mex.h", "matrix.h", "winds_wake.h", "winds_mlp.h"):
+    for h in ("winds_bs.h", "mex.h", "matrix.h", "winds_wake.h", "winds_mlp.h", "winds_kin.h"):
         path = os.path.join(ROOT, "include", h)
         if not os.path.exists(path):
             continue

@@ -24,7 +24,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O2", "-I" + INCLUDE, "-I" + CSRC]
 
 SOURCES = ["bs_kernels.cu", "engine.cu", "wake_kernels.cu", "wake_engine.cu", "kj_kernels.cu",
-           "mlp_kernels.cu", "mlp_engine.cu", "noalloc.cu", "mex_entry.cpp", "mx_shim.cpp"]
+           "mlp_kernels.cu", "mlp_engine.cu", "kin_kernels.cu", "noalloc.cu", "mex_entry.cpp", "mx_shim.cpp"]
 
 
 def nvcc() -> str:

@@ -420,3 +420,32 @@ def kj_features(kj: dict, s: int, bound, bound_last=None, uind=None) -> np.ndarr
             np.repeat(kj["twist"][:, None], nb, 1), np.repeat(np.sin(az)[None, :], ns, 0),
             np.repeat(np.cos(az)[None, :], ns, 0), vb[:, 0], vb[:, 1], vb[:, 2], bound, d]
     return np.stack([c.ravel(order="F") for c in cols], axis=1).astype(np.float32)
+
+
+def rotor_series(case: RotorCase, nsteps: int, pitch_deg: float = 0.0, tilt_deg: float = 5.0,
+                 precone_deg: float = -2.5, nac_yaw_deg: float = 0.0, platform_motion: bool = False,
+                 seed: int = 0) -> dict:
+    """Turbine time series and geometry in the form of core/kinematics.m's
+    inputs (fastout.*, blade.*, turbine.*): the synthetic blade (cosine
+    trailing nodes, stations at their midpoints, chord 3.5 -> 1.4 m, twist
+    13 -> 0 deg), constant rotor speed, blade pitch with a small per-blade
+    oscillation, nacelle yaw, and (optionally) a seeded platform motion."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    r, chord, twist = blade_geometry(case)
+    rm = 0.5 * (r[1:] + r[:-1])
+    s = (rm - case.r_root) / (case.R - case.r_root)
+    t = case.dt * np.arange(nsteps)
+    az = np.degrees(case.omega * t)
+    pitch = pitch_deg + 0.5 * np.sin(2 * np.pi * 0.1 * t[:, None] + np.arange(case.nb)[None, :])
+    ptfm = np.zeros((nsteps, 6))
+    if platform_motion:
+        amp = rng.uniform(0.2, 1.0, 6) * np.array([1.0, 0.5, 0.3, 2.0, 3.0, 1.5])
+        ph = rng.uniform(0, 2 * np.pi, 6)
+        ptfm = amp[None, :] * np.sin(2 * np.pi * 0.05 * t[:, None] + ph[None, :])
+    wind = np.zeros((nsteps, 3))
+    wind[:, 0] = case.U
+    return dict(time=t, azimuth=az, pitch=pitch, nac_yaw=np.full(nsteps, nac_yaw_deg), ptfm=ptfm,
+                wind=wind, r_trail=r, chord_trail=chord, twist_trail=np.degrees(twist), r_nodes=rm,
+                chord=3.5 + (1.4 - 3.5) * s, twist=13.0 * (1.0 - s),
+                precone=np.full(case.nb, precone_deg), overhang=-5.0, shaft_tilt=tilt_deg,
+                tower_ht=87.6, twr2shft=1.96, ptfm_ref=0.0)
