@@ -1,0 +1,130 @@
+"""Rotor model inputs in WInDS's own formats, and the wake / lifting-line
+cases built from them through the kinematics.
+
+  * ``read_airfoil(path)`` -- an AeroDyn airfoil table as
+    ``modeldata/NRELrotor.m:131-133`` reads it: 14 header lines, then rows of
+    AoA (deg), Cl, Cd, Cm; of two rows with the same AoA the first is dropped.
+  * ``stations(...)`` -- the blade stations of ``NRELrotor.m:40-47``: midpoints
+    of the trailing nodes, chord and twist interpolated linearly, the airfoil
+    index of the nearest trailing node (ties to the outer node), widths.
+  * ``operating_series(...)`` -- the turbine time series of ``NRELrotor.m``
+    for a constant wind, tip-speed ratio, pitch and nacelle yaw with the
+    platform at rest (``fastout.Azimuth = omega t``, ``RotSpeed``), from
+    ``t = -(na - 1) dt`` so the initial wake has a history.
+  * ``cases(...)`` -- a ``winds_wake_case`` and a ``winds_kj_case`` (dicts for
+    ``wake.WakeBatch`` / ``set_kj``) from the kinematics of that series.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+RHO = 1.225
+
+
+def read_airfoil(path: str) -> dict:
+    rows = []
+    with open(path) as f:
+        lines = f.read().splitlines()
+    for line in lines[14:]:
+        parts = line.split()
+        if len(parts) < 4:
+            continue
+        try:
+            rows.append([float(p) for p in parts[:4]])
+        except ValueError:
+            break
+    a = np.asarray(rows, dtype=np.float64)
+    keep = np.ones(len(a), dtype=bool)
+    keep[:-1] = np.diff(a[:, 0]) != 0  # NRELrotor.m:132-133
+    a = a[keep]
+    return dict(aoa=a[:, 0], cl=a[:, 1], cd=a[:, 2], cm=a[:, 3])
+
+
+def stations(r_trail, chord_trail, twist_trail, nfoil_trail) -> dict:
+    """Blade stations from trailing-node data (NRELrotor.m:40-47); ``nfoil``
+    is returned 1-based as in WInDS."""
+    rt = np.asarray(r_trail, np.float64)
+    rn = rt[:-1] + np.diff(rt) / 2
+    idx = np.searchsorted(rt, rn)               # rt[idx-1] < rn <= rt[idx]
+    lo = rt[idx - 1]
+    hi = rt[np.minimum(idx, len(rt) - 1)]
+    nearest = np.where(rn - lo < hi - rn, idx - 1, idx)
+    return dict(r_nodes=rn, chord=np.interp(rn, rt, chord_trail), twist=np.interp(rn, rt, twist_trail),
+                nfoil=np.asarray(nfoil_trail)[nearest].astype(np.int64), dr=np.abs(np.diff(rt)))
+
+
+def operating_series(model: dict, U=11.4, tsr=7.0, pitch=0.0, yaw=0.0, hz=10.0, nsteps=51,
+                     na=40) -> dict:
+    """Turbine time series (kinematics inputs) of a steady operating point,
+    samples ``-(na-1) .. nsteps`` at ``hz``."""
+    R = float(model["r_trail"][-1])
+    omega = tsr * U / R
+    t = (np.arange(-(na - 1), nsteps + 1)) / hz
+    nt, nb = t.size, int(model["nb"])
+    st = stations(model["r_trail"], model["chord_trail"], model["twist_trail"], model["nfoil_trail"])
+    wind = np.zeros((nt, 3))
+    wind[:, 0] = U
+    return dict(time=t, azimuth=omega * (180.0 / np.pi) * t, pitch=np.full((nt, nb), pitch),
+                nac_yaw=np.full(nt, yaw), ptfm=np.zeros((nt, 6)), wind=wind,
+                r_trail=model["r_trail"], chord_trail=model["chord_trail"],
+                twist_trail=model["twist_trail"], r_nodes=st["r_nodes"], chord=st["chord"],
+                twist=st["twist"], precone=np.full(nb, model["precone"]), overhang=model["overhang"],
+                shaft_tilt=model["shaft_tilt"], tower_ht=model["tower_ht"], twr2shft=model["twr2shft"],
+                ptfm_ref=0.0, _omega=omega, _U=U, _pitch=pitch, _na=na, _nsteps=nsteps, _hz=hz)
+
+
+def cases(model: dict, series: dict, kin: dict, rc0=0.1, delta=100.0, nu=1.5e-5, alpha=1.25643) -> tuple:
+    """(wake case, lifting-line case) from a series and its kinematics
+    ``kin`` (device ``kin.kinematics`` or the oracle): step 0 at t = 0, the
+    wake's older columns the trailing edge of earlier steps convected with the
+    wind; bound circulation starting at zero."""
+    na, nsteps, hz, U = series["_na"], series["_nsteps"], series["_hz"], series["_U"]
+    s0 = na - 1
+    nb = int(model["nb"])
+    nst = len(model["r_trail"])
+    ns = nst - 1
+    dt = 1.0 / hz
+    f = np.asfortranarray
+    quarter = kin["quarter"][:, :, s0:, :]
+    trail = kin["trail"][:, :, s0:, :]
+    dom = np.zeros((nst, 3, na, nb))
+    dom[:, :, 0, :] = quarter[:, :, 0, :]
+    dom[:, :, 1, :] = trail[:, :, 0, :]
+    for j in range(2, na):
+        te = kin["trail"][:, :, s0 - (j - 1), :].copy()
+        te[:, 0, :] += U * (j - 1) * dt
+        dom[:, :, j, :] = te
+    wind = np.zeros((3, nsteps + 1))
+    wind[0] = U
+    wake = dict(nst=nst, nb=nb, na=na, nsteps=nsteps + 1, dt=dt, t0=0.0, quarter=f(quarter),
+                trailing=f(trail), wind=f(wind), shear=0.0, hub_height=float(model["tower_ht"]),
+                core_mode=1, r0=rc0, rc0=rc0, alpha=alpha, nu=nu, a1=0.0, delta=delta, dom=f(dom),
+                bound=f(np.zeros((ns, nb))), trail_gamma=f(np.zeros((nst, na - 1, nb))))
+    st = stations(model["r_trail"], model["chord_trail"], model["twist_trail"], model["nfoil_trail"])
+    tabs = model["tables"]
+    R = float(model["r_trail"][-1])
+    az = np.radians(series["azimuth"][s0:])[:, None] + 2 * np.pi * np.arange(nb)[None, :] / nb
+    kj = dict(ll=f(kin["bound"][:, :, s0:, :]), bxn=f(kin["bxn"][:, :, s0:, :]),
+              byn=f(kin["byn"][:, :, s0:, :]), bzn=f(kin["bzn"][:, :, s0:, :]),
+              vblade=f(kin["vblade"][:, :, s0:, :]), chord=st["chord"],
+              foil=(st["nfoil"] - 1).astype(np.int32),
+              foil_points=np.array([len(t["aoa"]) for t in tabs], dtype=np.int32),
+              aoa=np.concatenate([t["aoa"] for t in tabs]), cl=np.concatenate([t["cl"] for t in tabs]),
+              cd=np.concatenate([t["cd"] for t in tabs]), r_over_R=st["r_nodes"] / R,
+              chord_over_R=st["chord"] / R, twist=np.radians(st["twist"] + series["_pitch"]),
+              azimuth=f(az), r_station=st["r_nodes"], dr_station=st["dr"],
+              rpm=np.full(nsteps + 1, series["_omega"] * 30.0 / np.pi), rho=RHO)
+    return wake, kj
+
+
+def load_model(path: str) -> dict:
+    """A rotor model saved as by ``tests/golden/make_nrel.py``: trailing-node
+    geometry, airfoil index, turbine constants and the airfoil tables."""
+    d = np.load(path, allow_pickle=False)
+    names = [str(n) for n in d["names"]]
+    model = {k: d[k] for k in ("r_trail", "chord_trail", "twist_trail", "nfoil_trail")}
+    for k in ("nb", "tower_ht", "twr2shft", "shaft_tilt", "precone", "overhang"):
+        model[k] = float(d[k]) if k != "nb" else int(d[k])
+    model["names"] = names
+    model["tables"] = [dict(aoa=d[f"aoa_{k}"], cl=d[f"cl_{k}"], cd=d[f"cd_{k}"]) for k in range(len(names))]
+    return model
