@@ -120,7 +120,7 @@ def test_every_tiling_agrees(wb, synth, oracle):
     nt = P.shape[0] * P.shape[2] * P.shape[3]
     nf = sum(f[0].shape[0] * f[0].shape[2] * f[0].shape[3] for f in fams)
     uo = sum(oracle.c_eval(F1, F2, P, g, rc, "visc2", 1000.0) for F1, F2, g, rc in fams)
-    for T in (2, 4, 8):
+    for T in (2, 3, 4, 8):
         for KF in (32, 64, 128):
             for waves in (1.0, 16.0):
                 wb.set_tuning(wb.bs.CORE_VATISTAS, nt, nf, T, KF, waves)

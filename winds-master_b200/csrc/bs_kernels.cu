@@ -478,11 +478,12 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, con
 }
 
 // Resident CTAs per SM the register allocation is capped for: 6 for T = 2
-// (80 registers), 4 for T = 4 (128), 2 for T = 8 (255). The packed loop keeps
-// each target as broadcast pairs and its sums as pairs (12 registers a target).
+// (80 registers), 5 for T = 3 (96), 4 for T = 4 (128), 2 for T = 8 (255). The
+// packed loop keeps each target as broadcast pairs and its sums as pairs (12
+// registers a target).
 template <int T>
 struct MinBlocks {
-  static constexpr int value = T <= 2 ? 6 : (T <= 4 ? 4 : 2);
+  static constexpr int value = T <= 2 ? 6 : (T == 3 ? 5 : (T <= 4 ? 4 : 2));
 };
 
 template <int T, int KF, int MODEL>
@@ -773,11 +774,15 @@ int occupancy_t() {
 #define WINDS_F32C_DISPATCH(FN, ...)                                                    \
   switch (model * 1000 + T * 100 + KF / 32) {                                          \
     WINDS_F32C_CASE(FN, 0, 2, 32, __VA_ARGS__) WINDS_F32C_CASE(FN, 0, 2, 64, __VA_ARGS__) \
-    WINDS_F32C_CASE(FN, 0, 2, 128, __VA_ARGS__) WINDS_F32C_CASE(FN, 0, 4, 32, __VA_ARGS__) \
+    WINDS_F32C_CASE(FN, 0, 2, 128, __VA_ARGS__) WINDS_F32C_CASE(FN, 0, 3, 32, __VA_ARGS__) \
+    WINDS_F32C_CASE(FN, 0, 3, 64, __VA_ARGS__) WINDS_F32C_CASE(FN, 0, 3, 128, __VA_ARGS__) \
+    WINDS_F32C_CASE(FN, 0, 4, 32, __VA_ARGS__) \
     WINDS_F32C_CASE(FN, 0, 4, 64, __VA_ARGS__) WINDS_F32C_CASE(FN, 0, 4, 128, __VA_ARGS__) \
     WINDS_F32C_CASE(FN, 0, 8, 32, __VA_ARGS__) WINDS_F32C_CASE(FN, 0, 8, 64, __VA_ARGS__) \
     WINDS_F32C_CASE(FN, 0, 8, 128, __VA_ARGS__) WINDS_F32C_CASE(FN, 1, 2, 32, __VA_ARGS__) \
     WINDS_F32C_CASE(FN, 1, 2, 64, __VA_ARGS__) WINDS_F32C_CASE(FN, 1, 2, 128, __VA_ARGS__) \
+    WINDS_F32C_CASE(FN, 1, 3, 32, __VA_ARGS__) WINDS_F32C_CASE(FN, 1, 3, 64, __VA_ARGS__) \
+    WINDS_F32C_CASE(FN, 1, 3, 128, __VA_ARGS__) \
     WINDS_F32C_CASE(FN, 1, 4, 32, __VA_ARGS__) WINDS_F32C_CASE(FN, 1, 4, 64, __VA_ARGS__) \
     WINDS_F32C_CASE(FN, 1, 4, 128, __VA_ARGS__) WINDS_F32C_CASE(FN, 1, 8, 32, __VA_ARGS__) \
     WINDS_F32C_CASE(FN, 1, 8, 64, __VA_ARGS__) WINDS_F32C_CASE(FN, 1, 8, 128, __VA_ARGS__) \
@@ -786,7 +791,7 @@ int occupancy_t() {
 }  // namespace
 
 bool f32c_config_supported(int T, int KF) {
-  return (T == 2 || T == 4 || T == 8) && (KF == 32 || KF == 64 || KF == 128);
+  return (T == 2 || T == 3 || T == 4 || T == 8) && (KF == 32 || KF == 64 || KF == 128);
 }
 
 int f32c_threads() { return kThreads; }
