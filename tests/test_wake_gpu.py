@@ -89,3 +89,17 @@ def test_kinematics_limit_is_enforced(wb, synth):
     batch = wake.WakeBatch(_cases(synth), integrator="fe")
     with pytest.raises(wb.WindsError):
         batch.step(20)
+
+
+def test_first_step_autotunes_the_batch_tiling(wb, synth):
+    """An FP32c batch whose size has no cached tiling times the candidates on
+    its first step and caches the fastest for its size bucket."""
+    wake = __import__("importlib").import_module("winds-master_b200.wake")
+    cases = [synth.make_wake_case(rc, nsteps=4) for rc in synth.batch_cases(5, seed=77, steps_range=(300, 400))]
+    nodes = sum(c["nst"] * c["na"] * c["nb"] for c in cases)
+    fil = sum(((c["nst"] - 1) * c["na"] + c["nst"] * (c["na"] - 1)) * c["nb"] for c in cases)
+    b = wake.WakeBatch(cases, integrator="fe", precision="f32c")
+    b.step(1)
+    T, KF, waves = wb.get_tuning(wb.bs.CORE_VATISTAS, nodes, fil)
+    assert T in (3, 4) and KF in (64, 128) and waves in (16.0, 32.0)
+    b.close()

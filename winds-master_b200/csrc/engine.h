@@ -80,6 +80,7 @@ int resolve_model(const winds_bs_params *prm, int *model, double *dcut, double *
 int validate_family(const winds_bs_family &f);
 TuneChoice default_choice(long long nt);
 bool lookup_tune(int model, long long nt, long long nf, TuneChoice *out);
+void store_tune(int model, long long nt, long long nf, const TuneChoice &ch);
 int cuda_fail(cudaError_t e, const char *what);
 Context *get_context(int *rc);
 int eval_device(Context *c, const winds_bs_family *fams, int nfam,

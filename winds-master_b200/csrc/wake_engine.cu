@@ -53,6 +53,7 @@ struct winds_wake_batch {
   int n_tiles = 0, n_items = 0, tile_cap = 0, grid = 0;
   TuneChoice ch;
   long long steps_done = 0;
+  bool tuned = true;         // tiling from the autotuner's cache (or not FP32c)
   long long min_nsteps = 0;  // kinematics rows available in every case
   int timed_steps = 0;       // steps between ev0 and ev1
   // Kutta-Joukowski lifting lines
@@ -551,7 +552,7 @@ int winds_wake_create(const winds_wake_case *cases, int ncases, const winds_wake
   }
   b->ch = default_choice(node);
   b->ch.waves = 32.0;
-  if (prec == WINDS_PREC_F32C) lookup_tune(model, node, fil, &b->ch);
+  if (prec == WINDS_PREC_F32C) b->tuned = lookup_tune(model, node, fil, &b->ch);
   if ((rc = alloc_all(b)) || (rc = build_plans(b))) {
     winds_wake_destroy(b);
     return rc;
@@ -625,6 +626,60 @@ int winds_wake_create(const winds_wake_case *cases, int ncases, const winds_wake
   return WINDS_BS_OK;
 }
 
+static int device_error_word(winds_wake_batch *b);
+
+// First-step tiling choice for an FP32c batch the cache has no entry for:
+// times the main evaluation of this batch for T in {3, 4}, KF in {64, 128}
+// and 16 or 32 items per resident CTA, keeps the fastest (cached for the
+// batch's size bucket) and rebuilds the plan. The evaluations only write
+// per-step scratch (velocities, cores, lengths) that the first step rewrites.
+static int autotune_batch(winds_wake_batch *b) {
+  int rc;
+  Context *c = get_context(&rc);
+  if (!c) return rc;
+  b->tuned = true;
+  if (!c->autotune) return build_plans(b);
+  cudaStream_t s = b->stream;
+  cudaError_t e = launch_wake_bookkeep(P<const WakeCase>(b->cases_d), b->ncases, b->max_cols,
+                                       P<const double>(b->bound), P<const double>(b->trail_prev),
+                                       P<double>(b->shed_cur), P<double>(b->trail_cur), s);
+  if (e != cudaSuccess) return cuda_fail(e, "autotune bookkeeping");
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  TuneChoice best = b->ch;
+  float best_ms = 1e30f;
+  for (int T : {3, 4})
+    for (int KF : {64, 128})
+      for (double w : {16.0, 32.0}) {
+        b->ch.T = T, b->ch.KF = KF, b->ch.waves = w;
+        if ((rc = build_plans(b))) break;
+        float ms = 0.f;
+        for (int rep = 0; rep < 2 && e == cudaSuccess; ++rep) {  // warm-up, then timed
+          int l = 0;
+          cudaEventRecord(e0, s);
+          e = enqueue_eval(b, P<const double>(b->dom), P<const double>(b->shed_cur),
+                           P<const double>(b->trail_cur), 0, P<const double>(b->len_old_s),
+                           P<const double>(b->len_old_t), 1, P<double>(b->len_s),
+                           P<double>(b->len_t), P<double>(b->rc_s), P<double>(b->rc_t),
+                           b->groups_main, l);
+          cudaEventRecord(e1, s);
+          if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+          cudaEventElapsedTime(&ms, e0, e1);
+        }
+        if (e != cudaSuccess) break;
+        if (ms < best_ms) best_ms = ms, best = b->ch;
+      }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  if (e != cudaSuccess) return cuda_fail(e, "wake autotune");
+  if ((rc = device_error_word(b))) return rc;
+  b->ch = best;
+  store_tune(b->model, b->nodes, b->fil_pad, best);
+  return build_plans(b);
+}
+
 // Error word of the direct-sum kernels (bounded waits that ran out).
 static int device_error_word(winds_wake_batch *b) {
   unsigned word = 0;
@@ -644,6 +699,10 @@ int winds_wake_step(winds_wake_batch *b, int nsteps, int use_graph) {
     return fail(WINDS_BS_ERR_ARG, "kinematics cover %lld steps; %lld done, %d more requested",
                 b->min_nsteps - 1, b->steps_done, nsteps);
   cudaSetDevice(b->dev);
+  if (!b->tuned && nsteps > 0) {
+    int rc = autotune_batch(b);
+    if (rc) return rc;
+  }
   cudaError_t e = cudaSuccess;
   if (b->kj) {
     // pre-commit part, the iteration (host loop on a device convergence flag), commit
