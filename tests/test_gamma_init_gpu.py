@@ -49,6 +49,37 @@ def test_features_and_start_value_match_host(wb):
     m.close()
 
 
+def test_graph_with_network_matches_host_loop(wb):
+    """With the network attached, the captured step (network forward inside
+    the graph, iteration as a conditional node) gives the host loop's results
+    bit for bit, and a new output scale set after capture reaches it."""
+    gi, mlp, wake, synth = _mods()
+    pts = gi.operating_points(3, seed=7, nst=13, wake_steps=10)
+    m = mlp.Mlp(gi.N_FEATURES, seed=3)
+    m.set_scaling(np.zeros(10, np.float32), np.full(10, 0.2, np.float32), 0.02)
+    ra = gi.run(pts, 3, mlp=m, graph=False)
+    rb = gi.run(pts, 3, mlp=m, graph=True)
+    np.testing.assert_array_equal(ra["iters"], rb["iters"])
+    np.testing.assert_array_equal(ra["evals"], rb["evals"])
+    for sa, sb in zip(ra["bounds"], rb["bounds"]):
+        for a, c in zip(sa, sb):
+            np.testing.assert_array_equal(a, c)
+    cases, kjs = gi.build(pts, 4)
+    b = wake.WakeBatch(cases, integrator="pcc")
+    b.set_kj(kjs, relax=0.3, tol=1e-6, maxiter=100)
+    b.set_mlp(m)
+    b.step(1, graph=True)
+    prev = [b.bound(k) for k in range(3)]
+    m.set_scaling(np.zeros(10, np.float32), np.full(10, 0.2, np.float32), 0.3)
+    b.step(1, graph=True)
+    for k in range(3):
+        x = b.kj_features(k)
+        gh = prev[k].ravel(order="F") + float(np.float32(0.3)) * m.forward(x).astype(np.float64)
+        np.testing.assert_allclose(b.kj_guess(k).ravel(order="F"), gh, rtol=1e-12, atol=1e-9)
+    b.close()
+    m.close()
+
+
 def test_trained_start_value_saves_iterations(wb):
     """Trained on plain-solver pairs (~4.5e5) of the attached-flow operating
     points among 400 candidates, the network's start value needs fewer

@@ -75,23 +75,40 @@ def test_kj_step_matches_oracle(wb, synth, prec):
         assert nev == int(iters.max())
 
 
-def test_kj_graph_replay_is_bit_identical(wb, synth):
+@pytest.mark.parametrize("maxiter", [25, 2])
+def test_kj_graph_replay_is_bit_identical(wb, synth, maxiter):
+    """The graph path runs each step as one graph whose lifting-line
+    iteration is a conditional WHILE node (no host round trip per iteration);
+    it must give the host-driven loop's results bit for bit, including the
+    iteration counts and the stop at maxiter."""
     wake = importlib.import_module("winds-master_b200.wake")
     cases = _cases(synth)
     out = []
     for graph in (False, True):
         b = wake.WakeBatch([c for c, _ in cases], integrator="pcc")
-        b.set_kj([k for _, k in cases], relax=0.3, tol=1e-4, maxiter=25)
-        b.step(3, graph=graph)
-        out.append([b.state(k) for k in range(2)] + [b.kj_stats()[0]])
+        b.set_kj([k for _, k in cases], relax=0.3, tol=1e-4, maxiter=maxiter)
+        rec = []
+        for _ in range(3):
+            b.step(1, graph=graph)
+            iters, res, nev = b.kj_stats()
+            rec.append((iters.copy(), res.copy(), nev, b.loads()))
+        out.append(([b.state(k) for k in range(2)], rec))
         b.close()
     for k in range(2):
         for key in ("dom", "bound", "shed", "trail"):
-            np.testing.assert_array_equal(out[0][k][key], out[1][k][key])
-    np.testing.assert_array_equal(out[0][2], out[1][2])
+            np.testing.assert_array_equal(out[0][0][k][key], out[1][0][k][key])
+    for (i0, r0, n0, l0), (i1, r1, n1, l1) in zip(out[0][1], out[1][1]):
+        np.testing.assert_array_equal(i0, i1)
+        np.testing.assert_array_equal(r0, r1)
+        assert n0 == n1 and n0 == i0.max() and n0 <= maxiter
+        for a, c in zip(l0, l1):
+            np.testing.assert_array_equal(a, c)
+    if maxiter == 2:
+        assert all((r[0] == 2).all() for r in out[1][1])
 
 
-def test_kj_diverged_reports_error(wb, synth):
+@pytest.mark.parametrize("graph", [False, True])
+def test_kj_diverged_reports_error(wb, synth, graph):
     """An angle of attack outside the airfoil table gives NaN Cl; the solver
     stops with the reference's 'Diverging soln!!!' as an error code."""
     wake = importlib.import_module("winds-master_b200.wake")
@@ -107,7 +124,7 @@ def test_kj_diverged_reports_error(wb, synth):
     b = wake.WakeBatch([c for c, _ in cases], integrator="fe", precision="f64")
     b.set_kj(kjs, relax=0.3, tol=1e-4, maxiter=5)
     with pytest.raises(bs.WindsError) as ei:
-        b.step(1)
+        b.step(1, graph=graph)
     assert ei.value.code == 6
     # the context stays usable
     b.close()

@@ -126,14 +126,14 @@ __global__ void kj_features(const WakeCase *cases, const KJCase *kc, const int *
 }
 
 __global__ void kj_apply_guess(const WakeCase *cases, const KJCase *kc, const float *y,
-                               float out_scale, double *bound) {
+                               const float *out_scale, double *bound) {
   const WakeCase c = cases[blockIdx.y];
   const KJCase k = kc[blockIdx.y];
   const int ns = c.nst - 1;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ns * c.nb) return;
   const int i = t % ns, b = t / ns;
-  bound[c.bound_off + i + (long long)ns * b] += (double)out_scale * (double)y[k.t_off + t];
+  bound[c.bound_off + i + (long long)ns * b] += (double)*out_scale * (double)y[k.t_off + t];
 }
 
 // Spanwise loads of one station (postproc/perform.m:20-55): the blade-frame
@@ -213,6 +213,42 @@ __global__ void kj_check(int ncases, double tol, int *converged, int *iters,
   if (r <= tol) converged[ci] = 1; else atomicOr(active, 1);
 }
 
+// kj_check inside a graph's conditional WHILE node: the same per-case update,
+// then one thread sets the loop condition -- continue while any case is active
+// and fewer than maxiter iterations ran (the counter makes the loop finite).
+__global__ void kj_check_cond(int ncases, double tol, int *converged, int *iters,
+                              unsigned long long *res_max, double *res_last, int *active,
+                              int *it_ctr, int maxiter, cudaGraphConditionalHandle h) {
+  __shared__ int any;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
+  for (int ci = threadIdx.x; ci < ncases; ci += blockDim.x) {
+    if (converged[ci]) continue;
+    const double r = __longlong_as_double((long long)res_max[ci]);
+    res_max[ci] = 0ull;
+    res_last[ci] = r;
+    iters[ci] += 1;
+    if (r <= tol) converged[ci] = 1; else atomicOr(&any, 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    *active = any;
+    const int it = *it_ctr + 1;
+    *it_ctr = it;
+    cudaGraphSetConditional(h, (any && it < maxiter) ? 1u : 0u);
+  }
+}
+
+cudaError_t launch_kj_check_cond(int ncases, double tol, int *converged, int *iters,
+                                 unsigned long long *res_max, double *res_last, int *active,
+                                 int *it_ctr, int maxiter, cudaGraphConditionalHandle h,
+                                 cudaStream_t s) {
+  const int bs = ncases <= 1024 ? ((ncases + 31) / 32) * 32 : 1024;
+  kj_check_cond<<<1, bs, 0, s>>>(ncases, tol, converged, iters, res_max, res_last, active, it_ctr,
+                                 maxiter, h);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_kj_targets(const WakeCase *cases, const KJCase *kc, int ncases, int max_st,
                               const int *step, const double *ll, double4 *tp, BBox *bb,
                               cudaStream_t s) {
@@ -247,7 +283,7 @@ cudaError_t launch_kj_features(const WakeCase *cases, const KJCase *kc, int ncas
 }
 
 cudaError_t launch_kj_apply_guess(const WakeCase *cases, const KJCase *kc, int ncases, int max_st,
-                                  const float *y, float out_scale, double *bound, cudaStream_t s) {
+                                  const float *y, const float *out_scale, double *bound, cudaStream_t s) {
   kj_apply_guess<<<dim3((max_st + 127) / 128, ncases), 128, 0, s>>>(cases, kc, y, out_scale, bound);
   return cudaGetLastError();
 }

@@ -46,7 +46,7 @@ cudaError_t launch_kj_features(const WakeCase *cases, const KJCase *kc, int ncas
                                float *x, cudaStream_t s);
 // bound += out_scale * y (row order of the lifting-line targets)
 cudaError_t launch_kj_apply_guess(const WakeCase *cases, const KJCase *kc, int ncases, int max_st,
-                                  const float *y, float out_scale, double *bound, cudaStream_t s);
+                                  const float *y, const float *out_scale, double *bound, cudaStream_t s);
 // Rotor thrust, torque and power of every case at the step
 // (postproc/perform.m:18-62): out[3*case + {0,1,2}] = T, Q, P; dl [rows][3]
 // holds the spanwise terms.
@@ -55,6 +55,11 @@ cudaError_t launch_kj_loads(const WakeCase *cases, const KJCase *kc, int ncases,
                             const double *cd, const double *aoa, const double *st_tw,
                             const double *chord, const double *st_rr, const double *st_dr,
                             const double *rpm, double *dl, double *out, cudaStream_t s);
+// kj_check that also sets a graph WHILE condition (see kj_kernels.cu).
+cudaError_t launch_kj_check_cond(int ncases, double tol, int *converged, int *iters,
+                                 unsigned long long *res_max, double *res_last, int *active,
+                                 int *it_ctr, int maxiter, cudaGraphConditionalHandle h,
+                                 cudaStream_t s);
 cudaError_t launch_kj_check(int ncases, double tol, int *converged, int *iters,
                             unsigned long long *res_max, double *res_last, int *active,
                             cudaStream_t s);

@@ -245,6 +245,8 @@ int mlp_forward(const winds_mlp *m, const __nv_bfloat16 *X, long long n, MlpWork
 const float *mlp_shift_dev(const winds_mlp *m) { return static_cast<const float *>(m->shift.p); }
 const float *mlp_scale_dev(const winds_mlp *m) { return static_cast<const float *>(m->scale.p); }
 float mlp_out_scale(const winds_mlp *m) { return m->out_scale; }
+// out_scale on the device (after the 16 input scales), read when a captured step replays
+const float *mlp_out_scale_dev(const winds_mlp *m) { return static_cast<const float *>(m->scale.p) + 16; }
 int mlp_n_in(const winds_mlp *m) { return m->n_in; }
 int mlp_device(const winds_mlp *m) { return m->dev; }
 unsigned *mlp_err_word(const winds_mlp *m) { return static_cast<unsigned *>(m->err.p); }
@@ -276,7 +278,7 @@ int winds_mlp_create(const winds_mlp_config *cfg, winds_mlp **out) {
   if ((rc = m->theta.ensure(kNParam * 4, s)) || (rc = m->theta_bf.ensure(kNParam * 2, s)) ||
       (rc = m->grad.ensure(kNParam * 4, s)) || (rc = m->mom.ensure(kNParam * 4, s)) ||
       (rc = m->vel.ensure(kNParam * 4, s)) || (rc = m->shift.ensure(64, s)) ||
-      (rc = m->scale.ensure(64, s)) || (rc = m->err.ensure(16, s)) ||
+      (rc = m->scale.ensure(128, s)) || (rc = m->err.ensure(16, s)) ||
       (rc = m->jobs.ensure(32 * sizeof(MlpReduceJob), s)) || (rc = m->loss.ensure(16, s))) {
     winds_mlp_destroy(m);
     return rc;
@@ -296,6 +298,8 @@ int winds_mlp_create(const winds_mlp_config *cfg, winds_mlp **out) {
   e = cudaMemcpy(m->theta.p, th.data(), kNParam * 4, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(m->shift.p, m->h_shift, 64, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(m->scale.p, m->h_scale, 64, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(P<float>(m->scale) + 16, &m->out_scale, 4, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemset(m->mom.p, 0, kNParam * 4);
   if (e == cudaSuccess) e = cudaMemset(m->vel.p, 0, kNParam * 4);
   if (e == cudaSuccess) e = cudaMemset(m->err.p, 0, 16);
@@ -348,6 +352,7 @@ int winds_mlp_set_scaling(winds_mlp *m, const float *shift, const float *scale, 
   cudaStreamSynchronize(m->stream);
   cudaError_t e = cudaMemcpy(m->shift.p, m->h_shift, 64, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(m->scale.p, m->h_scale, 64, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(P<float>(m->scale) + 16, &out_scale, 4, cudaMemcpyHostToDevice);
   return e == cudaSuccess ? WINDS_BS_OK : cuda_fail(e, "mlp scaling");
 }
 

@@ -76,6 +76,13 @@ struct winds_wake_batch {
   MlpWork mw;
   cudaGraphExec_t exec_pre = nullptr, exec_kj = nullptr, exec_post = nullptr;
   cudaGraph_t g_pre = nullptr, g_kj = nullptr, g_post = nullptr;
+  // whole step with the iteration as a conditional WHILE node (no host round trip)
+  cudaGraphExec_t exec_step = nullptr;
+  cudaGraph_t g_step = nullptr;
+  cudaStream_t body_stream = nullptr;
+  bool cond_ok = true;  // false after a failed build: host loop instead
+  int step_launches = 0;
+  DevBuf kj_it;         // iterations run in the current step
 };
 
 namespace {
@@ -332,8 +339,8 @@ cudaError_t enqueue_step(winds_wake_batch *b, int &launches) {
 // One Kutta-Joukowski iteration of every active case: Γ from the bound
 // iterate, filaments with the step's cores, induced velocity at the lifting
 // lines, station update and per-case convergence.
-cudaError_t enqueue_kj_iter(winds_wake_batch *b, int &launches) {
-  cudaStream_t s = b->stream;
+cudaError_t enqueue_kj_iter(winds_wake_batch *b, int &launches, cudaStream_t s,
+                            const cudaGraphConditionalHandle *cond = nullptr) {
   const WakeCase *cd = P<const WakeCase>(b->cases_d);
   const KJCase *kd = P<const KJCase>(b->kjc_d);
   PackedFilaments pf{P<float4>(b->pk),
@@ -385,8 +392,12 @@ cudaError_t enqueue_kj_iter(winds_wake_batch *b, int &launches) {
                          P<unsigned long long>(b->res_max), P<int>(b->diverged), P<double>(b->cl_o),
                          P<double>(b->cd_o), P<double>(b->aoa_o), s);
   if (e == cudaSuccess)
-    e = launch_kj_check(b->ncases, b->kjp.tol, P<int>(b->conv), P<int>(b->iters),
-                        P<unsigned long long>(b->res_max), P<double>(b->res_last), P<int>(b->active), s);
+    e = cond ? launch_kj_check_cond(b->ncases, b->kjp.tol, P<int>(b->conv), P<int>(b->iters),
+                                    P<unsigned long long>(b->res_max), P<double>(b->res_last),
+                                    P<int>(b->active), P<int>(b->kj_it), b->kjp.maxiter, *cond, s)
+             : launch_kj_check(b->ncases, b->kjp.tol, P<int>(b->conv), P<int>(b->iters),
+                               P<unsigned long long>(b->res_max), P<double>(b->res_last),
+                               P<int>(b->active), s);
   launches = 8;
   return e;
 }
@@ -401,6 +412,7 @@ cudaError_t enqueue_kj_begin(winds_wake_batch *b) {
                           P<double4>(b->tp_ll), P<BBox>(b->bbox), s);
   for (DevBuf *x : {&b->conv, &b->iters, &b->diverged, &b->res_max})
     if (e == cudaSuccess) e = cudaMemsetAsync(x->p, 0, b->ncases * 8, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(b->kj_it.p, 0, sizeof(int), s);
   const WakeCase *cd = P<const WakeCase>(b->cases_d);
   const KJCase *kd = P<const KJCase>(b->kjc_d);
   if (e == cudaSuccess && b->mlp_inputs)
@@ -424,12 +436,82 @@ cudaError_t enqueue_kj_begin(winds_wake_batch *b) {
       e = cudaErrorLaunchFailure;
     if (e == cudaSuccess)
       e = launch_kj_apply_guess(cd, kd, b->ncases, b->max_st, P<const float>(b->mw.y),
-                                mlp_out_scale(b->mlp), P<double>(b->bound), s);
+                                mlp_out_scale_dev(b->mlp), P<double>(b->bound), s);
   }
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(b->guess.p, b->bound.p, b->bound_n * sizeof(double),
                         cudaMemcpyDeviceToDevice, s);
   return e;
+}
+
+int kj_step_errors(winds_wake_batch *b);
+
+// One step as one graph: the part before the iteration, the lifting-line set-up,
+// a conditional WHILE node whose body is one iteration (kj_check_cond ends it),
+// then the commit. Built once, replayed every step.
+int build_step_graph(winds_wake_batch *b) {
+  cudaStream_t s = b->stream;
+  cudaError_t e = cudaSuccess;
+  if (!b->body_stream) e = cudaStreamCreateWithFlags(&b->body_stream, cudaStreamNonBlocking);
+  int l1 = 0, l2 = 0, l3 = 0;
+  cudaGraph_t g = nullptr;
+  bool capturing = false;
+  if (e == cudaSuccess) e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+  capturing = e == cudaSuccess;
+  if (e == cudaSuccess) e = enqueue_pre(b, l1);
+  if (e == cudaSuccess) e = enqueue_kj_begin(b);
+  cudaGraphConditionalHandle h = 0;
+  cudaGraphNode_t node = nullptr;
+  if (e == cudaSuccess) {
+    cudaStreamCaptureStatus st;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    e = cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &ndeps);
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+    // zero-filled storage: the parameter union has no usable default constructor
+    union NodeParams {
+      cudaGraphNodeParams p;
+      unsigned char raw[sizeof(cudaGraphNodeParams)];
+      NodeParams() { std::memset(raw, 0, sizeof(raw)); }
+      ~NodeParams() {}
+    } np;
+    cudaGraphNodeParams &cp = np.p;
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    if (e == cudaSuccess) e = cudaGraphAddNode(&node, g, deps, ndeps, &cp);
+    if (e == cudaSuccess)
+      e = cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
+    if (e == cudaSuccess) {
+      cudaGraph_t body = cp.conditional.phGraph_out[0];
+      e = cudaStreamBeginCaptureToGraph(b->body_stream, body, nullptr, nullptr, 0,
+                                        cudaStreamCaptureModeThreadLocal);
+      if (e == cudaSuccess) {
+        cudaError_t e2 = enqueue_kj_iter(b, l2, b->body_stream, &h);
+        e = cudaStreamEndCapture(b->body_stream, &body);
+        if (e2 != cudaSuccess) e = e2;
+      }
+    }
+  }
+  if (e == cudaSuccess) e = enqueue_post(b, l3);
+  if (capturing) {
+    cudaGraph_t done = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(s, &done);
+    if (e == cudaSuccess) e = e2;
+    g = done;
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec_step, g, 0);
+  if (e != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    b->exec_step = nullptr;
+    b->g_step = nullptr;
+    cudaGetLastError();
+    return cuda_fail(e, "step graph with conditional iteration");
+  }
+  b->g_step = g;
+  b->step_launches = l1 + l2 + l3;
+  return WINDS_BS_OK;
 }
 
 int run_kj(winds_wake_batch *b, bool use_graph) {
@@ -438,7 +520,7 @@ int run_kj(winds_wake_batch *b, bool use_graph) {
   if (use_graph && !b->exec_kj) {
     int l = 0;
     e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
-    cudaError_t e2 = e == cudaSuccess ? enqueue_kj_iter(b, l) : e;
+    cudaError_t e2 = e == cudaSuccess ? enqueue_kj_iter(b, l, b->stream) : e;
     e = cudaStreamEndCapture(b->stream, &b->g_kj);
     if (e2 != cudaSuccess) e = e2;
     if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec_kj, b->g_kj, 0);
@@ -448,15 +530,20 @@ int run_kj(winds_wake_batch *b, bool use_graph) {
   int active = 1;
   for (int it = 0; it < b->kjp.maxiter && active; ++it) {
     int l = 0;
-    e = use_graph ? cudaGraphLaunch(b->exec_kj, b->stream) : enqueue_kj_iter(b, l);
+    e = use_graph ? cudaGraphLaunch(b->exec_kj, b->stream) : enqueue_kj_iter(b, l, b->stream);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(&active, b->active.p, sizeof(int), cudaMemcpyDeviceToHost, b->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
     if (e != cudaSuccess) return cuda_fail(e, "kj iteration");
     ++b->kj_evals;
   }
+  return kj_step_errors(b);
+}
+
+// After a step's iteration: NaN Cl anywhere, or an error word of the network.
+int kj_step_errors(winds_wake_batch *b) {
   std::vector<int> div(b->ncases);
-  e = cudaMemcpy(div.data(), b->diverged.p, b->ncases * sizeof(int), cudaMemcpyDeviceToHost);
+  cudaError_t e = cudaMemcpy(div.data(), b->diverged.p, b->ncases * sizeof(int), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return cuda_fail(e, "kj flags");
   for (int k = 0; k < b->ncases; ++k)
     if (div[k]) return fail(WINDS_BS_ERR_DIVERGED, "case %d: Diverging soln!!! (Cl is NaN)", k);
@@ -704,6 +791,31 @@ int winds_wake_step(winds_wake_batch *b, int nsteps, int use_graph) {
     if (rc) return rc;
   }
   cudaError_t e = cudaSuccess;
+  if (b->kj && use_graph && b->cond_ok) {
+    // the whole step, iteration included, as one graph: one round trip per step
+    if (!b->exec_step && build_step_graph(b) != WINDS_BS_OK) b->cond_ok = false;
+  }
+  if (b->kj && use_graph && b->exec_step) {
+    b->launches = b->step_launches;
+    cudaEventRecord(b->ev0, b->stream);
+    for (int k = 0; k < nsteps; ++k) {
+      e = cudaGraphLaunch(b->exec_step, b->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+      if (e != cudaSuccess) return cuda_fail(e, "wake step");
+      int rc = kj_step_errors(b);
+      if (!rc) rc = device_error_word(b);
+      if (rc) return rc;
+      ++b->steps_done;
+      int it = 0;
+      if ((e = cudaMemcpy(&it, b->kj_it.p, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess)
+        return cuda_fail(e, "iteration count");
+      b->kj_evals = it;
+    }
+    cudaEventRecord(b->ev1, b->stream);
+    b->timed_steps = nsteps;
+    e = cudaStreamSynchronize(b->stream);
+    return e == cudaSuccess ? WINDS_BS_OK : cuda_fail(e, "wake step sync");
+  }
   if (b->kj) {
     // pre-commit part, the iteration (host loop on a device convergence flag), commit
     for (int k = 0; k < nsteps; ++k) {
@@ -827,9 +939,9 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
   cudaSetDevice(b->dev);
   cudaStreamSynchronize(b->stream);
   // graphs captured for an earlier attachment describe other buffers
-  for (cudaGraphExec_t *x : {&b->exec_pre, &b->exec_kj, &b->exec_post})
+  for (cudaGraphExec_t *x : {&b->exec_pre, &b->exec_kj, &b->exec_post, &b->exec_step})
     if (*x) cudaGraphExecDestroy(*x), *x = nullptr;
-  for (cudaGraph_t *x : {&b->g_pre, &b->g_kj, &b->g_post})
+  for (cudaGraph_t *x : {&b->g_pre, &b->g_kj, &b->g_post, &b->g_step})
     if (*x) cudaGraphDestroy(*x), *x = nullptr;
   cudaStream_t s = b->stream;
   b->kjp = *prm;
@@ -898,6 +1010,7 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
     return rc;
   for (DevBuf *x : {&b->conv, &b->iters, &b->diverged, &b->res_max, &b->res_last, &b->active})
     if ((rc = x->ensure(std::max(b->ncases, 1) * 8 + 8, s))) return rc;
+  if ((rc = b->kj_it.ensure(16, s))) return rc;
   for (DevBuf *x : {&b->cl_o, &b->cd_o, &b->aoa_o, &b->guess, &b->bound_last})
     if ((rc = x->ensure(b->bound_n * sizeof(double), s))) return rc;
   // no change before the first step
@@ -1026,6 +1139,11 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
 
 int winds_wake_set_mlp(winds_wake_batch *b, winds_mlp *m) {
   if (!b || !b->kj) return fail(WINDS_BS_ERR_ARG, "attach lifting lines before the MLP");
+  // a captured step holds (or lacks) the network's launches
+  cudaSetDevice(b->dev);
+  cudaStreamSynchronize(b->stream);
+  if (b->exec_step) cudaGraphExecDestroy(b->exec_step), b->exec_step = nullptr;
+  if (b->g_step) cudaGraphDestroy(b->g_step), b->g_step = nullptr;
   if (!m) {
     b->mlp = nullptr;
     return WINDS_BS_OK;
@@ -1113,10 +1231,12 @@ void winds_wake_destroy(winds_wake_batch *b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
-  for (cudaGraphExec_t x : {b->exec_pre, b->exec_kj, b->exec_post})
+  for (cudaGraphExec_t x : {b->exec_pre, b->exec_kj, b->exec_post, b->exec_step})
     if (x) cudaGraphExecDestroy(x);
-  for (cudaGraph_t x : {b->g_pre, b->g_kj, b->g_post})
+  for (cudaGraph_t x : {b->g_pre, b->g_kj, b->g_post, b->g_step})
     if (x) cudaGraphDestroy(x);
+  if (b->body_stream) cudaStreamDestroy(b->body_stream);
+  b->kj_it.release();
   for (DevBuf *x : {&b->kjc_d, &b->ll, &b->bxn, &b->byn, &b->bzn, &b->vblade, &b->chord, &b->foil,
                     &b->foil_off, &b->aoa_t, &b->cl_t, &b->cd_t, &b->tp_ll, &b->perm_ll, &b->uindb,
                     &b->kj_groups, &b->kj_tiles, &b->kj_items, &b->kj_part, &b->conv, &b->iters,
