@@ -138,8 +138,9 @@ int winds_bs_sync(void *stream);
 
 /* Autotuner control. The first FP32 evaluation of a (core model, log2 targets,
  * log2 filaments) bucket on the library's own stream times the candidate
- * tilings (targets per thread T in {2,4,8}, filaments per tile KF in {32,64,128},
- * work-queue depth) and caches the fastest; set_tuning / get_tuning read and
+ * tilings (targets per thread T in {2,3,4}, filaments per tile KF in {32,64,128},
+ * work-queue depth: items per resident warp) and caches the fastest (T = 8 is
+ * settable); set_tuning / get_tuning read and
  * write that cache directly (e.g. to restore a saved choice). */
 int winds_bs_set_autotune(int on);
 int winds_bs_set_tuning(int core_model, long long n_targets, long long n_filaments, int T, int KF,

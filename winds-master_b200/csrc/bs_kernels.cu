@@ -132,25 +132,40 @@ __device__ __forceinline__ bool co_can_trigger(const BBox *bb, double co) {
 }
 
 // ------------------------------------------------------- FP32 direct sum
-constexpr int kThreads = 128;
-constexpr int kStagesMax = 4;
+// Every warp is an independent worker: it takes work items (a tile of 32 x T
+// targets against a filament range) from the persistent queue by itself and
+// streams the range through its own ring of shared-memory stages, so warps
+// never wait for one another (no CTA barrier in the kernel). A CTA holds kWarps
+// workers that share nothing but the SM.
+constexpr int kWarps = 4;
+constexpr int kThreads = 32 * kWarps;
 constexpr uint64_t kDefaultWaitNs = 2000000000ull;  // 2 s per tile: far above any real latency
 
 template <int KF>
 struct StageSmem {
   static constexpr int kBytes = KF * 64;  // KF/2 pair records of 128 B
-  static constexpr int kStages = KF >= 128 ? 3 : kStagesMax;  // filament stages in flight
+  // stages in flight: a warp's tile takes ~10-50 us, a bulk copy ~2 us, so
+  // one stage ahead suffices; three for the short 32-filament tiles
+  static constexpr int kStages = KF >= 64 ? 2 : 3;
+  // tiles per Kahan fold: the FP32 partial sums span 128 filaments
+  static constexpr int kFold = KF >= 128 ? 1 : 128 / KF;
 };
 
-// Dynamic shared memory: the filament stages, the per-target Kahan state
-// (sum, compensation) x 3 components as floats, the near-singular bit words
-// of the current tile (KF/4 words per thread), then the barriers: full[s]
-// (bytes landed) and empty[s] (every warp done reading stage s).
+// Shared memory of one worker: its filament stages, the Kahan state of its
+// targets (sum, compensation) x 3 components as floats, the near-singular bit
+// words of the current tile (KF/4 words per lane), its full[s] barriers
+// (bytes landed) and its target ball (centre, radius, threshold).
+template <int T, int KF>
+__host__ __device__ constexpr size_t warp_smem_bytes() {
+  constexpr int S = StageSmem<KF>::kStages;
+  return ((size_t)S * StageSmem<KF>::kBytes + (size_t)6 * 32 * T * sizeof(float) +
+          (size_t)(KF / 4) * 32 * sizeof(unsigned) + S * sizeof(uint64_t) + 8 * sizeof(float) +
+          127) / 128 * 128;
+}
+
 template <int T, int KF>
 __host__ __device__ constexpr size_t f32c_smem_bytes_t() {
-  constexpr int S = StageSmem<KF>::kStages;
-  return (size_t)S * StageSmem<KF>::kBytes + (size_t)6 * kThreads * T * sizeof(float) +
-         (size_t)(KF / 4) * kThreads * sizeof(unsigned) + 2 * S * sizeof(uint64_t);
+  return kWarps * warp_smem_bytes<T, KF>();
 }
 
 // Kahan step: (sum, comp) += v.
@@ -161,6 +176,7 @@ __device__ __forceinline__ void kahan_add(float &sum, float &comp, float v) {
   sum = s;
 }
 
+// Hands filaments f0 .. f0+KF to the copy engine into `stage`, completing on `bar`.
 template <int KF>
 __device__ __forceinline__ void issue_stage(const F32cArgs &a, unsigned char *stage, uint64_t *bar,
                                             int f0) {
@@ -168,28 +184,10 @@ __device__ __forceinline__ void issue_stage(const F32cArgs &a, unsigned char *st
   bulk_g2s(stage, a.pk + (size_t)(f0 / 2) * 8, KF * 64, bar);
 }
 
-// Thread 0 hands global tile g (filaments f0 .. f0+KF) to the copy engine
-// once every warp has released the stage's previous use (tile g - S, S stages).
-template <int KF>
-__device__ __forceinline__ bool produce(const F32cArgs &a, unsigned char *smem, uint64_t *full,
-                                        uint64_t *empty, unsigned g, int f0) {
-  constexpr unsigned S = StageSmem<KF>::kStages;
-  const int st = g % S;
-  if (g >= S && !mbar_wait_bounded(&empty[st], ((g - S) / S) & 1u, a.err, a.wait_limit_ns))
-    return false;
-  issue_stage<KF>(a, smem + st * StageSmem<KF>::kBytes, &full[st], f0);
-  return true;
-}
-
-// Non-blocking variant: issues tile g only if its stage is already free.
-template <int KF>
-__device__ __forceinline__ bool try_produce(const F32cArgs &a, unsigned char *smem, uint64_t *full,
-                                            uint64_t *empty, unsigned g, int f0) {
-  constexpr unsigned S = StageSmem<KF>::kStages;
-  const int st = g % S;
-  if (g >= S && !mbar_try_wait(&empty[st], ((g - S) / S) & 1u)) return false;
-  issue_stage<KF>(a, smem + st * StageSmem<KF>::kBytes, &full[st], f0);
-  return true;
+// Orders this thread's earlier shared-memory accesses (generic proxy) before
+// later bulk copies into the same bytes (async proxy).
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
 // ----------------------------------------------------- packed FP32 arithmetic
@@ -297,16 +295,20 @@ __device__ __forceinline__ void interact2(float2 npx, float2 npy, float2 npz, co
   az = __ffma2_rn(ub, cz, az);
 }
 
-// One item: the thread's T targets against filaments [it.f_begin, it.f_end).
-// Returns false when a bounded wait ran out (the item is abandoned).
+// One item: the lane's T targets against filaments [it.f_begin, it.f_end),
+// streamed through the warp's S stages (tile g of the warp in stage g % S).
+// Returns false, for the whole warp, when a bounded wait ran out (the item is
+// abandoned after the copies in flight have landed).
 template <int T, int KF, int MODEL, bool CO>
-__device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, const Tile &tl,
-                                          unsigned char *smem, uint64_t *full,
-                                          uint64_t *empty, float *s_k, unsigned *s_nb,
+__device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, unsigned char *stages,
+                                          uint64_t *full, float *s_k, unsigned *s_nb,
                                           unsigned &gt, float2 (&npx)[T], float2 (&npy)[T],
                                           float2 (&npz)[T], float2 ncx, float2 ncy, float2 ncz,
-                                          float S2, const float *ws, unsigned &near_cnt) {
-  const int tid = threadIdx.x;
+                                          float S2, const float *ws, unsigned &near_cnt,
+                                          const Tile &tl) {
+  constexpr int S = StageSmem<KF>::kStages;
+  constexpr int kB = StageSmem<KF>::kBytes;
+  const int lane = threadIdx.x & 31;
   const int ntiles = (it.f_end - it.f_begin) / KF;
   const float co2 = (float)(a.co * a.co);
   RefParams rp;
@@ -314,40 +316,25 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, con
   rp.d = a.d;
   rp.n = a.n;
   rp.co = a.co;
-  const int lane = tid & 31;
-  bool ok = true;
-  int issued = 0;  // tiles of this item handed to the copy engine (thread 0)
-  if (tid == 0) {
-    for (; issued < StageSmem<KF>::kStages && issued < ntiles; ++issued)
-      if (!produce<KF>(a, smem, full, empty, gt + issued, it.f_begin + issued * KF)) {
-        ok = false;
-        break;
-      }
-  }
+  // Between items every stage of the warp is free: each copy issued was
+  // waited for and read before the previous item ended.
+  int issued = ntiles < S ? ntiles : S;
+  if (lane == 0)
+    for (int j = 0; j < issued; ++j)
+      issue_stage<KF>(a, stages + ((gt + j) % S) * kB, &full[(gt + j) % S], it.f_begin + j * KF);
   float2 ax[T], ay[T], az[T];
 #pragma unroll
   for (int t = 0; t < T; ++t) ax[t] = ay[t] = az[t] = make_float2(0.f, 0.f);
 
   int i = 0;
-  for (; ok && i < ntiles; ++i) {
+  for (; i < ntiles; ++i) {
     const unsigned g = gt + i;
-    const int st = g % StageSmem<KF>::kStages;
-    const unsigned par = (g / StageSmem<KF>::kStages) & 1u;
-    // Tile i must have been handed out before anyone waits for it.
-    if (tid == 0 && issued <= i) {
-      if (produce<KF>(a, smem, full, empty, gt + issued, it.f_begin + issued * KF))
-        ++issued;
-      else
-        ok = false;
-    }
-    const bool timed_out = !ok || !mbar_wait_bounded(&full[st], par, a.err, a.wait_limit_ns);
-    const unsigned char *stage = smem + st * StageSmem<KF>::kBytes;
+    const int st = g % S;
+    const bool landed = mbar_wait_bounded(&full[st], (g / S) & 1u, a.err, a.wait_limit_ns);
+    if (!__all_sync(0xffffffffu, landed)) break;
+    const unsigned char *stage = stages + st * kB;
     const float4 *sP = reinterpret_cast<const float4 *>(stage);  // KF/2 pair records
     const float *sF = reinterpret_cast<const float *>(stage);
-    if (timed_out) {
-      ok = false;
-      break;
-    }
     // Hot loop: filaments in groups of 4 (two pair records). A warp-level
     // screen (one filament per lane, every 32 filaments) sends groups that are
     // far from all of the warp's targets down the plain path; the others test
@@ -408,27 +395,27 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, con
                                          az[t], nbits, 1u << (8 * (2 * j) + t),
                                          1u << (8 * (2 * j + 1) + t));
           }
-          s_nb[(kk / 4) * kThreads + tid] = nbits;
+          s_nb[(kk / 4) * 32 + lane] = nbits;
         }
       }
     }
-    // This warp is done with the stage: release it to the producer.
+    // Every lane has consumed its reads of the stage: refill it with tile i + S.
     __syncwarp();
-    if (lane == 0) mbar_arrive(&empty[st]);
-    // Thread 0 refills every stage whose readers are all done, without waiting.
-    if (tid == 0) {
-      while (issued < ntiles && issued <= i + (int)StageSmem<KF>::kStages &&
-             try_produce<KF>(a, smem, full, empty, gt + issued, it.f_begin + issued * KF))
-        ++issued;
+    if (lane == 0 && issued < ntiles) {
+      fence_proxy_async_smem();
+      issue_stage<KF>(a, stages + st * kB, &full[st], it.f_begin + issued * KF);
+      ++issued;
     }
-    // Kahan-fold this tile's partial sums into the per-target totals.
+    // Kahan-fold the partial sums into the per-target totals every 128 filaments.
+    if ((i + 1) % StageSmem<KF>::kFold == 0 || i + 1 == ntiles) {
 #pragma unroll
-    for (int t = 0; t < T; ++t) {
-      const int sl = tid * T + t;
-      kahan_add(s_k[0 * kThreads * T + sl], s_k[1 * kThreads * T + sl], ax[t].x + ax[t].y);
-      kahan_add(s_k[2 * kThreads * T + sl], s_k[3 * kThreads * T + sl], ay[t].x + ay[t].y);
-      kahan_add(s_k[4 * kThreads * T + sl], s_k[5 * kThreads * T + sl], az[t].x + az[t].y);
-      ax[t] = ay[t] = az[t] = make_float2(0.f, 0.f);
+      for (int t = 0; t < T; ++t) {
+        const int sl = lane * T + t;
+        kahan_add(s_k[0 * 32 * T + sl], s_k[1 * 32 * T + sl], ax[t].x + ax[t].y);
+        kahan_add(s_k[2 * 32 * T + sl], s_k[3 * 32 * T + sl], ay[t].x + ay[t].y);
+        kahan_add(s_k[4 * 32 * T + sl], s_k[5 * 32 * T + sl], az[t].x + az[t].y);
+        ax[t] = ay[t] = az[t] = make_float2(0.f, 0.f);
+      }
     }
     // Near-singular pairs of this tile, each lane its own: the reference formula
     // in FP64, added to the Kahan state as an exact hi + lo pair.
@@ -437,40 +424,40 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, con
     while (cg) {
       const int w = __ffs(cg) - 1;
       cg &= cg - 1u;
-      unsigned bits = s_nb[w * kThreads + tid];
+      unsigned bits = s_nb[w * 32 + lane];
       while (bits) {
         const int b = __ffs(bits) - 1;
         bits &= bits - 1u;
         const int t = b & 7;
         const int fidx = it.f_begin + i * KF + 4 * w + (b >> 3);
-        int local = tid * T + t;
+        int local = lane * T + t;
         if (local >= tl.t_count) local = tl.t_count - 1;
         const double4 p = a.tp[tl.t_begin + local];
         double u[3] = {0.0, 0.0, 0.0};
         ref_pair<false>(a.ra[fidx], a.rb[fidx], p.x, p.y, p.z, rp, u[0], u[1], u[2]);
-        const int sl = tid * T + t;
+        const int sl = lane * T + t;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           const float hi = (float)u[c];
           const float lo = (float)(u[c] - (double)hi);
-          kahan_add(s_k[(2 * c) * kThreads * T + sl], s_k[(2 * c + 1) * kThreads * T + sl], hi);
-          kahan_add(s_k[(2 * c) * kThreads * T + sl], s_k[(2 * c + 1) * kThreads * T + sl], lo);
+          kahan_add(s_k[(2 * c) * 32 * T + sl], s_k[(2 * c + 1) * 32 * T + sl], hi);
+          kahan_add(s_k[(2 * c) * 32 * T + sl], s_k[(2 * c + 1) * 32 * T + sl], lo);
         }
         ++near_cnt;
       }
     }
+    __syncwarp();
   }
-  // A bounded wait that ran out anywhere abandons the item for the whole CTA.
-  if (__syncthreads_or(!ok)) {
-    // Let the copies already issued land (bounded) before the CTA leaves, so
-    // no bulk copy targets the shared memory of a finished CTA.
-    if (tid == 0) {
-      constexpr int S = StageSmem<KF>::kStages;
-      for (int j = (issued > S ? issued - S : 0); j < issued; ++j) {
+  if (i < ntiles) {
+    // A bounded wait ran out: let the copies already issued land (bounded)
+    // before the warp leaves, so no bulk copy targets the shared memory of a
+    // finished CTA.
+    if (lane == 0)
+      for (int j = i; j < issued; ++j) {
         const unsigned g = gt + j;
         mbar_wait_bounded(&full[g % S], (g / S) & 1u, a.err, a.wait_limit_ns);
       }
-    }
+    __syncwarp();
     return false;
   }
   gt += ntiles;
@@ -489,47 +476,43 @@ struct MinBlocks {
 template <int T, int KF, int MODEL>
 __global__ void __launch_bounds__(kThreads, MinBlocks<T>::value) bs_f32c(const F32cArgs a) {
   static_assert(KF % 32 == 0 && KF / 4 <= 32, "one screen word per 32 filaments, one bit per group");
+  constexpr int S = StageSmem<KF>::kStages;
   extern __shared__ __align__(128) unsigned char smem[];
-  float *s_k = reinterpret_cast<float *>(smem + StageSmem<KF>::kStages * StageSmem<KF>::kBytes);
-  unsigned *s_nb = reinterpret_cast<unsigned *>(s_k + 6 * kThreads * T);
-  uint64_t *full = reinterpret_cast<uint64_t *>(s_nb + (KF / 4) * kThreads);
-  uint64_t *empty = full + StageSmem<KF>::kStages;
-  __shared__ int s_item;
-  __shared__ float s_ws[kThreads / 32][8];
-  const int tid = threadIdx.x;
-  if (tid == 0) {
-    for (int s = 0; s < StageSmem<KF>::kStages; ++s) {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], kThreads / 32);
-    }
+  const int lane = threadIdx.x & 31;
+  unsigned char *stages = smem + (threadIdx.x >> 5) * warp_smem_bytes<T, KF>();
+  float *s_k = reinterpret_cast<float *>(stages + S * StageSmem<KF>::kBytes);
+  unsigned *s_nb = reinterpret_cast<unsigned *>(s_k + 6 * 32 * T);
+  uint64_t *full = reinterpret_cast<uint64_t *>(s_nb + (KF / 4) * 32);
+  float *ws = reinterpret_cast<float *>(full + S);
+  if (lane == 0) {
+    for (int st = 0; st < S; ++st) mbar_init(&full[st], 1);
     fence_mbar_init();
   }
-  __syncthreads();
+  __syncwarp();
   const bool co_on = co_can_trigger(a.bbox, a.co);
   unsigned gt = 0;
   unsigned near_cnt = 0;
   while (true) {
-    if (tid == 0) s_item = (int)atomicAdd(a.work_ctr, 1u);
-    __syncthreads();
-    const int item_id = s_item;
-    __syncthreads();
+    int item_id = 0;
+    if (lane == 0) item_id = (int)atomicAdd(a.work_ctr, 1u);
+    item_id = __shfl_sync(0xffffffffu, item_id, 0);
     if (item_id >= a.n_items) break;
     const Item it = a.items[item_id];
     const Tile tl = a.tiles[it.tile];
     if (tl.t_count <= 0 || ((it.f_end - it.f_begin) % KF) != 0) {
-      if (tid == 0) atomicOr(a.err, kErrBadItem);
+      if (lane == 0) atomicOr(a.err, kErrBadItem);
       continue;
     }
-    // This thread's T consecutive targets, relative to the FP32 image of the first.
+    // This lane's T consecutive targets, relative to the FP32 image of the first.
     float px[T], py[T], pz[T];
     float spread2 = 0.f;
-    int l0 = tid * T;
+    int l0 = lane * T;
     if (l0 >= tl.t_count) l0 = tl.t_count - 1;
     const double4 p0 = a.tp[tl.t_begin + l0];
     const float cx = (float)p0.x, cy = (float)p0.y, cz = (float)p0.z;
 #pragma unroll
     for (int t = 0; t < T; ++t) {
-      int l = tid * T + t;
+      int l = lane * T + t;
       if (l >= tl.t_count) l = tl.t_count - 1;
       const double4 p = a.tp[tl.t_begin + l];
       px[t] = (float)(p.x - (double)cx);
@@ -537,7 +520,7 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<T>::value) bs_f32c(const F
       pz[t] = (float)(p.z - (double)cz);
       spread2 = fmaxf(spread2, px[t] * px[t] + py[t] * py[t] + pz[t] * pz[t]);
 #pragma unroll
-      for (int c = 0; c < 6; ++c) s_k[c * kThreads * T + tid * T + t] = 0.f;
+      for (int c = 0; c < 6; ++c) s_k[c * 32 * T + lane * T + t] = 0.f;
     }
     const float S2 = 0.09f * spread2;  // pairs closer than 0.3 x spread go to FP64
     // -(P - c) in both lanes of a packed register, and -c likewise
@@ -570,8 +553,7 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<T>::value) bs_f32c(const F
       wr2 = fmaxf(wr2, __shfl_xor_sync(0xffffffffu, wr2, o));
       rn_floor = fmaxf(rn_floor, __shfl_xor_sync(0xffffffffu, rn_floor, o));
     }
-    float *ws = s_ws[tid >> 5];
-    if ((tid & 31) == 0) {
+    if (lane == 0) {
       ws[0] = wcx;
       ws[1] = wcy;
       ws[2] = wcz;
@@ -581,24 +563,24 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<T>::value) bs_f32c(const F
     __syncwarp();
     bool ok;
     if (co_on)
-      ok = f32c_item<T, KF, MODEL, true>(a, it, tl, smem, full, empty, s_k, s_nb, gt, npx, npy,
-                                         npz, ncx, ncy, ncz, S2, ws, near_cnt);
+      ok = f32c_item<T, KF, MODEL, true>(a, it, stages, full, s_k, s_nb, gt, npx, npy, npz, ncx,
+                                         ncy, ncz, S2, ws, near_cnt, tl);
     else
-      ok = f32c_item<T, KF, MODEL, false>(a, it, tl, smem, full, empty, s_k, s_nb, gt, npx, npy,
-                                          npz, ncx, ncy, ncz, S2, ws, near_cnt);
-    __syncwarp();
-    if (!ok) return;
+      ok = f32c_item<T, KF, MODEL, false>(a, it, stages, full, s_k, s_nb, gt, npx, npy, npz, ncx,
+                                          ncy, ncz, S2, ws, near_cnt, tl);
+    if (!ok) break;
     double *part = a.part + (size_t)item_id * 3 * a.tile_cap;
 #pragma unroll
     for (int t = 0; t < T; ++t) {
-      const int l = tid * T + t;
+      const int l = lane * T + t;
       if (l < tl.t_count) {
 #pragma unroll
         for (int c = 0; c < 3; ++c)
-          part[c * a.tile_cap + l] = (double)s_k[(2 * c) * kThreads * T + l] -
-                                     (double)s_k[(2 * c + 1) * kThreads * T + l];
+          part[c * a.tile_cap + l] = (double)s_k[(2 * c) * 32 * T + l] -
+                                     (double)s_k[(2 * c + 1) * 32 * T + l];
       }
     }
+    __syncwarp();
   }
   if (a.near_ctr && near_cnt) atomicAdd(a.near_ctr, (unsigned long long)near_cnt);
 }
@@ -664,6 +646,7 @@ __global__ void bs_reduce(const Tile *__restrict__ tiles, const Group *__restric
   const Group g = groups[tl.group];
   for (int l = threadIdx.x; l < tl.t_count; l += blockDim.x) {
     double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+#pragma unroll 4
     for (int k = 0; k < tl.n_items; ++k) {
       const double *p = part + (size_t)(tl.first_item + k) * 3 * tile_cap;
       s0 += p[l];
@@ -751,7 +734,8 @@ cudaError_t launch_f32c_t(const F32cArgs &a, int grid, cudaStream_t s) {
     if (e != cudaSuccess) return e;
     if (dev < 32) attr_set |= (1u << dev);
   }
-  bs_f32c<T, KF, MODEL><<<grid, kThreads, smem, s>>>(a);
+  // `grid` counts workers (warps); kWarps of them per CTA
+  bs_f32c<T, KF, MODEL><<<(grid + kWarps - 1) / kWarps, kThreads, smem, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -765,8 +749,8 @@ int occupancy_t() {
   int n = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bs_f32c<T, KF, MODEL>, kThreads, smem) !=
       cudaSuccess)
-    return 1;
-  return n > 0 ? n : 1;
+    return kWarps;
+  return (n > 0 ? n : 1) * kWarps;  // resident workers per SM
 }
 
 #define WINDS_F32C_CASE(FN, M, TT, KK, ...) \
@@ -794,7 +778,7 @@ bool f32c_config_supported(int T, int KF) {
   return (T == 2 || T == 3 || T == 4 || T == 8) && (KF == 32 || KF == 64 || KF == 128);
 }
 
-int f32c_threads() { return kThreads; }
+int f32c_threads() { return 32; }  // lanes of one worker: a tile holds 32 x T targets
 int f64_threads() { return kF64Threads; }
 int f64_tile() { return kF64Tile; }
 
@@ -880,7 +864,8 @@ cudaError_t sort_target_keys(void *temp, size_t *temp_bytes, const unsigned long
 cudaError_t launch_reduce(const Tile *tiles, int n_tiles, const Group *groups, const double *part,
                           const int *perm, int tile_cap, cudaStream_t s) {
   if (n_tiles <= 0) return cudaSuccess;
-  bs_reduce<<<n_tiles, 256, 0, s>>>(tiles, groups, part, perm, tile_cap);
+  const int bs = tile_cap >= 256 ? 256 : (tile_cap + 31) / 32 * 32;  // one thread per target
+  bs_reduce<<<n_tiles, bs, 0, s>>>(tiles, groups, part, perm, tile_cap);
   return cudaGetLastError();
 }
 

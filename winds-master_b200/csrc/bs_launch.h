@@ -17,6 +17,9 @@ struct PackedFilaments {
 constexpr int kFilamentPad = 128;
 
 bool f32c_config_supported(int T, int KF);
+// FP32c work runs on independent warp workers: a tile holds f32c_threads() * T
+// targets, f32c_occupancy() counts resident workers per SM, and launch_f32c's
+// grid counts workers.
 int f32c_threads();
 int f64_threads();
 int f64_tile();

@@ -182,7 +182,7 @@ void shutdown_all() {
 static long long round_up(long long x, long long m) { return (x + m - 1) / m * m; }
 
 // Splits each group into tiles of tile_cap targets and each tile's filament
-// range into chunks, aiming at `waves` rounds of the resident CTAs so the
+// range into chunks, aiming at `waves` rounds of the resident workers so the
 // persistent kernel's work queue stays balanced.
 void build_plan(Plan &pl, const std::vector<GroupSpec> &gs, int tile_cap, int resident,
                 double waves, int chunk_quantum) {
@@ -366,7 +366,7 @@ TuneChoice default_choice(long long nt) {
   TuneChoice ch;
   ch.T = nt >= 2048 ? 4 : 2;
   ch.KF = 64;
-  ch.waves = 8.0;
+  ch.waves = 32.0;
   return ch;
 }
 
@@ -400,10 +400,32 @@ int run_direct_sum(Context *c, const std::vector<GroupSpec> &gs, int model, doub
     quantum = kFilamentPad;
   }
   // sequential: one chunk per tile, so every target sums its filaments in order
-  build_plan(pl, gs, tile_cap, resident, sequential ? 0.0 : ch.waves,
-             sequential ? (1 << 30) : quantum);
+  const double waves = sequential ? 0.0 : ch.waves;
+  if (sequential) quantum = 1 << 30;
+  bool same = c->plan_tile_cap == tile_cap && c->plan_resident == resident &&
+              c->plan_quantum == quantum && c->plan_waves == waves &&
+              c->plan_gs.size() == gs.size();
+  for (size_t k = 0; same && k < gs.size(); ++k) {
+    const GroupSpec &x = gs[k], &y = c->plan_gs[k];
+    same = x.out == y.out && x.t_begin == y.t_begin && x.t_count == y.t_count &&
+           x.ns_p == y.ns_p && x.f_begin == y.f_begin && x.f_end == y.f_end &&
+           x.accumulate == y.accumulate;
+  }
   int rc;
-  if ((rc = upload_plan(c, pl, s))) return rc;
+  if (same) {
+    // the tables on the device are this plan's; order after their upload
+    cudaError_t e = cudaStreamWaitEvent(s, c->ev_upload, 0);
+    if (e != cudaSuccess) return cuda_fail(e, "plan reuse");
+  } else {
+    c->plan_tile_cap = -1;
+    build_plan(pl, gs, tile_cap, resident, waves, quantum);
+    if ((rc = upload_plan(c, pl, s))) return rc;
+    c->plan_gs = gs;
+    c->plan_tile_cap = tile_cap;
+    c->plan_resident = resident;
+    c->plan_quantum = quantum;
+    c->plan_waves = waves;
+  }
   const size_t part_bytes = pl.items.size() * 3 * (size_t)tile_cap * sizeof(double);
   if ((rc = c->part.ensure(part_bytes + 16, s))) return rc;
   F32cArgs a;
@@ -533,7 +555,7 @@ int autotune(Context *c, const std::vector<GroupSpec> &gs, int model, double dcu
   // T = 8 (supported, settable) is left out: its unrolled paths run slower
   const int Ts[3] = {2, 3, 4};
   const int KFs[3] = {32, 64, 128};
-  const double Ws[3] = {8.0, 16.0, 32.0};
+  const double Ws[3] = {16.0, 32.0, 64.0};
   float best_ms = 1e30f;
   TuneChoice bc = default_choice(nt);
   cudaEvent_t e0, e1;

@@ -68,6 +68,11 @@ struct Context {
   DevBuf in_P, in_F, out_u;
   HostBuf htab, hstat;
   Plan plan;
+  // what the uploaded plan was built from: a call with the same groups and
+  // tiling reuses it (no host rebuild, no upload)
+  std::vector<GroupSpec> plan_gs;
+  int plan_tile_cap = -1, plan_resident = -1, plan_quantum = -1;
+  double plan_waves = -1.0;
   int launches = 0;
   bool timed = false;
   bool autotune = true;

@@ -716,8 +716,8 @@ int winds_wake_create(const winds_wake_case *cases, int ncases, const winds_wake
 static int device_error_word(winds_wake_batch *b);
 
 // First-step tiling choice for an FP32c batch the cache has no entry for:
-// times the main evaluation of this batch for T in {3, 4}, KF in {64, 128}
-// and 16 or 32 items per resident CTA, keeps the fastest (cached for the
+// times the main evaluation of this batch for T in {3, 4}, KF in {32, 64}
+// and 32 or 64 items per resident worker, keeps the fastest (cached for the
 // batch's size bucket) and rebuilds the plan. The evaluations only write
 // per-step scratch (velocities, cores, lengths) that the first step rewrites.
 static int autotune_batch(winds_wake_batch *b) {
@@ -737,8 +737,8 @@ static int autotune_batch(winds_wake_batch *b) {
   TuneChoice best = b->ch;
   float best_ms = 1e30f;
   for (int T : {3, 4})
-    for (int KF : {64, 128})
-      for (double w : {16.0, 32.0}) {
+    for (int KF : {32, 64})
+      for (double w : {32.0, 64.0}) {
         b->ch.T = T, b->ch.KF = KF, b->ch.waves = w;
         if ((rc = build_plans(b))) break;
         float ms = 0.f;
