@@ -304,7 +304,8 @@ def e2e_run_bench(steps, ncases=16, ages=1440, seed=5):
             "thrust_history_N": f["T"].sum(1).round(1).tolist(),
             "power_history_W": f["P"].sum(1).round(1).tolist(),
             "mlp_training_s": round(train_s, 2), "timing": "CUDA events around each step "
-            "(host waits on the per-iteration convergence flag included)"}
+            "(fast path: the lifting-line loop runs inside the step's graph; plain path: the "
+            "host waits on a per-iteration convergence flag)"}
 
 
 # ------------------------------------------------------------------ our arm
