@@ -295,6 +295,13 @@ __device__ __forceinline__ void interact2(float2 npx, float2 npy, float2 npz, co
   az = __ffma2_rn(ub, cz, az);
 }
 
+// A near-singular pair of a tile, listed in the tile's consumed stage: the
+// FP64 reference term `u` of filament `fidx` at the owner's target `slot`.
+struct NearEntry {
+  double u[3];
+  int fidx, slot;
+};
+
 // One item: the lane's T targets against filaments [it.f_begin, it.f_end),
 // streamed through the warp's S stages (tile g of the warp in stage g % S).
 // Returns false, for the whole warp, when a bounded wait ran out (the item is
@@ -399,13 +406,7 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, uns
         }
       }
     }
-    // Every lane has consumed its reads of the stage: refill it with tile i + S.
     __syncwarp();
-    if (lane == 0 && issued < ntiles) {
-      fence_proxy_async_smem();
-      issue_stage<KF>(a, stages + st * kB, &full[st], it.f_begin + issued * KF);
-      ++issued;
-    }
     // Kahan-fold the partial sums into the per-target totals every 128 filaments.
     if ((i + 1) % StageSmem<KF>::kFold == 0 || i + 1 == ntiles) {
 #pragma unroll
@@ -417,34 +418,75 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, uns
         ax[t] = ay[t] = az[t] = make_float2(0.f, 0.f);
       }
     }
-    // Near-singular pairs of this tile, each lane its own: the reference formula
-    // in FP64, added to the Kahan state as an exact hi + lo pair.
-    unsigned cg = careful;
-#pragma unroll 1
-    while (cg) {
-      const int w = __ffs(cg) - 1;
-      cg &= cg - 1u;
-      unsigned bits = s_nb[w * 32 + lane];
-      while (bits) {
-        const int b = __ffs(bits) - 1;
-        bits &= bits - 1u;
-        const int t = b & 7;
-        const int fidx = it.f_begin + i * KF + 4 * w + (b >> 3);
-        int local = lane * T + t;
-        if (local >= tl.t_count) local = tl.t_count - 1;
-        const double4 p = a.tp[tl.t_begin + local];
-        double u[3] = {0.0, 0.0, 0.0};
-        ref_pair<false>(a.ra[fidx], a.rb[fidx], p.x, p.y, p.z, rp, u[0], u[1], u[2]);
-        const int sl = lane * T + t;
+    // Near-singular pairs of this tile: the reference formula in FP64, added to
+    // the owner's Kahan state as an exact hi + lo pair. The pairs are listed in
+    // the consumed stage (lane-major, in each lane's bit order), computed by all
+    // lanes together, then added by their owners in list order, so every target
+    // receives its terms in the same order as a lane-by-lane pass would.
+    if (careful) {  // warp-uniform
+      constexpr int kCap = kB / (int)sizeof(NearEntry);
+      NearEntry *ne = reinterpret_cast<NearEntry *>(stages + st * kB);
+      int cnt = 0;
+      for (unsigned cg = careful; cg; cg &= cg - 1u) cnt += __popc(s_nb[(__ffs(cg) - 1) * 32 + lane]);
+      int incl = cnt;
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const float hi = (float)u[c];
-          const float lo = (float)(u[c] - (double)hi);
-          kahan_add(s_k[(2 * c) * 32 * T + sl], s_k[(2 * c + 1) * 32 * T + sl], hi);
-          kahan_add(s_k[(2 * c) * 32 * T + sl], s_k[(2 * c + 1) * 32 * T + sl], lo);
-        }
-        ++near_cnt;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
       }
+      const int total = __shfl_sync(0xffffffffu, incl, 31);
+      const int first = incl - cnt;
+#pragma unroll 1
+      for (int base = 0; base < total; base += kCap) {
+        const int end = total < base + kCap ? total : base + kCap;
+        if (first < end && first + cnt > base) {
+          int k = first;
+          for (unsigned cg = careful; cg && k < end; cg &= cg - 1u) {
+            const int w = __ffs(cg) - 1;
+            for (unsigned bits = s_nb[w * 32 + lane]; bits && k < end; bits &= bits - 1u, ++k) {
+              if (k < base) continue;
+              const int b = __ffs(bits) - 1;
+              ne[k - base].fidx = it.f_begin + i * KF + 4 * w + (b >> 3);
+              ne[k - base].slot = lane * T + (b & 7);
+            }
+          }
+        }
+        __syncwarp();
+        for (int k = base + lane; k < end; k += 32) {
+          NearEntry &e = ne[k - base];
+          int local = e.slot;
+          if (local >= tl.t_count) local = tl.t_count - 1;
+          const double4 p = a.tp[tl.t_begin + local];
+          double u0 = 0.0, u1 = 0.0, u2 = 0.0;
+          ref_pair<false>(a.ra[e.fidx], a.rb[e.fidx], p.x, p.y, p.z, rp, u0, u1, u2);
+          e.u[0] = u0;
+          e.u[1] = u1;
+          e.u[2] = u2;
+        }
+        __syncwarp();
+        const int k0 = first > base ? first : base;
+        const int k1 = first + cnt < end ? first + cnt : end;
+        for (int k = k0; k < k1; ++k) {
+          const NearEntry &e = ne[k - base];
+          const int sl = e.slot;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const float hi = (float)e.u[c];
+            const float lo = (float)(e.u[c] - (double)hi);
+            kahan_add(s_k[(2 * c) * 32 * T + sl], s_k[(2 * c + 1) * 32 * T + sl], hi);
+            kahan_add(s_k[(2 * c) * 32 * T + sl], s_k[(2 * c + 1) * 32 * T + sl], lo);
+          }
+          ++near_cnt;
+        }
+        __syncwarp();
+      }
+    }
+    // Every lane is done with the stage (tile and near list): refill it with
+    // tile i + S.
+    if (lane == 0 && issued < ntiles) {
+      fence_proxy_async_smem();
+      issue_stage<KF>(a, stages + st * kB, &full[st], it.f_begin + issued * KF);
+      ++issued;
     }
     __syncwarp();
   }
