@@ -166,6 +166,46 @@ def cpu_rate(fams, P, n_targets, seed=0):
     return n_targets * nf / dt / 1e9, dt
 
 
+def other_cpu_baselines(fams, P, seed=3):
+    """The two other host paths, each on a small seeded target sample x all
+    filaments: the NumPy restatement of core/BiotSavart.m (vectorised over
+    filaments per target block, one process) and, when it was built, the
+    reference MEX's own serial host loop (cuda/source/BiotSavartMex.cu:268-282;
+    cut-off core only, so it runs the cut-off form d = 1e-4 on the same
+    geometry). Gint/s each; a reported baseline, not a target."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import biot_savart_ref as bsr
+    import oracle as orc
+    rng = np.random.default_rng(seed)
+    nf = sum(f[0].shape[0] * f[0].shape[2] * f[0].shape[3] for f in fams)
+    out = {}
+    idx = rng.choice(P.shape[0], 48, replace=False)
+    pts = np.ascontiguousarray(P[idx, :, 0, 0])
+    flat = []
+    for F1, F2, g, rc in fams:
+        m = lambda a: np.moveaxis(a, 1, -1).reshape(-1, a.shape[1], order="F")
+        flat.append((m(F1), m(F2), g.ravel(order="F"), rc.ravel(order="F")))
+    t0 = time.perf_counter()
+    for x1, x2, g, rc in flat:
+        bsr.biot_savart_flat(x1, x2, g, rc, pts, "visc2", 1000.0)
+    dt = time.perf_counter() - t0
+    out["numpy_port"] = {"value": len(idx) * nf / dt / 1e9, "unit": UNIT, "cores": 1,
+                         "sample": f"{len(idx)} sampled targets x {nf} filaments ({dt:.1f} s), NumPy "
+                                   "restatement of core/BiotSavart.m, Vatistas n=2"}
+    if orc.ref_available():
+        idx = rng.choice(P.shape[0], 256, replace=False)
+        Ps = np.asfortranarray(P[idx])
+        t0 = time.perf_counter()
+        for F1, F2, g, rc in fams:
+            orc.ref_host_eval(F1, F2, Ps, g, rc, 1e-4, 1000.0)
+        dt = time.perf_counter() - t0
+        out["reference_mex_host"] = {
+            "value": len(idx) * nf / dt / 1e9, "unit": UNIT, "cores": 1,
+            "sample": f"{len(idx)} sampled targets x {nf} filaments ({dt:.1f} s), the reference "
+                      "MEX host loop compiled from its source, cut-off core d=1e-4"}
+    return out
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -437,7 +477,8 @@ def ours(args):
         rate, dt = cpu_rate(fams, P, n, seed=1)
         cpu = {"value": rate, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                "sample": f"{n} sampled targets x {nf} filaments ({dt:.1f} s), FP64 C restatement "
-                         "of core/BiotSavart.m, OpenMP"}
+                         "of core/BiotSavart.m, OpenMP",
+               "others": other_cpu_baselines(fams, P)}
     wake_line = None
     if rank == 0 and args.wake_steps > 0 and not args.quick:
         wake_line = wake_bench(args)
