@@ -56,6 +56,9 @@ def parse():
                     help="skip the start-value study and the end-to-end run")
     ap.add_argument("--e2e-steps", type=int, default=3,
                     help="pcc steps of the 16-case end-to-end run (each path)")
+    ap.add_argument("--wake-only", action="store_true",
+                    help="profiling aid: only the 64-case batched wake (fast path, default "
+                         "tiling, no FP64 comparison); prints its sub-object")
     return ap.parse_args()
 
 
@@ -240,7 +243,7 @@ def reference_arm(args):
 
 
 # ------------------------------------------------------------------ batched wake
-def wake_bench(args, seed=2, ncases=64):
+def wake_bench(args, seed=2, ncases=64, plain=True):
     """64 uneven rotor cases (wake steps 60-720, span nodes 17-41, U 5-25 m/s,
     TSR 4-10, yaw 0-30 deg, shear 0-0.3), pcc predictor-corrector step: the
     FP32-compensated batched engine replaying one CUDA graph per step, against
@@ -257,12 +260,16 @@ def wake_bench(args, seed=2, ncases=64):
     ms, inter, launches = b.stats()
     b.close()
     plain_ms = 0.0
-    for c in cases:
+    for c in (cases if plain else []):
         p = wake.WakeBatch([c], integrator="pcc", precision="f64")
         p.step(1)
         p.step(1)
         plain_ms += p.stats()[0]
         p.close()
+    if not plain:
+        return {"cases": ncases, "integrator": "pcc", "graph": True, "steps_per_s": 1000.0 / ms,
+                "ms_per_step": ms, "launches_per_step": launches,
+                "nodes": int(sum(c["nst"] * c["na"] * c["nb"] for c in cases))}
     return {"cases": ncases, "integrator": "pcc", "graph": True,
             "steps_per_s": 1000.0 / ms, "ms_per_step": ms,
             "interactions_per_step": inter, "gint_per_s": inter / (ms * 1e-3) / 1e9,
@@ -528,5 +535,9 @@ if __name__ == "__main__":
     a = parse()
     if a.impl == "reference":
         reference_arm(a)
+    elif a.wake_only:
+        wbm = importlib.import_module("winds-master_b200")
+        wbm.set_autotune(False)
+        print(json.dumps({"wake_batch": wake_bench(a, plain=False)}), flush=True)
     else:
         ours(a)

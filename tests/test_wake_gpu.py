@@ -101,5 +101,5 @@ def test_first_step_autotunes_the_batch_tiling(wb, synth):
     b = wake.WakeBatch(cases, integrator="fe", precision="f32c")
     b.step(1)
     T, KF, waves = wb.get_tuning(wb.bs.CORE_VATISTAS, nodes, fil)
-    assert T in (3, 4) and KF in (64, 128) and waves in (16.0, 32.0)
+    assert T in (3, 4) and KF in (32, 64) and waves in (32.0, 64.0)
     b.close()

@@ -158,8 +158,12 @@ __device__ __forceinline__ void bbox_accumulate(const float lo[3], const float h
       a = fminf(a, smin[c][w]);
       b = fmaxf(b, smax[c][w]);
     }
-    atomicMin(&gmin[c], float_key(a));
-    atomicMax(&gmax[c], float_key(b));
+    // the box grows only at first: most blocks lie inside it already, so a
+    // plain read spares the contended atomic (the bound only ever tightens
+    // towards the block's value, so skipping a non-improving one is exact)
+    const int ka = float_key(a), kb = float_key(b);
+    if (a != FLT_MAX && ka < *(volatile const int *)&gmin[c]) atomicMin(&gmin[c], ka);
+    if (b != -FLT_MAX && kb > *(volatile const int *)&gmax[c]) atomicMax(&gmax[c], kb);
   }
 }
 
@@ -179,12 +183,13 @@ __device__ __forceinline__ float &pk_field(float4 *pk, long long f, int q) {
 // Vatistas n=2 in FP32: with c = K L x r1, the core factor
 // |L x r1|^2 / sqrt(|L x r1|^4 + (rc^2 |L|^2)^2) equals |c|^2 / sqrt(|c|^4 + D)
 // for D = (K^2 rc^2 |L|^2)^2, so the kernel never multiplies by K.
-__device__ __forceinline__ void pack_filament(long long f, double x1, double y1, double z1,
-                                              double x2, double y2, double z2, double g, double r,
-                                              int model, double dcut, float4 *pk, double4 *ra,
-                                              double4 *rb) {
-  ra[f] = make_double4(x1, y1, z1, g);
-  rb[f] = make_double4(x2, y2, z2, r);
+//
+// filament_fields computes the 16 FP32 fields; pack_filament writes them one
+// float at a time, store_pair_fields lets the two lanes of a pair write the
+// 128-byte record with four 16-byte stores each.
+__device__ __forceinline__ void filament_fields(double x1, double y1, double z1, double x2,
+                                                double y2, double z2, double g, double r,
+                                                int model, double dcut, float v[16]) {
   const double Lx = x2 - x1, Ly = y2 - y1, Lz = z2 - z1;
   const double L2 = Lx * Lx + Ly * Ly + Lz * Lz;
   double K = g / k4Pi;
@@ -206,24 +211,67 @@ __device__ __forceinline__ void pack_filament(long long f, double x1, double y1,
   if (isfinite(r) && 9.0 * r > Rn2) Rn2 = 9.0 * r;
   if (!(Rn2 > 1e-20)) Rn2 = 1e-20;
   const float hx = (float)x1, hy = (float)y1, hz = (float)z1;
-  const float v[16] = {hx, hy, hz, (float)L2,
-                       (float)(x1 - (double)hx), (float)(y1 - (double)hy),
-                       (float)(z1 - (double)hz), (float)Rn2,
-                       (float)Lx, (float)Ly, (float)Lz, (float)D,
-                       (float)(K * Lx), (float)(K * Ly), (float)(K * Lz), 0.f};
+  v[0] = hx, v[1] = hy, v[2] = hz, v[3] = (float)L2;
+  v[4] = (float)(x1 - (double)hx), v[5] = (float)(y1 - (double)hy);
+  v[6] = (float)(z1 - (double)hz), v[7] = (float)Rn2;
+  v[8] = (float)Lx, v[9] = (float)Ly, v[10] = (float)Lz, v[11] = (float)D;
+  v[12] = (float)(K * Lx), v[13] = (float)(K * Ly), v[14] = (float)(K * Lz), v[15] = 0.f;
+}
+
+// Fields of an inert filament (far away, zero length, zero circulation) for padding.
+__device__ __forceinline__ void inert_fields(float v[16]) {
+  const float far = 1e18f;
+#pragma unroll
+  for (int q = 0; q < 16; ++q) v[q] = 0.f;
+  v[0] = v[1] = v[2] = far;
+  v[11] = 1.f;
+}
+constexpr double kInertFar = 1e18;
+
+__device__ __forceinline__ void pack_filament(long long f, double x1, double y1, double z1,
+                                              double x2, double y2, double z2, double g, double r,
+                                              int model, double dcut, float4 *pk, double4 *ra,
+                                              double4 *rb) {
+  ra[f] = make_double4(x1, y1, z1, g);
+  rb[f] = make_double4(x2, y2, z2, r);
+  float v[16];
+  filament_fields(x1, y1, z1, x2, y2, z2, g, r, model, dcut, v);
 #pragma unroll
   for (int q = 0; q < 16; ++q) pk_field(pk, f, q) = v[q];
 }
 
-// Inert filament (far away, zero length, zero circulation) for padding.
 __device__ __forceinline__ void pack_inert(long long f, float4 *pk, double4 *ra, double4 *rb) {
-  const double far = 1e18;
-  const float v[16] = {(float)far, (float)far, (float)far, 0.f, 0.f, 0.f, 0.f, 0.f,
-                       0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 0.f};
+  float v[16];
+  inert_fields(v);
 #pragma unroll
   for (int q = 0; q < 16; ++q) pk_field(pk, f, q) = v[q];
-  ra[f] = make_double4(far, far, far, 0.0);
-  rb[f] = make_double4(far, far, far, 0.0);
+  ra[f] = make_double4(kInertFar, kInertFar, kInertFar, 0.0);
+  rb[f] = make_double4(kInertFar, kInertFar, kInertFar, 0.0);
+}
+
+// Pair record of filaments f and f ^ 1 from the two lanes holding them (f even
+// on the even lane of the pair): every lane of the warp calls this; a lane
+// with `active` false stores nothing (its pair partner must be inactive too).
+// Float4 k of the record is {e[2k], o[2k], e[2k+1], o[2k+1]} (e, o the even
+// and odd filament's fields); the even lane stores k = 0..3, the odd lane 4..7.
+__device__ __forceinline__ void store_pair_fields(float4 *pk, long long f, const float v[16],
+                                                  bool active) {
+  const bool odd = (threadIdx.x & 1) != 0;
+  // x: the partner's fields this lane stores -- the odd filament's 0..7 on
+  // the even lane, the even filament's 8..15 on the odd lane
+  float x[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) x[q] = __shfl_xor_sync(0xffffffffu, odd ? v[q] : v[q + 8], 1);
+  if (!active) return;
+  float4 *rec = pk + (f >> 1) * 8;
+  if (!odd) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) rec[k] = make_float4(v[2 * k], x[2 * k], v[2 * k + 1], x[2 * k + 1]);
+  } else {
+#pragma unroll
+    for (int k = 4; k < 8; ++k)
+      rec[k] = make_float4(x[2 * k - 8], v[2 * k], x[2 * k - 7], v[2 * k + 1]);
+  }
 }
 
 // ---------------------------------------------------- FP64 reference pair term

@@ -58,6 +58,8 @@ __device__ __forceinline__ double trail_col(const WakeCase &c, const double *bou
 
 }  // namespace
 
+// One thread per (column j, blade b); the span loops are unrolled so a
+// thread keeps several loads in flight (the data is small; latency bounds this).
 __global__ void wake_bookkeep(const WakeCase *cases, const double *bound, const double *trail_prev,
                               double *shed, double *trail) {
   const WakeCase c = cases[blockIdx.y];
@@ -66,23 +68,25 @@ __global__ void wake_bookkeep(const WakeCase *cases, const double *bound, const 
   const int j = u % c.na, b = u / c.na;
   const int ns = c.nst - 1, m = c.na - 1;  // m trailing columns
   if (j < m) {
+#pragma unroll 8
     for (int i = 0; i < c.nst; ++i)
       trail[c.trail_off + i + (long long)c.nst * (j + (long long)m * b)] =
           trail_col(c, bound, trail_prev, i, j, b);
   }
   // shed(:, 0) = G; shed(:, j) = C_j - C_{j-1}, C_k = cumsum over span of trail(1:end-1, k),
   // C_m = 0 (WInDS.m:139-140)
+  double *out = shed + c.shed_off + (long long)ns * (j + (long long)c.na * b);
+  if (j == 0) {
+#pragma unroll 8
+    for (int i = 0; i < ns; ++i) out[i] = bound[c.bound_off + i + (long long)ns * b];
+    return;
+  }
   double cj = 0.0, cjm1 = 0.0;
+#pragma unroll 8
   for (int i = 0; i < ns; ++i) {
-    double v;
-    if (j == 0) {
-      v = bound[c.bound_off + i + (long long)ns * b];
-    } else {
-      cjm1 += trail_col(c, bound, trail_prev, i, j - 1, b);
-      if (j < m) cj += trail_col(c, bound, trail_prev, i, j, b);
-      v = cj - cjm1;
-    }
-    shed[c.shed_off + i + (long long)ns * (j + (long long)c.na * b)] = v;
+    cjm1 += trail_col(c, bound, trail_prev, i, j - 1, b);
+    if (j < m) cj += trail_col(c, bound, trail_prev, i, j, b);
+    out[i] = cj - cjm1;
   }
 }
 
@@ -95,6 +99,7 @@ __global__ void wake_filaments(const WakeCase *cases, const int *step, int step_
   const WakeCase c = cases[blockIdx.y];
   const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+  float v[16];
   const int ns = c.nst - 1;
   const long long nsh = (long long)ns * c.na * c.nb;
   if (f < c.fil_count) {
@@ -106,9 +111,10 @@ __global__ void wake_filaments(const WakeCase *cases, const int *step, int step_
     const double *lold;
     double *lnew, *rcout;
     if (f < nsh) {  // shed: dom(i) -> dom(i+1) at column j
-      i = (int)(f % ns);
-      j = (int)((f / ns) % c.na);
-      b = (int)(f / ((long long)ns * c.na));
+      const int fi = (int)f, q = fi / ns;  // per-case indices fit in 32 bits
+      i = fi - q * ns;
+      j = q % c.na;
+      b = q / c.na;
       m = c.na;
       x1 = node_comp(dom, c, i, 0, j, b), y1 = node_comp(dom, c, i, 1, j, b);
       z1 = node_comp(dom, c, i, 2, j, b);
@@ -121,9 +127,10 @@ __global__ void wake_filaments(const WakeCase *cases, const int *step, int step_
       if (rc_in_s) rcout = nullptr;
     } else {  // trailing: dom(:, j+1) -> dom(:, j)
       const long long k = f - nsh;
-      i = (int)(k % c.nst);
-      j = (int)((k / c.nst) % (c.na - 1));
-      b = (int)(k / ((long long)c.nst * (c.na - 1)));
+      const int ki = (int)k, q = ki / c.nst;
+      i = ki - q * c.nst;
+      j = q % (c.na - 1);
+      b = q / (c.na - 1);
       m = c.na - 1;
       x1 = node_comp(dom, c, i, 0, j + 1, b), y1 = node_comp(dom, c, i, 1, j + 1, b);
       z1 = node_comp(dom, c, i, 2, j + 1, b);
@@ -152,12 +159,21 @@ __global__ void wake_filaments(const WakeCase *cases, const int *step, int step_
       lnew[slot] = L;
       if (rcout) rcout[slot] = rc;
     }
-    pack_filament(c.fil_off + f, x1, y1, z1, x2, y2, z2, g, rc, model, dcut, pf.pk, pf.ra, pf.rb);
+    pf.ra[c.fil_off + f] = make_double4(x1, y1, z1, g);
+    pf.rb[c.fil_off + f] = make_double4(x2, y2, z2, rc);
+    filament_fields(x1, y1, z1, x2, y2, z2, g, rc, model, dcut, v);
     lo[0] = (float)fmin(x1, x2), lo[1] = (float)fmin(y1, y2), lo[2] = (float)fmin(z1, z2);
     hi[0] = (float)fmax(x1, x2), hi[1] = (float)fmax(y1, y2), hi[2] = (float)fmax(z1, z2);
-  } else if (f < c.fil_pad) {
-    pack_inert(c.fil_off + f, pf.pk, pf.ra, pf.rb);
+  } else {
+    inert_fields(v);
+    if (f < c.fil_pad) {
+      pf.ra[c.fil_off + f] = make_double4(kInertFar, kInertFar, kInertFar, 0.0);
+      pf.rb[c.fil_off + f] = make_double4(kInertFar, kInertFar, kInertFar, 0.0);
+    }
   }
+  // fil_off and fil_pad are multiples of kFilamentPad, so both filaments of a
+  // pair are in this warp and both are stored (real or inert) or neither is
+  store_pair_fields(pf.pk, c.fil_off + f, v, f < c.fil_pad);
   bbox_accumulate(lo, hi, bb->fmin, bb->fmax);
 }
 
@@ -168,7 +184,7 @@ __global__ void wake_targets(const WakeCase *cases, const double *dom, double4 *
   const long long n = (long long)c.nst * c.na * c.nb;
   float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
   if (t < n) {
-    const long long jk = t / c.nst, i = t - jk * c.nst;
+    const int ti = (int)t, jk = ti / c.nst, i = ti - jk * c.nst;
     const long long base = c.node_off * 3 + i + c.nst * 3 * jk;
     const double x = dom[base], y = dom[base + c.nst], z = dom[base + 2 * c.nst];
     tp[c.node_off + t] = make_double4(x, y, z, 0.0);
@@ -195,7 +211,8 @@ __global__ void wake_convect(const WakeCase *cases, const int *step, int mode, c
   const long long n = (long long)c.nst * c.na * c.nb;
   if (t >= n) return;
   const int s = *step;
-  const int i = (int)(t % c.nst), j = (int)((t / c.nst) % c.na), b = (int)(t / ((long long)c.nst * c.na));
+  const int ti = (int)t, q = ti / c.nst;  // per-case indices fit in 32 bits
+  const int i = ti - q * c.nst, j = q % c.na, b = q / c.na;
   double v[3];
   if (mode != kConvectCorrector) {
     double w[3];
