@@ -132,6 +132,30 @@ def test_every_tiling_agrees(wb, synth, oracle):
                 assert per_target_rel(u, uc) < F32C_TOL, (T, KF, waves)
 
 
+def test_tiles_full_of_near_pairs(wb, oracle):
+    """A compact ring of 64 short filaments with a 1 m core inside a cloud of
+    1024 targets: every pair is near-singular, so each tile lists far more
+    FP64 pairs than one pass of its list holds. All of them are counted and
+    the sums match the FP64 oracle for every tiling."""
+    rng = np.random.default_rng(11)
+    nf, nt = 64, 1024
+    a = np.linspace(0.0, 2 * np.pi, nf + 1)
+    ring = np.stack([np.cos(a), np.sin(a), 0.1 * np.sin(3 * a)], 1)
+    F1 = np.asfortranarray(ring[:-1].reshape(nf, 3, 1, 1))
+    F2 = np.asfortranarray(ring[1:].reshape(nf, 3, 1, 1))
+    g = np.asfortranarray(rng.uniform(5.0, 15.0, (nf, 1, 1, 1)))
+    rc = np.full((nf, 1, 1, 1), 1.0, order="F")
+    P = np.asfortranarray(rng.uniform(-1.0, 1.0, (nt, 3, 1, 1)))
+    fams = [(F1, F2, g, rc)]
+    uo = oracle.c_eval(F1, F2, P, g, rc, "visc2", 1000.0)
+    for T in (2, 4, 8):
+        for KF in (32, 64):
+            wb.set_tuning(wb.bs.CORE_VATISTAS, nt, nf, T, KF, 4.0)
+            u = wb.eval_host(fams, P, wb.bs.CORE_VATISTAS, 2.0, 1000.0, "f32c")
+            assert wb.last_stats()[2] == nf * nt, (T, KF)
+            assert per_target_rel(u, uo) < 1e-6, (T, KF)
+
+
 def test_edge_cases_gpu(wb):
     """Zero-length filament, NaN circulation, targets on an endpoint, on a
     filament and on its extension, and the reach cut-off co."""

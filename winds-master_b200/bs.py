@@ -114,11 +114,13 @@ def _params(core, dval, co, precision, flags=0):
     return p
 
 
-def eval_host(families, P, core, dval, co, precision="f32c", flags=0):
+def eval_host(families, P, core, dval, co, precision="f32c", flags=0, out=None):
     """Induced velocity of host (NumPy) filament families at host points ``P``.
 
     ``families``: list of ``(F1, F2, gamma, rc)`` NumPy arrays in WInDS layout.
-    Returns ``uind`` with ``P``'s (4-D padded) shape, Fortran order."""
+    Returns ``uind`` with ``P``'s (4-D padded) shape, Fortran order; ``out``,
+    if given, is that array (float64, Fortran-contiguous, e.g. in pinned
+    memory so the device-to-host copy needs no staging)."""
     L = lib()
     P = np.asfortranarray(P, dtype=np.float64)
     pd = _dims4(P.shape)
@@ -133,7 +135,11 @@ def eval_host(families, P, core, dval, co, precision="f32c", flags=0):
         fams[k].F1, fams[k].F2 = F1.ctypes.data, F2.ctypes.data
         fams[k].gamma, fams[k].rc = g.ctypes.data, rc.ctypes.data
         fams[k].dims[:] = _dims4(F1.shape)
-    out = np.zeros(pd, order="F")
+    if out is None:
+        out = np.zeros(pd, order="F")
+    elif (out.dtype != np.float64 or tuple(out.shape) != tuple(pd)
+          or not out.flags.f_contiguous):
+        raise ValueError(f"out must be a Fortran-contiguous float64 array of shape {tuple(pd)}")
     prm = _params(core, dval, co, precision, flags)
     _check(L.winds_bs_eval_host(fams, len(families), P.ctypes.data, (C.c_longlong * 4)(*pd),
                                 C.byref(prm), out.ctypes.data))

@@ -449,6 +449,8 @@ int run_direct_sum(Context *c, const std::vector<GroupSpec> &gs, int model, doub
   a.co = co;
   a.wait_limit_ns = default_wait_limit_ns();
   cudaError_t e = cudaMemsetAsync(c->ctr.p, 0, sizeof(unsigned), s);
+  // near-singular pairs are counted per evaluation
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->nearctr.p, 0, sizeof(unsigned long long), s);
   if (e != cudaSuccess) return cuda_fail(e, "work counter reset");
   const int grid = (int)std::max<long long>(1, std::min<long long>(a.n_items, resident));
   if (time_main) cudaEventRecord(c->ev_main0, s);
