@@ -7,11 +7,12 @@
 //                      (+ FP64 copies), the device-side replacement of the host
 //                      crunch_f / crunch_rg packing (BiotSavartMex.cu:316-357)
 //   bs_pack_targets    MATLAB-layout P -> double4 targets (crunch_p, :361-379)
-//   bs_f32c            persistent FP32 direct sum: filament tiles staged into
-//                      shared memory by bulk copies (cp.async.bulk + mbarrier),
-//                      T register-resident targets per thread, Kahan-compensated
-//                      per-target sums across tiles, FP64 recomputation of the
-//                      near-singular pairs
+//   bs_f32c            persistent FP32 direct sum on independent warp workers:
+//                      each warp stages its filament tiles into its own shared
+//                      memory by bulk copies (cp.async.bulk + mbarrier), keeps
+//                      T register-resident targets per lane, Kahan-compensates
+//                      the per-target sums, and recomputes the near-singular
+//                      pairs in FP64 with all 32 lanes
 //   bs_f64             plain FP64 direct sum (the comparison GPU path)
 //   bs_reduce          deterministic sum of the per-chunk partials, written in
 //                      MATLAB layout (reassem_uind, :383-401)
