@@ -536,10 +536,11 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<T>::value) bs_f32c(const F
   unsigned gt = 0;
   unsigned near_cnt = 0;
   while (true) {
-    int item_id = 0;
-    if (lane == 0) item_id = (int)atomicAdd(a.work_ctr, 1u);
-    item_id = __shfl_sync(0xffffffffu, item_id, 0);
-    if (item_id >= a.n_items) break;
+    int q = 0;
+    if (lane == 0) q = (int)atomicAdd(a.work_ctr, 1u);
+    q = __shfl_sync(0xffffffffu, q, 0);
+    if (q >= a.n_items) break;
+    const int item_id = a.order ? a.order[q] : q;
     const Item it = a.items[item_id];
     const Tile tl = a.tiles[it.tile];
     if (tl.t_count <= 0 || ((it.f_end - it.f_begin) % KF) != 0) {
@@ -644,9 +645,10 @@ __global__ void __launch_bounds__(kF64Threads) bs_f64(const F32cArgs a) {
   while (true) {
     if (tid == 0) s_item = (int)atomicAdd(a.work_ctr, 1u);
     __syncthreads();
-    const int item_id = s_item;
+    const int q = s_item;
     __syncthreads();
-    if (item_id >= a.n_items) break;
+    if (q >= a.n_items) break;
+    const int item_id = a.order ? a.order[q] : q;
     const Item it = a.items[item_id];
     const Tile tl = a.tiles[it.tile];
     int l = tid < tl.t_count ? tid : tl.t_count - 1;

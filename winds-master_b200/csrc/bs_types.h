@@ -68,6 +68,7 @@ struct F32cArgs {
   const Group *groups;
   const Tile *tiles;
   const Item *items;
+  const int *order;  // work queue: queue position -> item (nullptr: identity)
   int n_items;
   int tile_cap;
   double *part;

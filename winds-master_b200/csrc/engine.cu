@@ -164,7 +164,8 @@ void shutdown_all() {
     cudaStreamSynchronize(c->stream);
     for (DevBuf *b : {&c->pk, &c->ra, &c->rb, &c->tp, &c->tp_raw,
                       &c->tgroup, &c->keys, &c->vals, &c->perm, &c->sort_tmp, &c->groups,
-                      &c->tiles, &c->items, &c->part, &c->bbox, &c->ctr, &c->err, &c->nearctr,
+                      &c->tiles, &c->items, &c->order, &c->part, &c->bbox, &c->ctr, &c->err,
+                      &c->nearctr,
                       &c->in_P, &c->in_F, &c->out_u})
       b->release();
     c->htab.release();
@@ -183,13 +184,20 @@ static long long round_up(long long x, long long m) { return (x + m - 1) / m * m
 
 // Splits each group into tiles of tile_cap targets and each tile's filament
 // range into chunks, aiming at `waves` rounds of the resident workers so the
-// persistent kernel's work queue stays balanced.
+// persistent kernel's work queue stays balanced. The last part of every
+// tile's range (a fraction min(1/4, 2/waves) of the work) is cut into
+// quarter-size chunks that the queue hands out after all full-size ones, so
+// the workers finish together (guided scheduling). Items stay tile-major in
+// `items` (the reduce sums a tile's partials in filament order); `order`
+// is the queue: queue position -> item.
 void build_plan(Plan &pl, const std::vector<GroupSpec> &gs, int tile_cap, int resident,
                 double waves, int chunk_quantum) {
   pl.tile_cap = tile_cap;
   pl.groups.clear();
   pl.tiles.clear();
   pl.items.clear();
+  pl.order.clear();
+  std::vector<int> tail_items;
   double total_work = 0.0;
   long long total_tiles = 0;
   for (const GroupSpec &g : gs) {
@@ -201,6 +209,8 @@ void build_plan(Plan &pl, const std::vector<GroupSpec> &gs, int tile_cap, int re
   long long chunk = (long long)std::ceil(total_work / want_items);
   chunk = std::max<long long>(round_up(std::max<long long>(chunk, 1), chunk_quantum),
                               chunk_quantum);
+  const long long tail_chunk = round_up(std::max<long long>(chunk / 4, 1), chunk_quantum);
+  const double tail_frac = waves > 0.0 && tail_chunk < chunk ? std::min(0.25, 2.0 / waves) : 0.0;
   for (size_t gi = 0; gi < gs.size(); ++gi) {
     const GroupSpec &g = gs[gi];
     Group G;
@@ -221,47 +231,61 @@ void build_plan(Plan &pl, const std::vector<GroupSpec> &gs, int tile_cap, int re
       T.group = (int)gi;
       T.first_item = (int)pl.items.size();
       T.n_items = 0;
-      for (long long f0 = g.f_begin; f0 < g.f_end; f0 += chunk) {
+      const long long range = (long long)g.f_end - g.f_begin;
+      const long long tail = (long long)(tail_frac * (double)range) / tail_chunk * tail_chunk;
+      const long long f_mid = g.f_end - tail;
+      for (long long f0 = g.f_begin; f0 < g.f_end;) {
+        const bool in_tail = f0 >= f_mid;
+        const long long f1 = std::min<long long>(f0 + (in_tail ? tail_chunk : chunk),
+                                                 in_tail ? g.f_end : f_mid);
         Item I;
         I.tile = (int)pl.tiles.size();
         I.f_begin = (int)f0;
-        I.f_end = (int)std::min<long long>(f0 + chunk, g.f_end);
+        I.f_end = (int)f1;
         I.pad = 0;
+        (in_tail ? tail_items : pl.order).push_back((int)pl.items.size());
         pl.items.push_back(I);
         ++T.n_items;
+        f0 = f1;
       }
       if (T.n_items == 0) {  // empty filament range: one empty item writes zeros
         Item I;
         I.tile = (int)pl.tiles.size();
         I.f_begin = I.f_end = g.f_begin;
         I.pad = 0;
+        pl.order.push_back((int)pl.items.size());
         pl.items.push_back(I);
         T.n_items = 1;
       }
       pl.tiles.push_back(T);
     }
   }
+  pl.order.insert(pl.order.end(), tail_items.begin(), tail_items.end());
 }
 
 int upload_plan(Context *c, const Plan &pl, cudaStream_t s) {
   const size_t gb = pl.groups.size() * sizeof(Group);
   const size_t tb = pl.tiles.size() * sizeof(Tile);
   const size_t ib = pl.items.size() * sizeof(Item);
+  const size_t ob = pl.order.size() * sizeof(int);
   int rc;
   if ((rc = c->groups.ensure(gb + 16, s)) || (rc = c->tiles.ensure(tb + 16, s)) ||
-      (rc = c->items.ensure(ib + 16, s)))
+      (rc = c->items.ensure(ib + 16, s)) || (rc = c->order.ensure(ob + 16, s)))
     return rc;
   // the pinned staging may still feed the previous upload
   cudaEventSynchronize(c->ev_upload);
-  if ((rc = c->htab.ensure(gb + tb + ib + 64))) return rc;
+  if ((rc = c->htab.ensure(gb + tb + ib + ob + 64))) return rc;
   char *h = static_cast<char *>(c->htab.p);
   std::memcpy(h, pl.groups.data(), gb);
   std::memcpy(h + gb, pl.tiles.data(), tb);
   std::memcpy(h + gb + tb, pl.items.data(), ib);
+  std::memcpy(h + gb + tb + ib, pl.order.data(), ob);
   cudaError_t e;
   if ((e = cudaMemcpyAsync(c->groups.p, h, gb, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
       (e = cudaMemcpyAsync(c->tiles.p, h + gb, tb, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
-      (e = cudaMemcpyAsync(c->items.p, h + gb + tb, ib, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+      (e = cudaMemcpyAsync(c->items.p, h + gb + tb, ib, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(c->order.p, h + gb + tb + ib, ob, cudaMemcpyHostToDevice, s)) !=
+          cudaSuccess)
     return cuda_fail(e, "plan upload");
   cudaEventRecord(c->ev_upload, s);
   return WINDS_BS_OK;
@@ -436,6 +460,7 @@ int run_direct_sum(Context *c, const std::vector<GroupSpec> &gs, int model, doub
   a.groups = (const Group *)c->groups.p;
   a.tiles = (const Tile *)c->tiles.p;
   a.items = (const Item *)c->items.p;
+  a.order = (const int *)c->order.p;
   a.n_items = (int)pl.items.size();
   a.tile_cap = tile_cap;
   a.part = (double *)c->part.p;

@@ -44,6 +44,7 @@ struct Plan {
   std::vector<Group> groups;
   std::vector<Tile> tiles;
   std::vector<Item> items;
+  std::vector<int> order;  // work queue: queue position -> item
 };
 
 struct TuneChoice {
@@ -61,7 +62,7 @@ struct Context {
   // packed inputs; targets sorted (tp) from their packed order (tp_raw)
   DevBuf pk, ra, rb, tp, tp_raw, tgroup, keys, vals, perm, sort_tmp;
   // plan tables and partial sums
-  DevBuf groups, tiles, items, part;
+  DevBuf groups, tiles, items, order, part;
   // small words
   DevBuf bbox, ctr, err, nearctr;
   // device copies of host inputs/outputs (host API)

@@ -243,6 +243,7 @@ extern "C" int winds_bs_eval_device_noalloc(const winds_bs_family *fams, int nfa
   a.groups = groups;
   a.tiles = tiles;
   a.items = items;
+  a.order = nullptr;  // items are generated in queue order
   a.n_items = n_items;
   a.tile_cap = tile_cap;
   a.part = part;

@@ -48,7 +48,7 @@ struct winds_wake_batch {
   DevBuf quarter, trailing, wind;
   // direct-sum buffers
   DevBuf pk, ra, rb, tp, tp_raw, tgroup, keys, vals, perm, sort_tmp;
-  DevBuf groups_main, groups_pred, tiles, items, part, bbox, ctr, err, nearctr;
+  DevBuf groups_main, groups_pred, tiles, items, order, part, bbox, ctr, err, nearctr;
   size_t sort_bytes = 0;
   int n_tiles = 0, n_items = 0, tile_cap = 0, grid = 0;
   TuneChoice ch;
@@ -63,7 +63,7 @@ struct winds_wake_batch {
   long long n_ll = 0, frames_n = 0, stations_n = 0;
   int max_st = 0;
   DevBuf kjc_d, ll, bxn, byn, bzn, vblade, chord, foil, foil_off, aoa_t, cl_t, cd_t;
-  DevBuf tp_ll, perm_ll, uindb, kj_groups, kj_tiles, kj_items, kj_part;
+  DevBuf tp_ll, perm_ll, uindb, kj_groups, kj_tiles, kj_items, kj_order, kj_part;
   DevBuf conv, iters, res_max, res_last, active, diverged, cl_o, cd_o, aoa_o;
   int kj_ntiles = 0, kj_nitems = 0, kj_grid = 0, kj_tile_cap = 0, kj_T = 2, kj_KF = 64;
   long long kj_evals = 0;
@@ -169,6 +169,7 @@ int build_plans(winds_wake_batch *b) {
       (rc = b->groups_pred.ensure(gp.size() * sizeof(Group), s)) ||
       (rc = b->tiles.ensure(pl.tiles.size() * sizeof(Tile), s)) ||
       (rc = b->items.ensure(pl.items.size() * sizeof(Item), s)) ||
+      (rc = b->order.ensure(pl.order.size() * sizeof(int), s)) ||
       (rc = b->part.ensure((size_t)b->n_items * 3 * b->tile_cap * sizeof(double), s)))
     return rc;
   cudaError_t e;
@@ -179,6 +180,8 @@ int build_plans(winds_wake_batch *b) {
       (e = cudaMemcpy(b->tiles.p, pl.tiles.data(), pl.tiles.size() * sizeof(Tile),
                       cudaMemcpyHostToDevice)) != cudaSuccess ||
       (e = cudaMemcpy(b->items.p, pl.items.data(), pl.items.size() * sizeof(Item),
+                      cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMemcpy(b->order.p, pl.order.data(), pl.order.size() * sizeof(int),
                       cudaMemcpyHostToDevice)) != cudaSuccess)
     return cuda_fail(e, "wake plan upload");
   return WINDS_BS_OK;
@@ -221,6 +224,7 @@ cudaError_t enqueue_eval(winds_wake_batch *b, const double *dom, const double *s
   a.groups = P<const Group>(groups);
   a.tiles = P<const Tile>(b->tiles);
   a.items = P<const Item>(b->items);
+  a.order = P<const int>(b->order);
   a.n_items = b->n_items;
   a.tile_cap = b->tile_cap;
   a.part = P<double>(b->part);
@@ -364,6 +368,7 @@ cudaError_t enqueue_kj_iter(winds_wake_batch *b, int &launches, cudaStream_t s,
   a.groups = P<const Group>(b->kj_groups);
   a.tiles = P<const Tile>(b->kj_tiles);
   a.items = P<const Item>(b->kj_items);
+  a.order = P<const int>(b->kj_order);
   a.n_items = b->kj_nitems;
   a.tile_cap = b->kj_tile_cap;
   a.part = P<double>(b->kj_part);
@@ -1122,11 +1127,13 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
   if ((rc = b->kj_groups.ensure(pl.groups.size() * sizeof(Group), s)) ||
       (rc = b->kj_tiles.ensure(pl.tiles.size() * sizeof(Tile), s)) ||
       (rc = b->kj_items.ensure(pl.items.size() * sizeof(Item), s)) ||
+      (rc = b->kj_order.ensure(pl.order.size() * sizeof(int), s)) ||
       (rc = b->kj_part.ensure((size_t)b->kj_nitems * 3 * b->kj_tile_cap * sizeof(double), s)))
     return rc;
   if ((e = cudaMemcpy(b->kj_groups.p, pl.groups.data(), pl.groups.size() * sizeof(Group), cudaMemcpyHostToDevice)) != cudaSuccess ||
       (e = cudaMemcpy(b->kj_tiles.p, pl.tiles.data(), pl.tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice)) != cudaSuccess ||
-      (e = cudaMemcpy(b->kj_items.p, pl.items.data(), pl.items.size() * sizeof(Item), cudaMemcpyHostToDevice)) != cudaSuccess)
+      (e = cudaMemcpy(b->kj_items.p, pl.items.data(), pl.items.size() * sizeof(Item), cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMemcpy(b->kj_order.p, pl.order.data(), pl.order.size() * sizeof(int), cudaMemcpyHostToDevice)) != cudaSuccess)
     return cuda_fail(e, "lifting-line plan upload");
   // graphs captured without the iteration must be rebuilt
   if (b->exec) {
@@ -1239,7 +1246,8 @@ void winds_wake_destroy(winds_wake_batch *b) {
   b->kj_it.release();
   for (DevBuf *x : {&b->kjc_d, &b->ll, &b->bxn, &b->byn, &b->bzn, &b->vblade, &b->chord, &b->foil,
                     &b->foil_off, &b->aoa_t, &b->cl_t, &b->cd_t, &b->tp_ll, &b->perm_ll, &b->uindb,
-                    &b->kj_groups, &b->kj_tiles, &b->kj_items, &b->kj_part, &b->conv, &b->iters,
+                    &b->kj_groups, &b->kj_tiles, &b->kj_items, &b->kj_order, &b->kj_part,
+                    &b->conv, &b->iters,
                     &b->res_max, &b->res_last, &b->active, &b->diverged, &b->cl_o, &b->cd_o,
                     &b->aoa_o, &b->st_r, &b->st_c, &b->st_tw, &b->azim, &b->guess, &b->feat,
                     &b->bound_last, &b->st_rr, &b->st_dr, &b->rpm, &b->dl, &b->loads_out})
@@ -1251,7 +1259,7 @@ void winds_wake_destroy(winds_wake_batch *b) {
                     &b->rc_t, &b->len_old_s, &b->len_old_t, &b->len_s, &b->len_t, &b->len_ps,
                     &b->len_pt, &b->quarter, &b->trailing, &b->wind, &b->pk, &b->ra, &b->rb, &b->tp, &b->tp_raw, &b->tgroup, &b->keys, &b->vals,
                     &b->perm, &b->sort_tmp, &b->groups_main, &b->groups_pred, &b->tiles,
-                    &b->items, &b->part, &b->bbox, &b->ctr, &b->err, &b->nearctr})
+                    &b->items, &b->order, &b->part, &b->bbox, &b->ctr, &b->err, &b->nearctr})
     x->release();
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
