@@ -80,6 +80,33 @@ def test_graph_with_network_matches_host_loop(wb):
     m.close()
 
 
+def test_attach_detach_between_graph_steps(wb):
+    """Attaching and detaching the network between steps rebuilds the
+    captured step each time: graph replay and the host loop agree bit for
+    bit through attach, detach and re-attach."""
+    gi, mlp, wake, synth = _mods()
+    pts = gi.operating_points(3, seed=7, nst=13, wake_steps=10)
+    m = mlp.Mlp(gi.N_FEATURES, seed=5)
+    m.set_scaling(np.zeros(10, np.float32), np.full(10, 0.2, np.float32), 0.02)
+    out = []
+    for graph in (False, True):
+        cases, kjs = gi.build(pts, 5)
+        b = wake.WakeBatch(cases, integrator="pcc")
+        b.set_kj(kjs, relax=0.3, tol=1e-6, maxiter=100)
+        rec = []
+        for net in (m, None, m):
+            b.set_mlp(net)
+            b.step(1, graph=graph)
+            rec.append(b.kj_stats()[0].copy())
+        out.append((rec, [b.bound(k) for k in range(3)]))
+        b.close()
+    for a, c in zip(out[0][0], out[1][0]):
+        np.testing.assert_array_equal(a, c)
+    for a, c in zip(out[0][1], out[1][1]):
+        np.testing.assert_array_equal(a, c)
+    m.close()
+
+
 def test_trained_start_value_saves_iterations(wb):
     """Trained on plain-solver pairs (~4.5e5) of the attached-flow operating
     points among 400 candidates, the network's start value needs fewer
