@@ -67,3 +67,65 @@ def test_nrel_oracle_step_is_plausible():
     r.step()
     assert r.kj_iters < 200
     assert 2e5 < r.T < 1.5e6 and r.P > 0
+
+
+def _fast_channels(m, nsteps=30, na=12):
+    """FAST-style channels of a yawed rotor on a pitching platform."""
+    md = _md()
+    ser = md.operating_series(m, U=10.0, tsr=7.5, pitch=2.0, yaw=8.0, nsteps=nsteps, na=na)
+    t = ser["time"]
+    ch = {"Time": t, "Azimuth": ser["azimuth"]}
+    for b in range(int(m["nb"])):
+        ch[f"BldPitch{b + 1}"] = ser["pitch"][:, b] + 0.5 * np.sin(0.3 * t + b)
+    ch["NacYaw"] = ser["nac_yaw"]
+    names = ("PtfmSurge", "PtfmSway", "PtfmHeave", "PtfmRoll", "PtfmPitch", "PtfmYaw")
+    amp = (0.4, 0.1, 0.05, 0.3, 1.2, 0.2)
+    for k, (n, a) in enumerate(zip(names, amp)):
+        ch[n] = a * np.sin(0.2 * t + k)
+    ch["WindVxi"], ch["WindVyi"], ch["WindVzi"] = ser["wind"][:, 0], ser["wind"][:, 1], ser["wind"][:, 2]
+    ch["RotSpeed"] = np.full_like(t, ser["_omega"] * 30.0 / np.pi)
+    return ser, ch
+
+
+def test_fast_out_roundtrip_and_resampling(tmp_path):
+    """output_import.m's reading: names on line 7, units on 8, samples after;
+    channels interpolated linearly to t0:1/freq:t1, clamped to the record."""
+    md = _md()
+    m = md.load_model(os.path.join(GOLDEN, "nrel5mw.npz"))
+    _, ch = _fast_channels(m)
+    path = str(tmp_path / "run.out")
+    md.write_fast_out(path, ch)
+    fo = md.read_fast_out(path)
+    assert fo["units"]["Time"] == "(s)" and fo["units"]["Azimuth"] == "(deg)"
+    for k, v in ch.items():
+        np.testing.assert_allclose(fo[k], v, rtol=1e-9, atol=1e-9)
+    t = ch["Time"]
+    t0, t1, freq = float(t[2]) + 0.03, float(t[-3]), 25.0
+    fr = md.read_fast_out(path, (t0, t1, freq))
+    ti = t0 + np.arange(int(np.floor((t1 - t0) * freq + 1e-9)) + 1) / freq
+    np.testing.assert_allclose(fr["Time"], ti, rtol=0, atol=1e-12)
+    for k in ("Azimuth", "PtfmPitch", "BldPitch2"):
+        np.testing.assert_allclose(fr[k], np.interp(ti, fo["Time"], fo[k]), rtol=1e-12, atol=1e-12)
+    fc = md.read_fast_out(path, (float(t[0]) - 5.0, float(t[-1]) + 5.0, 0.0))
+    assert fc["Time"][0] == fo["Time"][0] and abs(fc["Time"][-1] - fo["Time"][-1]) < 1e-9
+
+
+def test_series_from_fastout_matches_kinematics(tmp_path):
+    """A FAST time series through series_from_fastout gives the same blade
+    kinematics (FP64 oracle) as the series it was written from."""
+    import kin_ref
+    md = _md()
+    m = md.load_model(os.path.join(GOLDEN, "nrel5mw.npz"))
+    ser, ch = _fast_channels(m)
+    ser = dict(ser, pitch=np.stack([ch[f"BldPitch{b + 1}"] for b in range(int(m["nb"]))], 1),
+               ptfm=np.stack([ch[n] for n in ("PtfmSurge", "PtfmSway", "PtfmHeave", "PtfmRoll",
+                                              "PtfmPitch", "PtfmYaw")], 1))
+    path = str(tmp_path / "run.out")
+    md.write_fast_out(path, ch)
+    fs = md.series_from_fastout(m, md.read_fast_out(path), na=12)
+    k0, k1 = kin_ref.kinematics(ser), kin_ref.kinematics(fs)
+    for name in ("quarter", "trail", "bound", "bxn", "vblade"):
+        np.testing.assert_allclose(k1[name], k0[name], rtol=1e-8, atol=1e-8)
+    wc, kj = md.cases(m, fs, k1)
+    assert wc["nsteps"] == fs["_nsteps"] + 1 and kj["rpm"].shape == (wc["nsteps"],)
+    np.testing.assert_allclose(kj["rpm"], ch["RotSpeed"][11:], rtol=1e-9)  # 11 digits written

@@ -11,6 +11,13 @@ cases built from them through the kinematics.
     for a constant wind, tip-speed ratio, pitch and nacelle yaw with the
     platform at rest (``fastout.Azimuth = omega t``, ``RotSpeed``), from
     ``t = -(na - 1) dt`` so the initial wake has a history.
+  * ``read_fast_out(path, t)`` -- a FAST output file as
+    ``core/output_import.m:37-72`` reads it: channel names on line 7, units
+    on line 8, tab-separated samples after; every channel interpolated
+    linearly to ``t0 : 1/freq : t1`` (clamped to the recorded times).
+  * ``series_from_fastout(model, fo)`` -- the kinematics inputs of a FAST time
+    series (``fastout.Azimuth``, ``BldPitch1..nb``, ``NacYaw``, ``Ptfm*``,
+    ``WindV*i``, ``RotSpeed``), in the form ``operating_series`` returns.
   * ``cases(...)`` -- a ``winds_wake_case`` and a ``winds_kj_case`` (dicts for
     ``wake.WakeBatch`` / ``set_kj``) from the kinematics of that series.
 """
@@ -73,6 +80,96 @@ def operating_series(model: dict, U=11.4, tsr=7.0, pitch=0.0, yaw=0.0, hz=10.0, 
                 ptfm_ref=0.0, _omega=omega, _U=U, _pitch=pitch, _na=na, _nsteps=nsteps, _hz=hz)
 
 
+FAST_CHANNELS = ("Time", "Azimuth", "NacYaw", "PtfmSurge", "PtfmSway", "PtfmHeave", "PtfmRoll",
+                 "PtfmPitch", "PtfmYaw", "WindVxi", "WindVyi", "WindVzi", "RotSpeed")
+
+
+def read_fast_out(path: str, t=(-float("inf"), float("inf"), 0.0), dt=None, verbose=False) -> dict:
+    """Channels of a FAST output file (output_import.m:37-72): line 7 holds the
+    tab-separated channel names, line 8 the units, the samples follow.
+    ``dt``, when given (the .fst integration step of a non-Simulink run,
+    output_import.m:44-46), regrids the time column as ``t_first:dt:t_last``.
+    ``t = (t0, t1, freq)``: every channel is interpolated linearly to
+    ``t0 : 1/freq : t1``, with t0 and t1 clamped to the recorded range;
+    ``freq == 0`` keeps the file's mean sample rate. (The reference takes that
+    rate from differences along the first sample row, across channels; the
+    time column is what it means.) Returns name -> array, plus ``units``."""
+    with open(path) as f:
+        lines = f.read().splitlines()
+    names = lines[6].split("\t")
+    names = [n.strip() for n in names if n.strip()]
+    units = [u.strip() for u in lines[7].split("\t") if u.strip()]
+    rows = [[float(v) for v in ln.split()] for ln in lines[8:] if ln.strip()]
+    data = np.asarray(rows, dtype=np.float64)
+    if data.ndim != 2 or data.shape[1] != len(names):
+        raise ValueError(f"{path}: {len(names)} channel names, samples of width {data.shape}")
+    if dt is not None:
+        data[:, 0] = data[0, 0] + dt * np.arange(data.shape[0])
+    t0, t1, freq = (float(x) for x in t)
+    if freq == 0.0:
+        freq = 1.0 / float(np.mean(np.diff(data[:, 0])))
+    if t0 < data[0, 0]:
+        t0 = float(data[0, 0])
+        if verbose:
+            print(f"User selected initial time out-of-range, reset to {t0:g} seconds.")
+    if t1 > data[-1, 0]:
+        t1 = float(data[-1, 0])
+        if verbose:
+            print(f"User selected final time out-of-range, reset to {t1:g} seconds.")
+    n = int(np.floor((t1 - t0) * freq + 1e-9)) + 1
+    ti = t0 + np.arange(n) / freq
+    out = {"units": dict(zip(names, units))}
+    out[names[0]] = ti
+    for k, name in enumerate(names[1:], start=1):
+        out[name] = np.interp(ti, data[:, 0], data[:, k])
+    return out
+
+
+def series_from_fastout(model: dict, fo: dict, na: int = 40) -> dict:
+    """Kinematics inputs of a FAST time series (kinematics.m:27-109 reads
+    these channels), in ``operating_series``'s form: the first ``na - 1``
+    samples make the initial wake's history and step 0 is sample ``na - 1``.
+    The lifting line takes each station's twist plus the series' mean blade
+    pitch (the device loads use one pitch per case)."""
+    nb = int(model["nb"])
+    t = np.asarray(fo["Time"], np.float64)
+    nt = t.size
+    if nt < na + 1:
+        raise ValueError(f"{nt} samples; the initial wake needs na = {na} plus a step")
+    pitch = np.stack([np.asarray(fo[f"BldPitch{b + 1}"], np.float64) for b in range(nb)], 1)
+    ptfm = np.stack([np.asarray(fo[k], np.float64) for k in
+                     ("PtfmSurge", "PtfmSway", "PtfmHeave", "PtfmRoll", "PtfmPitch", "PtfmYaw")], 1)
+    wind = np.stack([np.asarray(fo[k], np.float64) for k in ("WindVxi", "WindVyi", "WindVzi")], 1)
+    st = stations(model["r_trail"], model["chord_trail"], model["twist_trail"], model["nfoil_trail"])
+    hz = 1.0 / float(np.mean(np.diff(t)))
+    omega = float(np.mean(fo["RotSpeed"])) * np.pi / 30.0
+    return dict(time=t, azimuth=np.asarray(fo["Azimuth"], np.float64), pitch=pitch,
+                nac_yaw=np.asarray(fo["NacYaw"], np.float64), ptfm=ptfm, wind=wind,
+                r_trail=model["r_trail"], chord_trail=model["chord_trail"],
+                twist_trail=model["twist_trail"], r_nodes=st["r_nodes"], chord=st["chord"],
+                twist=st["twist"], precone=np.full(nb, model["precone"]), overhang=model["overhang"],
+                shaft_tilt=model["shaft_tilt"], tower_ht=model["tower_ht"], twr2shft=model["twr2shft"],
+                ptfm_ref=0.0, rpm=np.asarray(fo["RotSpeed"], np.float64), _omega=omega,
+                _U=float(np.mean(wind[:, 0])), _pitch=float(pitch.mean()), _na=na,
+                _nsteps=nt - na, _hz=hz)
+
+
+def write_fast_out(path: str, channels: dict, title: str = "synthetic FAST output") -> None:
+    """Writes ``channels`` (name -> array, ``Time`` first) in the layout
+    ``read_fast_out`` reads: six header lines, names, units, samples."""
+    names = list(channels)
+    units = {"Time": "(s)", "Azimuth": "(deg)", "NacYaw": "(deg)", "RotSpeed": "(rpm)"}
+    with open(path, "w") as f:
+        f.write(f"{title}\n\n\n\n\n\n")
+        f.write("\t".join(names) + "\n")
+        f.write("\t".join(units.get(n, "(deg)" if "Pitch" in n or n[-3:] in ("oll", "Yaw")
+                                     else "(m)" if n.startswith("Ptfm") else "(m/s)")
+                          for n in names) + "\n")
+        data = np.stack([np.asarray(channels[n], np.float64) for n in names], 1)
+        for row in data:
+            f.write("\t".join(f"{v:.10E}" for v in row) + "\n")
+
+
 def cases(model: dict, series: dict, kin: dict, rc0=0.1, delta=100.0, nu=1.5e-5, alpha=1.25643) -> tuple:
     """(wake case, lifting-line case) from a series and its kinematics
     ``kin`` (device ``kin.kinematics`` or the oracle): step 0 at t = 0, the
@@ -113,7 +210,8 @@ def cases(model: dict, series: dict, kin: dict, rc0=0.1, delta=100.0, nu=1.5e-5,
               cd=np.concatenate([t["cd"] for t in tabs]), r_over_R=st["r_nodes"] / R,
               chord_over_R=st["chord"] / R, twist=np.radians(st["twist"] + series["_pitch"]),
               azimuth=f(az), r_station=st["r_nodes"], dr_station=st["dr"],
-              rpm=np.full(nsteps + 1, series["_omega"] * 30.0 / np.pi), rho=RHO)
+              rpm=(np.asarray(series["rpm"][s0:s0 + nsteps + 1], np.float64) if "rpm" in series
+                   else np.full(nsteps + 1, series["_omega"] * 30.0 / np.pi)), rho=RHO)
     return wake, kj
 
 
