@@ -129,6 +129,11 @@ typedef struct {
   const double *dr_station;   /* [ns] station width (blade.DRNodes), m             */
   const double *rpm;          /* [nsteps] rotor speed (fastout.RotSpeed), rpm      */
   double rho;                 /* air density (const.rho), kg/m^3                  */
+  /* Blade pitch per step and blade (fastout.BldPitch<b>), deg; optional. Given,
+   * the loads rotate by and subtract twist + pitch(step, blade) as
+   * perform.m:22-33 does and `twist` is the aerodynamic twist alone; NULL: a
+   * constant pitch is part of `twist`. */
+  const double *pitch;        /* [nsteps,nb]                                      */
 } winds_kj_case;
 
 typedef struct {

@@ -88,6 +88,9 @@ class KJWakeRef(wake_ref.WakeRef):
         kj = self.kj
         if "r_station" in kj:  # rotor loads of the step (postproc/perform.m)
             import perform_ref
+            theta = np.degrees(kj["twist"])
+            if kj.get("pitch") is not None:  # per step and blade (perform.m:22-33)
+                theta = theta[:, None] + np.asarray(kj["pitch"])[s][None, :]
             self.T, self.Q, self.P, _ = perform_ref.loads(
-                self.cl, self.cd, self.aoa, kj["vblade"][:, :, s, :], np.degrees(kj["twist"]),
+                self.cl, self.cd, self.aoa, kj["vblade"][:, :, s, :], theta,
                 kj["chord"], kj["r_station"], kj["dr_station"], kj["rpm"][s], kj["rho"])

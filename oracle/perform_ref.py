@@ -27,13 +27,16 @@ def rz(t_deg):
 
 def loads(cl, cd, aoa, vblade, theta_deg, chord, r, dr, rpm, rho):
     """cl, cd, aoa [ns, nb] (aoa in deg); vblade [ns, 3, nb]; theta_deg [ns]
-    (twist + blade pitch); chord, r, dr [ns]; rpm scalar. Returns T, Q, P and
-    the spanwise dT [ns, nb]."""
-    R = rz(np.asarray(theta_deg) - 90.0)                       # [ns, 3, 3]
-    velX = -np.einsum("sij,sjb->sib", R, vblade)               # [ns, 3, nb]
+    or [ns, nb] (twist + blade pitch, perform.m:22-33 per blade); chord, r, dr
+    [ns]; rpm scalar. Returns T, Q, P and the spanwise dT [ns, nb]."""
+    th = np.asarray(theta_deg, dtype=np.float64)
+    if th.ndim == 1:
+        th = np.repeat(th[:, None], np.shape(aoa)[1], axis=1)
+    R = rz(th - 90.0)                                          # [ns, nb, 3, 3]
+    velX = -np.einsum("sbij,sjb->sib", R, vblade)              # [ns, 3, nb]
     v1, v2 = velX[:, 0], velX[:, 1]
     tsr = v2 / v1
-    phi = aoa - np.asarray(theta_deg)[:, None]
+    phi = aoa - th
     tp = np.tan(np.radians(phi))
     aap = tsr / tp
     a = aap * (v1 - tp * v2) / (aap * v1 + tp * v2)

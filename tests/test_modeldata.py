@@ -129,3 +129,8 @@ def test_series_from_fastout_matches_kinematics(tmp_path):
     wc, kj = md.cases(m, fs, k1)
     assert wc["nsteps"] == fs["_nsteps"] + 1 and kj["rpm"].shape == (wc["nsteps"],)
     np.testing.assert_allclose(kj["rpm"], ch["RotSpeed"][11:], rtol=1e-9)  # 11 digits written
+    # blade pitch per step and blade for the loads; the twist is the aerodynamic twist alone
+    assert kj["pitch"].shape == (wc["nsteps"], int(m["nb"]))
+    np.testing.assert_allclose(kj["pitch"][:, 1], ch["BldPitch2"][11:], rtol=1e-9, atol=1e-9)
+    st = md.stations(m["r_trail"], m["chord_trail"], m["twist_trail"], m["nfoil_trail"])
+    np.testing.assert_allclose(kj["twist"], np.radians(st["twist"]), rtol=1e-15)

@@ -130,3 +130,27 @@ def test_perform_oracle_rotation_and_totals():
     cl[2, 1] = cd[2, 1] = 0.0
     _, _, _, dT0 = perform_ref.loads(cl, cd, aoa, vb, th, chord, r, dr, 12.1, 1.225)
     assert dT0[2, 1] == 0.0
+
+
+def test_perform_pitch_per_blade_matches_blade_by_blade():
+    """perform.m:22-33 rotates and subtracts twist + BldPitch<b> per blade:
+    the loads with a [ns, nb] angle equal the sum of single-blade loads."""
+    import perform_ref
+    rng = np.random.default_rng(4)
+    ns, nb = 9, 3
+    cl, cd = rng.uniform(0.2, 1.2, (ns, nb)), rng.uniform(0.01, 0.05, (ns, nb))
+    aoa = rng.uniform(2.0, 10.0, (ns, nb))
+    vb = np.stack([rng.uniform(-10, -5, (ns, nb)), rng.uniform(40, 60, (ns, nb)),
+                   rng.uniform(-1, 1, (ns, nb))], 1)
+    twist = rng.uniform(0.0, 13.0, ns)
+    pitch = rng.uniform(0.0, 8.0, nb)
+    chord, r, dr = rng.uniform(1.5, 4.0, ns), np.linspace(5, 60, ns), np.full(ns, 6.0)
+    T, Q, P, dT = perform_ref.loads(cl, cd, aoa, vb, twist[:, None] + pitch[None, :], chord, r, dr,
+                                    12.1, 1.225)
+    tot = np.zeros(3)
+    for b in range(nb):
+        t1, q1, p1, d1 = perform_ref.loads(cl[:, b:b + 1], cd[:, b:b + 1], aoa[:, b:b + 1],
+                                           vb[:, :, b:b + 1], twist + pitch[b], chord, r, dr, 12.1, 1.225)
+        tot += (t1, q1, p1)
+        np.testing.assert_allclose(dT[:, b], d1[:, 0], rtol=1e-14)
+    np.testing.assert_allclose((T, Q, P), tot, rtol=1e-12)

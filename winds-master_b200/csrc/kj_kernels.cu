@@ -145,7 +145,7 @@ __global__ void kj_dloads(const WakeCase *cases, const KJCase *kc, const int *st
                           const double *vblade, const double *cl, const double *cd,
                           const double *aoa, const double *st_tw, const double *chord,
                           const double *st_rr, const double *st_dr, const double *rpm,
-                          double *dl) {
+                          const double *pitch, double *dl) {
   const WakeCase c = cases[blockIdx.y];
   const KJCase k = kc[blockIdx.y];
   const int ns = c.nst - 1;
@@ -156,7 +156,8 @@ __global__ void kj_dloads(const WakeCase *cases, const KJCase *kc, const int *st
   const long long fo = k.frame_off + i + (long long)ns * (3 * (s + (long long)c.nsteps * b));
   const long long st = k.station_off + i;
   const long long q = c.bound_off + i + (long long)ns * b;
-  const double th = st_tw[st] * (180.0 / kPi);  // deg
+  double th = st_tw[st] * (180.0 / kPi);  // deg
+  if (k.has_pitch) th += pitch[k.az_off + s + (long long)c.nsteps * b];
   const double rot = (th - 90.0) * (kPi / 180.0);
   const double cr = cos(rot), sr = sin(rot);
   const double u0 = vblade[fo], u1 = vblade[fo + ns];
@@ -292,9 +293,10 @@ cudaError_t launch_kj_loads(const WakeCase *cases, const KJCase *kc, int ncases,
                             const int *step, const double *vblade, const double *cl,
                             const double *cd, const double *aoa, const double *st_tw,
                             const double *chord, const double *st_rr, const double *st_dr,
-                            const double *rpm, double *dl, double *out, cudaStream_t s) {
+                            const double *rpm, const double *pitch, double *dl, double *out,
+                            cudaStream_t s) {
   kj_dloads<<<dim3((max_st + 127) / 128, ncases), 128, 0, s>>>(
-      cases, kc, step, vblade, cl, cd, aoa, st_tw, chord, st_rr, st_dr, rpm, dl);
+      cases, kc, step, vblade, cl, cd, aoa, st_tw, chord, st_rr, st_dr, rpm, pitch, dl);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   kj_sum_loads<<<(ncases + 127) / 128, 128, 0, s>>>(cases, kc, ncases, dl, out);

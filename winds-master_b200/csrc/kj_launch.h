@@ -15,6 +15,7 @@ struct KJCase {
   long long az_off;       // nsteps*nb per case: blade azimuth (MLP features)
   long long rpm_off;      // nsteps per case: rotor speed (loads)
   double rho;             // air density (loads)
+  int has_pitch;          // blade pitch per step at az_off (loads), else in the twist
   int foil_base;          // this case's first entry in the foil offset table
   int n_foils;
 };
@@ -54,7 +55,8 @@ cudaError_t launch_kj_loads(const WakeCase *cases, const KJCase *kc, int ncases,
                             const int *step, const double *vblade, const double *cl,
                             const double *cd, const double *aoa, const double *st_tw,
                             const double *chord, const double *st_rr, const double *st_dr,
-                            const double *rpm, double *dl, double *out, cudaStream_t s);
+                            const double *rpm, const double *pitch, double *dl, double *out,
+                            cudaStream_t s);
 // kj_check that also sets a graph WHILE condition (see kj_kernels.cu).
 cudaError_t launch_kj_check_cond(int ncases, double tol, int *converged, int *iters,
                                  unsigned long long *res_max, double *res_last, int *active,

@@ -70,7 +70,7 @@ struct winds_wake_batch {
   // bound-circulation MLP start value
   bool mlp_inputs = false;      // every case gave the station arrays
   bool loads = false;           // every case gave the loads inputs
-  DevBuf st_rr, st_dr, rpm, dl, loads_out;
+  DevBuf st_rr, st_dr, rpm, pitch, dl, loads_out;
   DevBuf st_r, st_c, st_tw, azim, guess, feat, bound_last;
   winds_mlp *mlp = nullptr;
   MlpWork mw;
@@ -314,8 +314,8 @@ cudaError_t enqueue_post(winds_wake_batch *b, int &launches) {
                           P<const double>(b->cl_o), P<const double>(b->cd_o),
                           P<const double>(b->aoa_o), P<const double>(b->st_tw),
                           P<const double>(b->chord), P<const double>(b->st_rr),
-                          P<const double>(b->st_dr), P<const double>(b->rpm), P<double>(b->dl),
-                          P<double>(b->loads_out), s);
+                          P<const double>(b->st_dr), P<const double>(b->rpm),
+                          P<const double>(b->pitch), P<double>(b->dl), P<double>(b->loads_out), s);
       launches += 2;
     }
   }
@@ -952,7 +952,7 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
   b->kjp = *prm;
   b->kjc.clear();
   long long fr = 0, tt = 0, st = 0, tab = 0, az = 0, rp = 0;
-  bool all_inputs = true, have_twist = true, all_loads = true;
+  bool all_inputs = true, have_twist = true, all_loads = true, any_pitch = false;
   std::vector<int> foil_off, foils;
   std::vector<double> aoa, cl, cd, chord;
   b->max_st = 0;
@@ -973,6 +973,8 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
     if (!h.r_station || !h.dr_station || !h.rpm || !(h.rho > 0)) all_loads = false;
     q.rpm_off = rp;
     q.rho = h.rho;
+    q.has_pitch = h.pitch != nullptr;
+    any_pitch = any_pitch || h.pitch;
     q.foil_base = (int)foil_off.size();
     q.n_foils = h.n_foils;
     long long o = 0;
@@ -1048,6 +1050,14 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
         e2 = cudaMemcpy(P<double>(b->rpm) + b->kjc[k].rpm_off, kj[k].rpm,
                         (size_t)b->cases[k].nsteps * 8, cudaMemcpyHostToDevice);
       if (e2 != cudaSuccess) return cuda_fail(e2, "loads upload");
+    }
+    if ((rc = b->pitch.ensure(std::max<long long>(az, 1) * sizeof(double), s))) return rc;
+    for (int k = 0; k < b->ncases && any_pitch; ++k) {
+      if (!kj[k].pitch) continue;
+      const WakeCase &c = b->cases[k];
+      cudaError_t e2 = cudaMemcpy(P<double>(b->pitch) + b->kjc[k].az_off, kj[k].pitch,
+                                  (size_t)c.nsteps * c.nb * 8, cudaMemcpyHostToDevice);
+      if (e2 != cudaSuccess) return cuda_fail(e2, "pitch upload");
     }
     if (cudaError_t e0 = cudaMemset(b->loads_out.p, 0, b->ncases * 3 * sizeof(double)); e0 != cudaSuccess)
       return cuda_fail(e0, "loads reset");
@@ -1250,7 +1260,8 @@ void winds_wake_destroy(winds_wake_batch *b) {
                     &b->conv, &b->iters,
                     &b->res_max, &b->res_last, &b->active, &b->diverged, &b->cl_o, &b->cd_o,
                     &b->aoa_o, &b->st_r, &b->st_c, &b->st_tw, &b->azim, &b->guess, &b->feat,
-                    &b->bound_last, &b->st_rr, &b->st_dr, &b->rpm, &b->dl, &b->loads_out})
+                    &b->bound_last, &b->st_rr, &b->st_dr, &b->rpm, &b->pitch, &b->dl,
+                    &b->loads_out})
     x->release();
   b->mw.release();
   for (DevBuf *x : {&b->cases_d, &b->step_d, &b->dom, &b->dom_pred, &b->dom_new, &b->vel, &b->h1,

@@ -129,8 +129,8 @@ def series_from_fastout(model: dict, fo: dict, na: int = 40) -> dict:
     """Kinematics inputs of a FAST time series (kinematics.m:27-109 reads
     these channels), in ``operating_series``'s form: the first ``na - 1``
     samples make the initial wake's history and step 0 is sample ``na - 1``.
-    The lifting line takes each station's twist plus the series' mean blade
-    pitch (the device loads use one pitch per case)."""
+    The blade pitch goes to the loads per step and blade (``pitch``), as
+    perform.m:22-33 uses fastout.BldPitch<b>."""
     nb = int(model["nb"])
     t = np.asarray(fo["Time"], np.float64)
     nt = t.size
@@ -151,7 +151,7 @@ def series_from_fastout(model: dict, fo: dict, na: int = 40) -> dict:
                 shaft_tilt=model["shaft_tilt"], tower_ht=model["tower_ht"], twr2shft=model["twr2shft"],
                 ptfm_ref=0.0, rpm=np.asarray(fo["RotSpeed"], np.float64), _omega=omega,
                 _U=float(np.mean(wind[:, 0])), _pitch=float(pitch.mean()), _na=na,
-                _nsteps=nt - na, _hz=hz)
+                _nsteps=nt - na, _hz=hz, _pitch_per_step=True)
 
 
 def write_fast_out(path: str, channels: dict, title: str = "synthetic FAST output") -> None:
@@ -201,6 +201,7 @@ def cases(model: dict, series: dict, kin: dict, rc0=0.1, delta=100.0, nu=1.5e-5,
     tabs = model["tables"]
     R = float(model["r_trail"][-1])
     az = np.radians(series["azimuth"][s0:])[:, None] + 2 * np.pi * np.arange(nb)[None, :] / nb
+    per_step = bool(series.get("_pitch_per_step", False))
     kj = dict(ll=f(kin["bound"][:, :, s0:, :]), bxn=f(kin["bxn"][:, :, s0:, :]),
               byn=f(kin["byn"][:, :, s0:, :]), bzn=f(kin["bzn"][:, :, s0:, :]),
               vblade=f(kin["vblade"][:, :, s0:, :]), chord=st["chord"],
@@ -208,10 +209,13 @@ def cases(model: dict, series: dict, kin: dict, rc0=0.1, delta=100.0, nu=1.5e-5,
               foil_points=np.array([len(t["aoa"]) for t in tabs], dtype=np.int32),
               aoa=np.concatenate([t["aoa"] for t in tabs]), cl=np.concatenate([t["cl"] for t in tabs]),
               cd=np.concatenate([t["cd"] for t in tabs]), r_over_R=st["r_nodes"] / R,
-              chord_over_R=st["chord"] / R, twist=np.radians(st["twist"] + series["_pitch"]),
+              chord_over_R=st["chord"] / R,
+              twist=np.radians(st["twist"] + (0.0 if per_step else series["_pitch"])),
               azimuth=f(az), r_station=st["r_nodes"], dr_station=st["dr"],
               rpm=(np.asarray(series["rpm"][s0:s0 + nsteps + 1], np.float64) if "rpm" in series
                    else np.full(nsteps + 1, series["_omega"] * 30.0 / np.pi)), rho=RHO)
+    if per_step:  # blade pitch per step and blade for the loads (perform.m:22-33)
+        kj["pitch"] = f(np.asarray(series["pitch"], np.float64)[s0:s0 + nsteps + 1])
     return wake, kj
 
 

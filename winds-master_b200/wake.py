@@ -34,7 +34,7 @@ class KJCaseC(C.Structure):
                 ("cl", C.c_void_p), ("cd", C.c_void_p), ("r_over_R", C.c_void_p),
                 ("chord_over_R", C.c_void_p), ("twist", C.c_void_p), ("azimuth", C.c_void_p),
                 ("r_station", C.c_void_p), ("dr_station", C.c_void_p), ("rpm", C.c_void_p),
-                ("rho", C.c_double)]
+                ("rho", C.c_double), ("pitch", C.c_void_p)]
 
 
 class KJParamsC(C.Structure):
@@ -137,7 +137,8 @@ class WakeBatch:
                 setattr(a, f, x.ctypes.data)
             a.n_foils = len(j["foil_points"])
             # MLP and loads inputs, optional
-            for f in ("r_over_R", "chord_over_R", "twist", "azimuth", "r_station", "dr_station", "rpm"):
+            for f in ("r_over_R", "chord_over_R", "twist", "azimuth", "r_station", "dr_station", "rpm",
+                      "pitch"):
                 if f in j:
                     x = np.asfortranarray(j[f], dtype=np.float64)
                     self._keep.append(x)
