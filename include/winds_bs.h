@@ -128,7 +128,8 @@ int winds_bs_length_device(const double *F1, const double *F2, const long long d
 /* Wall-free timing hook for benchmarks: device time in ms of the last
  * winds_bs_eval_* call's main direct-sum kernel(s), measured with CUDA events
  * on the launch stream; also reports how many kernels that call launched and
- * how many near-singular pairs were recomputed in FP64 (if counted). */
+ * how many near-singular pairs its FP32c direct sum recomputed in FP64 (0 for
+ * the FP64 path). */
 int winds_bs_last_stats(double *main_ms, int *launches, long long *near_pairs);
 
 /* Synchronises `stream` (NULL: the library's stream) and reports a device-side
