@@ -493,11 +493,13 @@ def ours(args):
                "sample": f"{n} sampled targets x {nf} filaments ({dt:.1f} s), FP64 C restatement "
                          "of core/BiotSavart.m, OpenMP",
                "others": other_cpu_baselines(fams, P)}
+    # the sub-benchmarks run on one GPU only: under torchrun the other ranks
+    # would wait at the final barrier for minutes, past the group's timeout
     wake_line = None
-    if rank == 0 and args.wake_steps > 0 and not args.quick:
+    if rank == 0 and world == 1 and args.wake_steps > 0 and not args.quick:
         wake_line = wake_bench(args)
     mlp_line = e2e_line_run = None
-    if rank == 0 and not (args.quick or args.no_studies):
+    if rank == 0 and world == 1 and not (args.quick or args.no_studies):
         mlp_line = kj_mlp_bench()
         if args.e2e_steps > 0:
             e2e_line_run = e2e_run_bench(args.e2e_steps)
