@@ -62,6 +62,7 @@ struct winds_wake_batch {
   std::vector<KJCase> kjc;
   long long n_ll = 0, frames_n = 0, stations_n = 0;
   int max_st = 0;
+  long long max_bound_cols = 0;  // largest nb (2 ns + nst): the loop's repack
   DevBuf kjc_d, ll, bxn, byn, bzn, vblade, chord, foil, foil_off, aoa_t, cl_t, cd_t;
   DevBuf tp_ll, perm_ll, uindb, kj_groups, kj_tiles, kj_items, kj_order, kj_part;
   DevBuf conv, iters, res_max, res_last, active, diverged, cl_o, cd_o, aoa_o;
@@ -350,15 +351,16 @@ cudaError_t enqueue_kj_iter(winds_wake_batch *b, int &launches, cudaStream_t s,
   PackedFilaments pf{P<float4>(b->pk),
                      P<double4>(b->ra), P<double4>(b->rb)};
   BBox *bb = P<BBox>(b->bbox);
+  // Γ of the bound iterate; only its columns are repacked (enqueue_kj_begin
+  // packed every filament with the step's positions and cores)
   cudaError_t e = launch_wake_bookkeep(cd, b->ncases, b->max_cols, P<const double>(b->bound),
                                        P<const double>(b->trail_prev), P<double>(b->shed_cur),
                                        P<double>(b->trail_cur), s);
   if (e == cudaSuccess)
-    e = launch_wake_filaments(cd, b->ncases, b->max_fil, P<const int>(b->step_d), 0,
-                              P<const double>(b->dom), P<const double>(b->shed_cur),
-                              P<const double>(b->trail_cur), nullptr, nullptr, 0, 0, nullptr,
-                              nullptr, nullptr, nullptr, P<const double>(b->rc_s),
-                              P<const double>(b->rc_t), b->model, b->dcut, pf, bb, s);
+    e = launch_wake_filaments_bound_cols(cd, b->ncases, b->max_bound_cols, P<const double>(b->dom),
+                                         P<const double>(b->shed_cur), P<const double>(b->trail_cur),
+                                         P<const double>(b->rc_s), P<const double>(b->rc_t),
+                                         b->model, b->dcut, pf, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(b->ctr.p, 0, sizeof(unsigned), s);
   F32cArgs a;
   a.pk = pf.pk;
@@ -446,6 +448,21 @@ cudaError_t enqueue_kj_begin(winds_wake_batch *b) {
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(b->guess.p, b->bound.p, b->bound_n * sizeof(double),
                         cudaMemcpyDeviceToDevice, s);
+  // every filament at the step's positions with the step's cores held fixed
+  // (as kj() does), Γ from the start value; the iterations repack only the
+  // columns that follow the bound iterate
+  if (e == cudaSuccess)
+    e = launch_wake_bookkeep(cd, b->ncases, b->max_cols, P<const double>(b->bound),
+                             P<const double>(b->trail_prev), P<double>(b->shed_cur),
+                             P<double>(b->trail_cur), s);
+  if (e == cudaSuccess) {
+    PackedFilaments pf{P<float4>(b->pk), P<double4>(b->ra), P<double4>(b->rb)};
+    e = launch_wake_filaments(cd, b->ncases, b->max_fil, P<const int>(b->step_d), 0,
+                              P<const double>(b->dom), P<const double>(b->shed_cur),
+                              P<const double>(b->trail_cur), nullptr, nullptr, 0, 0, nullptr,
+                              nullptr, nullptr, nullptr, P<const double>(b->rc_s),
+                              P<const double>(b->rc_t), b->model, b->dcut, pf, P<BBox>(b->bbox), s);
+  }
   return e;
 }
 
@@ -956,6 +973,7 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
   std::vector<int> foil_off, foils;
   std::vector<double> aoa, cl, cd, chord;
   b->max_st = 0;
+  b->max_bound_cols = 0;
   for (int k = 0; k < b->ncases; ++k) {
     const WakeCase &c = b->cases[k];
     const winds_kj_case &h = kj[k];
@@ -1002,6 +1020,7 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
     tt += (long long)ns * c.nb;
     st += ns;
     b->max_st = std::max(b->max_st, ns * c.nb);
+    b->max_bound_cols = std::max<long long>(b->max_bound_cols, (long long)c.nb * (2 * ns + c.nst));
     b->kjc.push_back(q);
   }
   b->frames_n = fr, b->n_ll = tt, b->stations_n = st;

@@ -177,6 +177,52 @@ __global__ void wake_filaments(const WakeCase *cases, const int *step, int step_
   bbox_accumulate(lo, hi, bb->fmin, bb->fmax);
 }
 
+// Repacks only the filaments whose circulation follows the bound iterate of
+// the Kutta-Joukowski loop -- shed columns 0 and 1 and trailing column 0 (the
+// bookkeeping's other columns come from the previous step) -- with the step's
+// positions and held cores; the other records stay as the full pack before
+// the loop wrote them. Same arithmetic as wake_filaments, so the records are
+// identical to a full repack. Needs na >= 3 (checked at batch creation).
+__global__ void wake_filaments_bound_cols(const WakeCase *cases, const double *dom,
+                                          const double *shed, const double *trail,
+                                          const double *rc_in_s, const double *rc_in_t, int model,
+                                          double dcut, PackedFilaments pf) {
+  const WakeCase c = cases[blockIdx.y];
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ns = c.nst - 1;
+  const int n_shed = c.nb * 2 * ns;
+  if (t >= n_shed + c.nb * c.nst) return;
+  int i, j, b;
+  double x1, y1, z1, x2, y2, z2, g, rc;
+  long long f;
+  if (t < n_shed) {  // shed column j in {0, 1}: dom(i) -> dom(i+1)
+    b = t / (2 * ns);
+    const int r = t - b * 2 * ns;
+    j = r / ns;
+    i = r - j * ns;
+    f = i + (long long)ns * (j + (long long)c.na * b);
+    x1 = node_comp(dom, c, i, 0, j, b), y1 = node_comp(dom, c, i, 1, j, b);
+    z1 = node_comp(dom, c, i, 2, j, b);
+    x2 = node_comp(dom, c, i + 1, 0, j, b), y2 = node_comp(dom, c, i + 1, 1, j, b);
+    z2 = node_comp(dom, c, i + 1, 2, j, b);
+    g = shed[c.shed_off + f];
+    rc = rc_in_s[c.shed_off + f];
+  } else {  // trailing column 0: dom(:, 1) -> dom(:, 0)
+    const int u = t - n_shed;
+    b = u / c.nst;
+    i = u - b * c.nst;
+    const long long kk = i + (long long)c.nst * ((long long)(c.na - 1) * b);
+    f = (long long)ns * c.na * c.nb + kk;
+    x1 = node_comp(dom, c, i, 0, 1, b), y1 = node_comp(dom, c, i, 1, 1, b);
+    z1 = node_comp(dom, c, i, 2, 1, b);
+    x2 = node_comp(dom, c, i, 0, 0, b), y2 = node_comp(dom, c, i, 1, 0, b);
+    z2 = node_comp(dom, c, i, 2, 0, b);
+    g = trail[c.trail_off + kk];
+    rc = rc_in_t[c.trail_off + kk];
+  }
+  pack_filament(c.fil_off + f, x1, y1, z1, x2, y2, z2, g, rc, model, dcut, pf.pk, pf.ra, pf.rb);
+}
+
 __global__ void wake_targets(const WakeCase *cases, const double *dom, double4 *tp, int *tgroup,
                              BBox *bb) {
   const WakeCase c = cases[blockIdx.y];
@@ -304,6 +350,16 @@ cudaError_t launch_wake_bookkeep(const WakeCase *cases, int ncases, long long ma
                                  double *trail, cudaStream_t s) {
   wake_bookkeep<<<case_grid(max_cols, ncases, 128), 128, 0, s>>>(cases, bound, trail_prev, shed,
                                                                   trail);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wake_filaments_bound_cols(const WakeCase *cases, int ncases, long long per_case,
+                                             const double *dom, const double *shed,
+                                             const double *trail, const double *rc_in_s,
+                                             const double *rc_in_t, int model, double dcut,
+                                             const PackedFilaments &pf, cudaStream_t s) {
+  wake_filaments_bound_cols<<<case_grid(per_case, ncases, 128), 128, 0, s>>>(
+      cases, dom, shed, trail, rc_in_s, rc_in_t, model, dcut, pf);
   return cudaGetLastError();
 }
 

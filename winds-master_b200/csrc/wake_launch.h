@@ -18,6 +18,13 @@ enum WakeConvectMode : int {
 cudaError_t launch_wake_bookkeep(const WakeCase *cases, int ncases, long long max_cols,
                                  const double *bound, const double *trail_prev, double *shed,
                                  double *trail, cudaStream_t s);
+// The Kutta-Joukowski loop's repack: shed columns 0-1 and trailing column 0
+// only; per_case is the largest nb * (2 (nst - 1) + nst) of the batch.
+cudaError_t launch_wake_filaments_bound_cols(const WakeCase *cases, int ncases, long long per_case,
+                                             const double *dom, const double *shed,
+                                             const double *trail, const double *rc_in_s,
+                                             const double *rc_in_t, int model, double dcut,
+                                             const PackedFilaments &pf, cudaStream_t s);
 cudaError_t launch_wake_filaments(const WakeCase *cases, int ncases, long long max_fil_pad,
                                   const int *step, int step_add, const double *dom,
                                   const double *shed, const double *trail,
