@@ -134,3 +134,16 @@ def test_series_from_fastout_matches_kinematics(tmp_path):
     np.testing.assert_allclose(kj["pitch"][:, 1], ch["BldPitch2"][11:], rtol=1e-9, atol=1e-9)
     st = md.stations(m["r_trail"], m["chord_trail"], m["twist_trail"], m["nfoil_trail"])
     np.testing.assert_allclose(kj["twist"], np.radians(st["twist"]), rtol=1e-15)
+
+
+def test_fast_out_regrids_time_with_the_integration_step(tmp_path):
+    """output_import.m:44-46: for a non-Simulink run the time column is
+    rebuilt as t_first:dt:t_last from the .fst integration step."""
+    md = _md()
+    t = np.array([0.0, 0.0999, 0.2001, 0.3, 0.4])  # rounded times as a file may hold them
+    ch = {"Time": t, "Azimuth": 90.0 * t}
+    path = str(tmp_path / "run.out")
+    md.write_fast_out(path, ch)
+    fo = md.read_fast_out(path, dt=0.1)
+    np.testing.assert_allclose(fo["Time"], 0.1 * np.arange(5), rtol=0, atol=1e-12)
+    np.testing.assert_allclose(fo["Azimuth"], 90.0 * t, rtol=1e-9)
