@@ -276,7 +276,51 @@ def wake_bench(args, seed=2, ncases=64, plain=True):
             "launches_per_step": launches,
             "plain_fp64_steps_per_s": 1000.0 / plain_ms,
             "speedup_vs_plain_fp64": plain_ms / ms,
-            "nodes": int(sum(c["nst"] * c["na"] * c["nb"] for c in cases))}
+            "nodes": int(sum(c["nst"] * c["na"] * c["nb"] for c in cases)),
+            "lifting_line": wake_kj_bench(rcases, cases)}
+
+
+def wake_kj_bench(rcases, cases, tol=1e-6, relax=0.3, maxiter=200):
+    """The 64-case batch with the lifting line and rotor loads: every pcc step
+    runs the Kutta-Joukowski fixed point to the same tolerance on both paths.
+    Fast: FP32c, one CUDA graph per step (the iteration a conditional node).
+    Plain: each case alone, FP64, eager, the host waiting on the convergence
+    flag every iteration. One warm step, then one timed step each."""
+    synth = importlib.import_module("winds-master_b200.synth")
+    wake = importlib.import_module("winds-master_b200.wake")
+    kjs = [synth.make_kj_case(rc, nsteps=c["nsteps"], t0=c["t0"]) for rc, c in zip(rcases, cases)]
+    b = wake.WakeBatch(cases, integrator="pcc", precision="f32c")
+    b.set_kj(kjs, relax=relax, tol=tol, maxiter=maxiter)
+    b.step(1, graph=True)
+    b.step(1, graph=True)
+    ms = b.stats()[0]
+    it_f = b.kj_stats()[0].copy()
+    T_f = b.loads()[0].copy()
+    G_f = [b.bound(k) for k in range(len(cases))]
+    b.close()
+    plain_ms, it_p, T_p, G_p = 0.0, [], [], []
+    for c, kj in zip(cases, kjs):
+        p = wake.WakeBatch([c], integrator="pcc", precision="f64")
+        p.set_kj([kj], relax=relax, tol=tol, maxiter=maxiter)
+        p.step(1)
+        p.step(1)
+        plain_ms += p.stats()[0]
+        it_p.append(int(p.kj_stats()[0][0]))
+        T_p.append(float(p.loads()[0][0]))
+        G_p.append(p.bound(0))
+        p.close()
+    it_p = np.array(it_p)
+    both = (it_f < maxiter) & (it_p < maxiter)
+    dT = np.abs(T_f - np.array(T_p)) / np.abs(np.array(T_p))
+    dG = [float(np.abs(gf - gp).max() / np.abs(gp).max()) for gf, gp in zip(G_f, G_p)]
+    return {"tol": tol, "relax": relax, "maxiter": maxiter,
+            "steps_per_s": 1000.0 / ms, "ms_per_step": ms,
+            "plain_fp64_steps_per_s": 1000.0 / plain_ms, "speedup_vs_plain_fp64": plain_ms / ms,
+            "kj_iterations_fast": int(it_f.sum()), "kj_iterations_plain": int(it_p.sum()),
+            "converged_fast": float(np.mean(it_f < maxiter)),
+            "converged_plain": float(np.mean(it_p < maxiter)),
+            "thrust_rel_diff_max": float(dT[both].max()) if both.any() else None,
+            "bound_rel_diff_max": float(np.max(np.array(dG)[both])) if both.any() else None}
 
 
 # ------------------------------------------------------------------ start value
