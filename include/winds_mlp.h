@@ -61,6 +61,16 @@ int winds_mlp_set_params(winds_mlp *m, const float *theta);
 int winds_mlp_set_scaling(winds_mlp *m, const float *shift, const float *scale, float out_scale);
 int winds_mlp_get_scaling(winds_mlp *m, float *shift, float *scale, float *out_scale);
 
+/* What the wake engine adds the scaled output to when the network is its
+ * lifting-line start value: the previous step's converged bound circulation
+ * (the reference's start, WInDS.m:131; the default) or its linear
+ * extrapolation over the last two steps, Gamma_prev + (Gamma_prev - Gamma_prev2),
+ * so that the network learns the residual of the extrapolation. */
+#define WINDS_MLP_BASE_PREVIOUS 0
+#define WINDS_MLP_BASE_EXTRAPOLATED 1
+int winds_mlp_set_base(winds_mlp *m, int base);
+int winds_mlp_get_base(const winds_mlp *m);
+
 /* y[i] = network(x[i]) for host rows x [n][n_in]. Synchronous. */
 int winds_mlp_forward_host(winds_mlp *m, const float *x, long long n, float *y);
 

@@ -49,6 +49,42 @@ def test_features_and_start_value_match_host(wb):
     m.close()
 
 
+def test_extrapolated_base_start_value(wb):
+    """With the extrapolated base the start value is Gamma_prev + dGamma_prev
+    + out_scale * network(features), dGamma_prev the last step's change
+    (feature 9); with an output scale of zero it is the extrapolation alone."""
+    gi, mlp, wake, synth = _mods()
+    pts = gi.operating_points(3, seed=7, nst=13, wake_steps=10)
+    cases, kjs = gi.build(pts, 4)
+    b = wake.WakeBatch(cases, integrator="pcc")
+    b.set_kj(kjs, relax=0.3, tol=1e-6, maxiter=100)
+    m = mlp.Mlp(gi.N_FEATURES, seed=3)
+    m.set_scaling(np.zeros(10, np.float32), np.full(10, 0.2, np.float32), 0.05)
+    m.set_base("extrapolated")
+    assert m.base == "extrapolated"
+    b.step(1)
+    b.set_mlp(m)
+    for _ in range(2):
+        prev = [b.bound(k) for k in range(3)]
+        b.step(1, graph=True)
+        for k in range(3):
+            x = b.kj_features(k)
+            gh = ((prev[k].ravel(order="F") + x[:, 9].astype(np.float64))
+                  + float(np.float32(0.05)) * m.forward(x).astype(np.float64))
+            np.testing.assert_allclose(b.kj_guess(k).ravel(order="F"), gh, rtol=1e-12, atol=1e-9)
+    xo = gi.extrapolation_only()
+    b.set_mlp(xo)
+    prev = [b.bound(k) for k in range(3)]
+    b.step(1)
+    for k in range(3):
+        x = b.kj_features(k)
+        np.testing.assert_array_equal(b.kj_guess(k).ravel(order="F"),
+                                      prev[k].ravel(order="F") + x[:, 9].astype(np.float64))
+    b.close()
+    m.close()
+    xo.close()
+
+
 def test_graph_with_network_matches_host_loop(wb):
     """With the network attached, the captured step (network forward inside
     the graph, iteration as a conditional node) gives the host loop's results

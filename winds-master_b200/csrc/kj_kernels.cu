@@ -125,15 +125,20 @@ __global__ void kj_features(const WakeCase *cases, const KJCase *kc, const int *
   f[9] = (float)(bound[q] - bound_last[q]);
 }
 
+// bound = base + out_scale * y, base Gamma_prev or, with *base != 0, its
+// extrapolation Gamma_prev + dGamma_prev (feature 9 of the row).
 __global__ void kj_apply_guess(const WakeCase *cases, const KJCase *kc, const float *y,
-                               const float *out_scale, double *bound) {
+                               const float *out_scale, const float *feat, const float *base,
+                               double *bound) {
   const WakeCase c = cases[blockIdx.y];
   const KJCase k = kc[blockIdx.y];
   const int ns = c.nst - 1;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ns * c.nb) return;
   const int i = t % ns, b = t / ns;
-  bound[c.bound_off + i + (long long)ns * b] += (double)*out_scale * (double)y[k.t_off + t];
+  double g = bound[c.bound_off + i + (long long)ns * b];
+  if (*base != 0.f) g += (double)feat[(k.t_off + t) * kKJFeatures + 9];
+  bound[c.bound_off + i + (long long)ns * b] = g + (double)*out_scale * (double)y[k.t_off + t];
 }
 
 // Spanwise loads of one station (postproc/perform.m:20-55): the blade-frame
@@ -284,8 +289,10 @@ cudaError_t launch_kj_features(const WakeCase *cases, const KJCase *kc, int ncas
 }
 
 cudaError_t launch_kj_apply_guess(const WakeCase *cases, const KJCase *kc, int ncases, int max_st,
-                                  const float *y, const float *out_scale, double *bound, cudaStream_t s) {
-  kj_apply_guess<<<dim3((max_st + 127) / 128, ncases), 128, 0, s>>>(cases, kc, y, out_scale, bound);
+                                  const float *y, const float *out_scale, const float *feat,
+                                  const float *base, double *bound, cudaStream_t s) {
+  kj_apply_guess<<<dim3((max_st + 127) / 128, ncases), 128, 0, s>>>(cases, kc, y, out_scale, feat,
+                                                                    base, bound);
   return cudaGetLastError();
 }
 

@@ -27,6 +27,7 @@ struct winds_mlp {
   winds::DevBuf theta, theta_bf, grad, mom, vel, shift, scale, err, jobs, loss, lossbuf, idx;
   winds::DevBuf Xall, Tall, xall_raw;
   float out_scale = 1.f;
+  int base = 0;  // start value the output is added to (winds_mlp_set_base)
   float h_shift[16], h_scale[16];
   long long adam_t = 0;
   winds::MlpWork w;
@@ -245,8 +246,10 @@ int mlp_forward(const winds_mlp *m, const __nv_bfloat16 *X, long long n, MlpWork
 const float *mlp_shift_dev(const winds_mlp *m) { return static_cast<const float *>(m->shift.p); }
 const float *mlp_scale_dev(const winds_mlp *m) { return static_cast<const float *>(m->scale.p); }
 float mlp_out_scale(const winds_mlp *m) { return m->out_scale; }
-// out_scale on the device (after the 16 input scales), read when a captured step replays
+// out_scale and the base flag on the device (after the 16 input scales), read
+// when a captured step replays
 const float *mlp_out_scale_dev(const winds_mlp *m) { return static_cast<const float *>(m->scale.p) + 16; }
+const float *mlp_base_dev(const winds_mlp *m) { return static_cast<const float *>(m->scale.p) + 17; }
 int mlp_n_in(const winds_mlp *m) { return m->n_in; }
 int mlp_device(const winds_mlp *m) { return m->dev; }
 unsigned *mlp_err_word(const winds_mlp *m) { return static_cast<unsigned *>(m->err.p); }
@@ -300,6 +303,7 @@ int winds_mlp_create(const winds_mlp_config *cfg, winds_mlp **out) {
   if (e == cudaSuccess) e = cudaMemcpy(m->scale.p, m->h_scale, 64, cudaMemcpyHostToDevice);
   if (e == cudaSuccess)
     e = cudaMemcpy(P<float>(m->scale) + 16, &m->out_scale, 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(P<float>(m->scale) + 17, 0, 4);  // base 0
   if (e == cudaSuccess) e = cudaMemset(m->mom.p, 0, kNParam * 4);
   if (e == cudaSuccess) e = cudaMemset(m->vel.p, 0, kNParam * 4);
   if (e == cudaSuccess) e = cudaMemset(m->err.p, 0, 16);
@@ -355,6 +359,20 @@ int winds_mlp_set_scaling(winds_mlp *m, const float *shift, const float *scale, 
   if (e == cudaSuccess) e = cudaMemcpy(P<float>(m->scale) + 16, &out_scale, 4, cudaMemcpyHostToDevice);
   return e == cudaSuccess ? WINDS_BS_OK : cuda_fail(e, "mlp scaling");
 }
+
+int winds_mlp_set_base(winds_mlp *m, int base) {
+  if (!m || (base != WINDS_MLP_BASE_PREVIOUS && base != WINDS_MLP_BASE_EXTRAPOLATED))
+    return fail(WINDS_BS_ERR_ARG, "bad start-value base %d", base);
+  cudaSetDevice(m->dev);
+  cudaStreamSynchronize(m->stream);
+  const float f = (float)base;
+  cudaError_t e = cudaMemcpy(P<float>(m->scale) + 17, &f, 4, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(e, "mlp base");
+  m->base = base;
+  return WINDS_BS_OK;
+}
+
+int winds_mlp_get_base(const winds_mlp *m) { return m ? m->base : -1; }
 
 int winds_mlp_get_scaling(winds_mlp *m, float *shift, float *scale, float *out_scale) {
   if (!m) return fail(WINDS_BS_ERR_ARG, "null model");

@@ -30,6 +30,7 @@ const float *mlp_shift_dev(const winds_mlp *m);
 const float *mlp_scale_dev(const winds_mlp *m);
 float mlp_out_scale(const winds_mlp *m);
 const float *mlp_out_scale_dev(const winds_mlp *m);
+const float *mlp_base_dev(const winds_mlp *m);
 int mlp_n_in(const winds_mlp *m);
 int mlp_device(const winds_mlp *m);
 unsigned *mlp_err_word(const winds_mlp *m);

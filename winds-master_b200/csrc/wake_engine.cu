@@ -443,7 +443,8 @@ cudaError_t enqueue_kj_begin(winds_wake_batch *b) {
       e = cudaErrorLaunchFailure;
     if (e == cudaSuccess)
       e = launch_kj_apply_guess(cd, kd, b->ncases, b->max_st, P<const float>(b->mw.y),
-                                mlp_out_scale_dev(b->mlp), P<double>(b->bound), s);
+                                mlp_out_scale_dev(b->mlp), P<const float>(b->feat),
+                                mlp_base_dev(b->mlp), P<double>(b->bound), s);
   }
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(b->guess.p, b->bound.p, b->bound_n * sizeof(double),

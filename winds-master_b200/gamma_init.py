@@ -5,7 +5,10 @@ point of ``core/KuttaJoukowski.m:42-49``, started from the previous step's
 bound circulation as ``WInDS.m:131`` does) generates pairs (station state,
 converged bound circulation); the MLP of ``winds_mlp.h`` learns the change
 ``Gamma_conv - Gamma_prev`` from the state and then starts each step's
-iteration at ``Gamma_prev + out_scale * network(state)``. The iteration still
+iteration at ``Gamma_prev + out_scale * network(state)``; with the
+extrapolated base (the default of ``study``) it learns the residual of the
+linear extrapolation instead and starts at ``Gamma_prev + dGamma_prev +
+out_scale * network(state)``. The iteration still
 runs to the same tolerance, so converged results are unchanged and only
 iterations (each one two Biot-Savart calls in the reference: shed and
 trailing filaments onto the lifting line) are saved.
@@ -129,45 +132,97 @@ def attached(points, run_steps=12, stall_deg=12.0, **kw):
     return [p for p, a in zip(points, r["aoa_max"]) if a < stall_deg]
 
 
-def train(X, dG, epochs=30, batch=4096, lr=2e-3, seed=0, weight_decay=0.0):
-    """An MLP fitted to dG (the change of the converged bound circulation)
-    from the features X, with standardised inputs and target; Adam with the
-    learning rate stepped down (x1, x1/4, x1/16) over three equal phases."""
+def train(X, dG, epochs=30, batch=4096, lr=2e-3, seed=0, weight_decay=0.0, base="previous"):
+    """An MLP fitted to dG (the change of the converged bound circulation
+    over the previous step's) from the features X, with standardised inputs
+    and target; Adam with the learning rate stepped down (x1, x1/4, x1/16)
+    over three equal phases. ``base="extrapolated"``: the network learns the
+    residual dG - dGamma_prev of the linear extrapolation (feature 9) and the
+    wake engine adds its output to that extrapolation."""
+    target = dG - X[:, 9] if base == "extrapolated" else dG
     shift = X.mean(0)
     sd = X.std(0)
     scale = np.where(sd > 0, 1.0 / np.maximum(sd, 1e-12), 1.0).astype(np.float32)
-    out_scale = float(max(dG.std(), 1e-12))
+    out_scale = float(max(target.std(), 1e-12))
     m = Mlp(N_FEATURES, seed=seed)
     m.set_scaling(shift.astype(np.float32), scale, out_scale)
+    m.set_base(base)
     losses = []
     per = [epochs - 2 * (epochs // 3), epochs // 3, epochs // 3]
     for k, (ep, f) in enumerate(zip(per, (1.0, 0.25, 0.0625))):
         if ep > 0:
-            losses.append(m.train(X, dG / out_scale, epochs=ep, batch=batch, lr=lr * f,
+            losses.append(m.train(X, target / out_scale, epochs=ep, batch=batch, lr=lr * f,
                                   seed=seed + 1 + k, weight_decay=weight_decay))
+    m.shrink, m.full_out_scale = 1.0, out_scale
     return m, np.concatenate(losses) if losses else np.zeros(0)
+
+
+def choose_shrink(m, points, run_steps, skip=4, alphas=(0.0, 0.25, 0.5, 0.75, 1.0), **kw):
+    """Scales the network's output by the alpha of ``alphas`` whose start
+    value needs the fewest iterations (steps >= ``skip``, (step, case) pairs
+    converged under every alpha) when the solver actually runs on
+    ``points`` -- validation points kept out of the training pairs. The
+    stopping rule sees the largest spanwise residual, and how fast the fixed
+    point damps a start error depends on its spanwise shape, so no error
+    norm of the start value predicts this as well as the iteration itself.
+    alpha = 0 leaves the base alone. Sets and returns ``m.shrink``."""
+    shift, scale, _ = m.scaling()
+    full = m.full_out_scale
+    maxiter = kw.get("maxiter", 200)
+    its = []
+    for a in alphas:
+        m.set_scaling(shift, scale, full * a)
+        its.append(run(points, run_steps, mlp=m, **kw)["iters"])
+    ok = np.ones_like(its[0], dtype=bool)
+    for it in its:
+        ok &= it < maxiter
+    ok[:skip] = False
+    tot = [int(it[ok].sum()) for it in its]
+    best = int(np.argmin(tot))
+    m.shrink = float(alphas[best])
+    m.set_scaling(shift, scale, full * m.shrink)
+    return m.shrink
+
+
+def extrapolation_only():
+    """A start value with no learned part: the linear extrapolation
+    Gamma_prev + dGamma_prev (an output scale of zero on the extrapolated base)."""
+    m = Mlp(N_FEATURES, seed=0)
+    m.set_scaling(np.zeros(N_FEATURES, np.float32), np.ones(N_FEATURES, np.float32), 0.0)
+    m.set_base("extrapolated")
+    return m
 
 
 def study(n_train: int = 400, n_test: int = 120, train_steps: int = 42, test_steps: int = 30,
           skip: int = 4, epochs: int = 60, relax: float = 0.3, tol: float = 1e-6,
-          maxiter: int = 200, seed: int = 1, precision: str = "f32c"):
+          maxiter: int = 200, seed: int = 1, precision: str = "f32c", base: str = "extrapolated"):
     """Trains the start value on the attached-flow points among ``n_train``
     seeded candidates (pairs from steps >= ``skip``, past the start-up
     transient of the synthetic initial circulation) and compares the
     iteration with and without it on the attached points among ``n_test``
-    other candidates. Returns a dict of the measurements."""
+    other candidates; also the extrapolation alone (no network), so the
+    network's own share shows. Returns a dict of the measurements."""
     t0 = time.perf_counter()
     kw = dict(relax=relax, tol=tol, maxiter=maxiter, precision=precision)
     train_pts = attached(operating_points(n_train, seed=seed), **kw)
     d = run(train_pts, train_steps, record=True, **kw)
     keep = d["step_case"][:, 0] >= skip
     t1 = time.perf_counter()
-    m, losses = train(d["X"][keep], d["dG"][keep], epochs=epochs, seed=seed)
+    # pairs from most points; the rest validate the network's output scale
+    n_val = max(1, len(train_pts) // 5)
+    fit_rows = keep & (d["step_case"][:, 1] < len(train_pts) - n_val)
+    m, losses = train(d["X"][fit_rows], d["dG"][fit_rows], epochs=epochs, seed=seed, base=base)
+    choose_shrink(m, train_pts[-n_val:], test_steps, skip=skip, **kw)
     t2 = time.perf_counter()
     test_pts = attached(operating_points(n_test, seed=seed + 1), **kw)
     a = run(test_pts, test_steps, **kw)
     b = run(test_pts, test_steps, mlp=m, **kw)
-    ia, ib = a["iters"], b["iters"]
+    xo = extrapolation_only()
+    e = run(test_pts, test_steps, mlp=xo, **kw)
+    xo.close()
+    ia, ib, ie = a["iters"], b["iters"], e["iters"]
+    all3 = (ia < maxiter) & (ib < maxiter) & (ie < maxiter)
+    all3[:skip] = False
     # iterations are compared over (step, case) that converged in both runs;
     # the converged circulation over cases that converged at every step
     both = (ia < maxiter) & (ib < maxiter)
@@ -187,6 +242,9 @@ def study(n_train: int = 400, n_test: int = 120, train_steps: int = 42, test_ste
         converged_plain=float((ia < maxiter).mean()), converged_mlp=float((ib < maxiter).mean()),
         saved=1.0 - ib[both].sum() / max(ia[both].sum(), 1),
         saved_steady=1.0 - ib[steady].sum() / max(ia[steady].sum(), 1),
+        base=base, output_shrink=m.shrink, iters_extrap_steady=int(ie[all3].sum()),
+        saved_extrap_steady=1.0 - ie[all3].sum() / max(ia[all3].sum(), 1),
+        saved_vs_extrap_steady=1.0 - ib[all3].sum() / max(ie[all3].sum(), 1),
         cases_improved=int((np.where(both, ib, 0).sum(0) < np.where(both, ia, 0).sum(0)).sum()),
         cases_compared=int(ok_case.sum()),
         bound_rel_diff_max=max(rel) if rel else 0.0,

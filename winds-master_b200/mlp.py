@@ -30,6 +30,8 @@ def _bind():
         L.winds_mlp_set_params.argtypes = [C.c_void_p, C.c_void_p]
         L.winds_mlp_set_scaling.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_float]
         L.winds_mlp_get_scaling.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_float)]
+        L.winds_mlp_set_base.argtypes = [C.c_void_p, C.c_int]
+        L.winds_mlp_get_base.argtypes = [C.c_void_p]
         L.winds_mlp_forward_host.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong, C.c_void_p]
         L.winds_mlp_loss_grad_host.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong,
                                                C.POINTER(C.c_double), C.c_void_p]
@@ -76,6 +78,19 @@ class Mlp:
     def set_scaling(self, shift, scale, out_scale=1.0):
         sh, sc = _f32(shift), _f32(scale)
         _check(_bind().winds_mlp_set_scaling(self.h, sh.ctypes.data, sc.ctypes.data, float(out_scale)))
+
+    BASES = {"previous": 0, "extrapolated": 1}
+
+    def set_base(self, base="previous"):
+        """What the wake engine adds the scaled output to: the previous step's
+        converged bound circulation, or its linear extrapolation over the last
+        two steps (``"extrapolated"``: the network then learns the residual)."""
+        _check(_bind().winds_mlp_set_base(self.h, self.BASES[base]))
+
+    @property
+    def base(self) -> str:
+        k = int(_bind().winds_mlp_get_base(self.h))
+        return {v: n for n, v in self.BASES.items()}[k]
 
     def scaling(self):
         sh = np.zeros(self.n_in, np.float32)
