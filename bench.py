@@ -366,7 +366,7 @@ def e2e_run_bench(steps, ncases=16, ages=1440, seed=5):
     m, _ = gi.train(tr["X"][keep], tr["dG"][keep], epochs=40, base="previous")
     # output scale from solver runs on validation points of the same conditions
     gi.choose_shrink(m, points(120, rng.uniform(0.0, 30.0, 8), 950), 16, maxiter=200)
-    mlp_base, mlp_shrink = m.base, m.shrink
+    mlp_base, mlp_shrink, mlp_val = m.base, m.shrink, m.validation
     train_s = time.perf_counter() - t0
     pts = points(ages, yaws, 100)
     cases, kjs = gi.build(pts, steps + 1)
@@ -402,6 +402,7 @@ def e2e_run_bench(steps, ncases=16, ages=1440, seed=5):
             "thrust_history_N": f["T"].sum(1).round(1).tolist(),
             "power_history_W": f["P"].sum(1).round(1).tolist(),
             "mlp_training_s": round(train_s, 2), "mlp_base": mlp_base, "mlp_output_shrink": mlp_shrink,
+            "mlp_validation": mlp_val,
             "timing": "CUDA events around each step "
             "(fast path: the lifting-line loop runs inside the step's graph; plain path: the "
             "host waits on a per-iteration convergence flag)"}
