@@ -38,6 +38,7 @@ struct winds_wake_batch {
   std::vector<WakeCase> cases;
   long long nodes = 0, shed_n = 0, trail_n = 0, bound_n = 0, fil_pad = 0, kin_n = 0, wind_n = 0;
   long long max_nodes = 0, max_cols = 0, max_fil = 0, max_slots = 0;
+  int max_nb = 0;  // most blades of a case
   long long interactions = 0;
   int launches = 0;
   // state and work buffers
@@ -351,11 +352,12 @@ cudaError_t enqueue_kj_iter(winds_wake_batch *b, int &launches, cudaStream_t s,
   PackedFilaments pf{P<float4>(b->pk),
                      P<double4>(b->ra), P<double4>(b->rb)};
   BBox *bb = P<BBox>(b->bbox);
-  // Γ of the bound iterate; only its columns are repacked (enqueue_kj_begin
-  // packed every filament with the step's positions and cores)
-  cudaError_t e = launch_wake_bookkeep(cd, b->ncases, b->max_cols, P<const double>(b->bound),
+  // Γ of the bound iterate: columns 0-1 follow it (the others come from the
+  // previous step); only those are recomputed and repacked (enqueue_kj_begin
+  // did every column and every filament with the step's positions and cores)
+  cudaError_t e = launch_wake_bookkeep(cd, b->ncases, 2LL * b->max_nb, P<const double>(b->bound),
                                        P<const double>(b->trail_prev), P<double>(b->shed_cur),
-                                       P<double>(b->trail_cur), s);
+                                       P<double>(b->trail_cur), s, 2);
   if (e == cudaSuccess)
     e = launch_wake_filaments_bound_cols(cd, b->ncases, b->max_bound_cols, P<const double>(b->dom),
                                          P<const double>(b->shed_cur), P<const double>(b->trail_cur),
@@ -647,6 +649,7 @@ int winds_wake_create(const winds_wake_case *cases, int ncases, const winds_wake
     wnd += 3LL * h.nsteps;
     b->max_nodes = std::max(b->max_nodes, nn);
     b->max_cols = std::max<long long>(b->max_cols, (long long)h.na * h.nb);
+    b->max_nb = std::max(b->max_nb, h.nb);
     b->max_fil = std::max(b->max_fil, c.fil_pad);
     b->max_slots = std::max(b->max_slots, nn);
     b->interactions += nn * c.fil_count;

@@ -60,12 +60,15 @@ __device__ __forceinline__ double trail_col(const WakeCase &c, const double *bou
 
 // One thread per (column j, blade b); the span loops are unrolled so a
 // thread keeps several loads in flight (the data is small; latency bounds this).
+// cols > 0: only columns j < cols (the Kutta-Joukowski loop's bound-dependent
+// columns); the same arithmetic per column as the full pass.
 __global__ void wake_bookkeep(const WakeCase *cases, const double *bound, const double *trail_prev,
-                              double *shed, double *trail) {
+                              double *shed, double *trail, int cols) {
   const WakeCase c = cases[blockIdx.y];
   const int u = blockIdx.x * blockDim.x + threadIdx.x;  // (column j, blade b)
-  if (u >= c.na * c.nb) return;
-  const int j = u % c.na, b = u / c.na;
+  const int nc = cols > 0 && cols < c.na ? cols : c.na;
+  if (u >= nc * c.nb) return;
+  const int j = u % nc, b = u / nc;
   const int ns = c.nst - 1, m = c.na - 1;  // m trailing columns
   if (j < m) {
 #pragma unroll 8
@@ -347,9 +350,9 @@ static dim3 case_grid(long long max_per_case, int ncases, int bs) {
 
 cudaError_t launch_wake_bookkeep(const WakeCase *cases, int ncases, long long max_cols,
                                  const double *bound, const double *trail_prev, double *shed,
-                                 double *trail, cudaStream_t s) {
+                                 double *trail, cudaStream_t s, int cols) {
   wake_bookkeep<<<case_grid(max_cols, ncases, 128), 128, 0, s>>>(cases, bound, trail_prev, shed,
-                                                                  trail);
+                                                                  trail, cols);
   return cudaGetLastError();
 }
 

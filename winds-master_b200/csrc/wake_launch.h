@@ -15,9 +15,10 @@ enum WakeConvectMode : int {
   kConvectCorrector = 3,  // numerical/pcc.m:74-75
 };
 
+// cols > 0: columns j < cols only (max_cols then nb * cols at most).
 cudaError_t launch_wake_bookkeep(const WakeCase *cases, int ncases, long long max_cols,
                                  const double *bound, const double *trail_prev, double *shed,
-                                 double *trail, cudaStream_t s);
+                                 double *trail, cudaStream_t s, int cols = 0);
 // The Kutta-Joukowski loop's repack: shed columns 0-1 and trailing column 0
 // only; per_case is the largest nb * (2 (nst - 1) + nst) of the batch.
 cudaError_t launch_wake_filaments_bound_cols(const WakeCase *cases, int ncases, long long per_case,
