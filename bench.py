@@ -298,6 +298,14 @@ def wake_kj_bench(rcases, cases, tol=1e-6, relax=0.3, maxiter=200):
     T_f = b.loads()[0].copy()
     G_f = [b.bound(k) for k in range(len(cases))]
     b.close()
+    # the same FP32c batch with the host driving the iteration (a 4-byte
+    # convergence flag read back after every iteration, no graphs)
+    h = wake.WakeBatch(cases, integrator="pcc", precision="f32c")
+    h.set_kj(kjs, relax=relax, tol=tol, maxiter=maxiter)
+    h.step(1)
+    h.step(1)
+    ms_host = h.stats()[0]
+    h.close()
     plain_ms, it_p, T_p, G_p = 0.0, [], [], []
     for c, kj in zip(cases, kjs):
         p = wake.WakeBatch([c], integrator="pcc", precision="f64")
@@ -315,6 +323,7 @@ def wake_kj_bench(rcases, cases, tol=1e-6, relax=0.3, maxiter=200):
     dG = [float(np.abs(gf - gp).max() / np.abs(gp).max()) for gf, gp in zip(G_f, G_p)]
     return {"tol": tol, "relax": relax, "maxiter": maxiter,
             "steps_per_s": 1000.0 / ms, "ms_per_step": ms,
+            "host_loop_steps_per_s": 1000.0 / ms_host,
             "plain_fp64_steps_per_s": 1000.0 / plain_ms, "speedup_vs_plain_fp64": plain_ms / ms,
             "kj_iterations_fast": int(it_f.sum()), "kj_iterations_plain": int(it_p.sum()),
             "converged_fast": float(np.mean(it_f < maxiter)),
