@@ -32,7 +32,11 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
-FLOP_PER_INTERACTION = 52  # Vatistas n=2 kernel, FMA = 2
+# FLOP per target-filament interaction of the Vatistas n=2 kernel, FMA = 2:
+# r1, r2 (6), |r1|^2, |r2|^2 (10), r1.r2 (5), r1 x r2 (9), |r1||r2| and the
+# denominator (3), numerator (2), L.r1 and h^2 (8), the Vatistas factor (3),
+# scale (1), accumulate (6); rsqrt/rcp are counted apart (3 per interaction)
+FLOP_PER_INTERACTION = 52
 METRIC = "biot_savart_gint_per_s"
 UNIT = "Gint/s"
 

@@ -105,14 +105,19 @@ int winds_bs_eval_host(const winds_bs_family *fams, int nfam, const double *P,
  * synchronising the device, stalls a solver that calls the engine every step.
  * All scratch lives in one static __device__ array of
  * WINDS_BS_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds
- * until exit. Inputs, outputs and semantics are those of
- * winds_bs_eval_device (device pointers; stream NULL = the default stream).
- * Limits: at most WINDS_BS_NOALLOC_MAX_FILAMENTS filaments and
- * WINDS_BS_NOALLOC_MAX_TARGETS targets per call (WINDS_BS_ERR_ARG beyond).
- * The call waits for its stream and reports device-side errors. Its first
- * call on a device looks up the array's device address: make that call
- * before any stream capture. Calls share the array: calls that overlap on the
- * GPU race. */
+ * until exit. Inputs and outputs are those of winds_bs_eval_device (device
+ * pointers), with two differences: the work runs on the calling thread's
+ * current CUDA device (winds_bs_eval_device uses the device chosen by
+ * winds_bs_set_device, which also makes it current on that thread), and a
+ * NULL stream is the legacy default stream (winds_bs_eval_device: the
+ * library's own stream). Limits: at most WINDS_BS_NOALLOC_MAX_FILAMENTS
+ * filaments and WINDS_BS_NOALLOC_MAX_TARGETS targets per call
+ * (WINDS_BS_ERR_ARG beyond). The call waits for its stream and reports
+ * device-side errors. Every call looks up the array's device address (a
+ * host-side lookup); the first call on a device also loads the library's
+ * device code, which commits the array's memory: make that first call before
+ * any stream capture. Calls share the array: calls that overlap on the GPU
+ * race. */
 #define WINDS_BS_NOALLOC_SCRATCH_BYTES (64ull << 20)
 #define WINDS_BS_NOALLOC_MAX_FILAMENTS 131072
 #define WINDS_BS_NOALLOC_MAX_TARGETS 65536

@@ -13,13 +13,29 @@
  *                          numerical/pcc.m:55-71 (two more for the corrector)
  *   convection             numerical/fe.m:31, ab2.m:38-39, ab4.m:77-81, pcc.m:37-75
  *
- * Differences from the reference loop, all deliberate:
- *   * each case's wake keeps `na` age columns: the oldest column is dropped
- *     every step (the reference grows the wake by one column per step);
- *   * the integrators start in their full form when history exists (the
- *     reference switches on fixed step indices: ab2.m:35, ab4.m:74, pcc.m:40);
- *   * filament stretching compares new and previous lengths by column index
- *     as filamentmod.m does, whenever a previous step exists.
+ * Wake length. Each case holds `na` age columns of capacity. The wake starts
+ * with `na_start` live columns and gains one per step, as the reference's
+ * wake.domain{p} of p+1 columns does (core/initials.m:44-51,84-87, WInDS.m:127);
+ * once it reaches `na` the oldest column is dropped every step (a truncated
+ * wake). na_start = 2 starts from core/initials.m's wake.domain{1} (quarter
+ * chord and trailing edge); na_start = na (or 0) keeps a truncated wake of na
+ * columns from the first step. The live column count is kept on the device, so
+ * one captured step graph stays valid while the wake grows.
+ *
+ * Start-up (winds_wake_params.startup). WINDS_STARTUP_REFERENCE follows the
+ * reference's switches on the time index p = s + 1 of step s: step 0 is the
+ * step of core/initials.m:138-152 (forward Euler, no Kutta-Joukowski
+ * iteration); ab2 runs in full form from p = 2 (ab2.m:35), ab4 from p = 4
+ * (ab4.m:35), the pcc corrector from p = 3 (pcc.m:40, `time>2`, before that
+ * the predictor stands), filament stretching from time index 4
+ * (filamentmod.m:26, `time>3`, for the corrector's evaluation of p+1 too),
+ * and the corrector's induced velocity is added again at the next step
+ * (pcc.m:71 then WInDS.m:168) only after a corrector step.
+ * WINDS_STARTUP_FULL runs every part in its full form as soon as its history
+ * exists (ab2 and ab4 as above, the corrector and stretching from step 0, the
+ * iteration at every step): the form for a truncated wake that starts with a
+ * history. Filament stretching compares new and previous lengths by column
+ * index as filamentmod.m does.
  * Arrays use WInDS's MATLAB layout [span, xyz, age, blade], column-major.
  */
 #ifndef WINDS_WAKE_H
@@ -36,13 +52,16 @@ extern "C" {
 #define WINDS_INTEG_AB4 2
 #define WINDS_INTEG_PCC 3
 
+#define WINDS_STARTUP_FULL 0
+#define WINDS_STARTUP_REFERENCE 1
+
 typedef struct winds_wake_batch winds_wake_batch;
 
 /* One rotor case. Host arrays are copied at creation. */
 typedef struct {
   int nst;            /* span nodes (trailing filaments per age column); ns = nst-1 stations */
   int nb;             /* blades */
-  int na;             /* age columns kept in the wake */
+  int na;             /* age columns of capacity (the most the wake keeps) */
   int nsteps;         /* time steps of kinematics and wind provided */
   double dt;          /* time step (1/user.t(3)) */
   double t0;          /* time of step 0 */
@@ -54,9 +73,16 @@ typedef struct {
   int core_mode;      /* 0: vcore.m, rc^2 = r0^2 + 4 alpha nu (1+a1 Re) t (absolute time)
                          1: age form rc^2 = rc0^2 + 4 alpha delta nu (1+a1 Re) age       */
   double r0, rc0, alpha, nu, a1, delta;
-  const double *dom;         /* [nst,3,na,nb] initial node positions (wake.domain)      */
+  const double *dom;         /* [nst,3,na,nb] initial node positions (wake.domain); only
+                                the first na_start columns are read                    */
   const double *bound;       /* [nst-1,nb] bound circulation (shed column 1)            */
   const double *trail_gamma; /* [nst,na-1,nb] trailing circulation (wake.gamma.trail)   */
+  int na_start;              /* live age columns at step 0: 2..na (0: na)                */
+  const double *time;        /* [nsteps] absolute time of each step (fastout.Time), the
+                                t of core_mode 0; NULL: t0 + step * dt                  */
+  const double *r0_step;     /* [nsteps] initial core radius of each step (wake.r0(time),
+                                core/initials.m:134-135, read by core/vcore.m:34);
+                                NULL: the scalar r0                                     */
 } winds_wake_case;
 
 typedef struct {
@@ -68,6 +94,7 @@ typedef struct {
   int pcc_double_add;  /* 1: the corrector's induced velocity is also added to the next
                           step's velocity (numerical/pcc.m:71 then WInDS.m:168) */
   int stretch;         /* 1: filament stretching (user.roll = 'true') */
+  int startup;         /* WINDS_STARTUP_* (see the top of this file) */
 } winds_wake_params;
 
 /* Creates the batch on the current device and uploads every case. */
@@ -78,14 +105,22 @@ int winds_wake_create(const winds_wake_case *cases, int ncases, const winds_wake
  * CUDA graph on the first call and replay it. Synchronous. */
 int winds_wake_step(winds_wake_batch *b, int nsteps, int use_graph);
 
-/* Copies one case's state to host arrays (any pointer may be NULL):
- * dom [nst,3,na,nb], bound [ns,nb], shed [ns,na,nb], trail [nst,na-1,nb],
- * rc_shed / rc_trail (effective squared cores of the last evaluation, same
- * shapes), uind [nst,3,na,nb] (induced velocity of the last step's first
- * evaluation). */
+/* Copies one case's state to host arrays (any pointer may be NULL), in the
+ * capacity's shapes: dom [nst,3,na,nb], bound [ns,nb], shed [ns,na,nb], trail
+ * [nst,na-1,nb], rc_shed / rc_trail (effective squared cores of the last
+ * evaluation, same shapes), uind [nst,3,na,nb] (induced velocity of the last
+ * step's first evaluation). After k steps, dom holds the positions of step k
+ * in its first live_cols(k) columns and the other arrays those of step k-1 in
+ * their first live_cols(k-1) (shed, uind) or live_cols(k-1) - 1 (trail)
+ * columns, live_cols(s) = min(na_start + s, na); winds_wake_get_live gives
+ * the count. */
 int winds_wake_get_state(winds_wake_batch *b, int icase, double *dom, double *bound,
                          double *shed, double *trail, double *rc_shed, double *rc_trail,
                          double *uind);
+
+/* Live age columns of one case's wake at the current step (the columns of
+ * the positions winds_wake_get_state returns) and the steps run so far. */
+int winds_wake_get_live(winds_wake_batch *b, int icase, int *na_live, long long *steps_done);
 
 /* Replaces one case's bound circulation [ns,nb] (e.g. after a Kutta-Joukowski
  * iteration); it enters at the next step's bookkeeping. */
@@ -93,7 +128,8 @@ int winds_wake_set_bound(winds_wake_batch *b, int icase, const double *bound);
 
 /* Mean device time per step of the last winds_wake_step call (ms, CUDA
  * events around its steps), interactions per step over all cases and
- * evaluations, and the number of kernels one step launches. */
+ * evaluations (the mean over that call's steps while a wake grows), and the
+ * number of kernels one step launches. */
 int winds_wake_stats(winds_wake_batch *b, double *step_ms, long long *interactions,
                      int *launches_per_step);
 

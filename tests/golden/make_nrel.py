@@ -73,4 +73,7 @@ def main(ref: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    src_tree = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("WINDS_REFERENCE")
+    if not src_tree:
+        sys.exit("usage: make_nrel.py <reference tree>  (or set WINDS_REFERENCE)")
+    main(src_tree)

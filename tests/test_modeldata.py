@@ -34,7 +34,11 @@ def test_nrel_fixture_and_stations():
     assert np.all(m["tables"][0]["cl"] == 0.0)
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference/modeldata"), reason="reference tree absent")
+REF_TREE = os.environ.get("WINDS_REFERENCE", "")
+
+
+@pytest.mark.skipif(not os.path.isdir(os.path.join(REF_TREE, "modeldata")) or not REF_TREE,
+                    reason="reference tree not given (WINDS_REFERENCE)")
 def test_fixture_regenerates_from_reference(tmp_path):
     import importlib.util
     spec = importlib.util.spec_from_file_location("make_nrel", os.path.join(GOLDEN, "make_nrel.py"))
@@ -43,7 +47,7 @@ def test_fixture_regenerates_from_reference(tmp_path):
     d0 = dict(np.load(os.path.join(GOLDEN, "nrel5mw.npz")))
     cwd = os.getcwd()
     try:
-        mk.main("/root/reference")
+        mk.main(REF_TREE)
     finally:
         os.chdir(cwd)
     d1 = dict(np.load(os.path.join(GOLDEN, "nrel5mw.npz")))

@@ -93,7 +93,7 @@ __device__ __forceinline__ unsigned long long spread3(unsigned v) {
 }
 
 // Sort key of a target: group id above a 30-bit Morton code of its position
-// in the targets' bounding box.
+// in the targets' bounding box (bit 31: the target is unused).
 __global__ void bs_target_keys(const double4 *__restrict__ tp, const int *__restrict__ tgroup,
                                long long n, const BBox *bb, unsigned long long *keys, int *vals) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -109,6 +109,9 @@ __global__ void bs_target_keys(const double4 *__restrict__ tp, const int *__rest
     if (u > 1023.0) u = 1023.0;
     code |= spread3((unsigned)u) << c;
   }
+  // a target marked unused (w != 0: past a growing wake's live columns) sorts
+  // after every live target of its group
+  if (p.w != 0.0) code |= 1ull << 31;
   keys[t] = ((unsigned long long)(unsigned)tgroup[t] << 32) | code;
   vals[t] = (int)t;
 }
@@ -130,6 +133,18 @@ __device__ __forceinline__ bool co_can_trigger(const BBox *bb, double co) {
     d2 += m * m;
   }
   return co * co < d2;  // false for NaN co: r > NaN is never true
+}
+
+// Cuts a work item to the live part of its group (GroupLive): the tile to its
+// live targets, the filament range to the live filaments. False when nothing
+// of the item is live; its partial sums are then neither written nor read.
+__device__ __forceinline__ bool clip_live(const GroupLive *live, Item &it, Tile &tl) {
+  const GroupLive gl = live[tl.group];
+  const long long tn = gl.t_end - tl.t_begin;
+  if (tn <= 0 || it.f_begin >= gl.f_end) return false;
+  if (tn < tl.t_count) tl.t_count = (int)tn;
+  if (it.f_end > gl.f_end) it.f_end = gl.f_end;
+  return true;
 }
 
 // ------------------------------------------------------- FP32 direct sum
@@ -541,8 +556,9 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<T>::value) bs_f32c(const F
     q = __shfl_sync(0xffffffffu, q, 0);
     if (q >= a.n_items) break;
     const int item_id = a.order ? a.order[q] : q;
-    const Item it = a.items[item_id];
-    const Tile tl = a.tiles[it.tile];
+    Item it = a.items[item_id];
+    Tile tl = a.tiles[it.tile];
+    if (a.live && !clip_live(a.live, it, tl)) continue;
     if (tl.t_count <= 0 || ((it.f_end - it.f_begin) % KF) != 0) {
       if (lane == 0) atomicOr(a.err, kErrBadItem);
       continue;
@@ -649,8 +665,9 @@ __global__ void __launch_bounds__(kF64Threads) bs_f64(const F32cArgs a) {
     __syncthreads();
     if (q >= a.n_items) break;
     const int item_id = a.order ? a.order[q] : q;
-    const Item it = a.items[item_id];
-    const Tile tl = a.tiles[it.tile];
+    Item it = a.items[item_id];
+    Tile tl = a.tiles[it.tile];
+    if (a.live && !clip_live(a.live, it, tl)) continue;  // uniform over the block
     int l = tid < tl.t_count ? tid : tl.t_count - 1;
     const double4 p = a.tp[tl.t_begin + l];
     double ux = 0.0, uy = 0.0, uz = 0.0;
@@ -684,11 +701,24 @@ __global__ void __launch_bounds__(kF64Threads) bs_f64(const F32cArgs a) {
 }
 
 // --------------------------------------------------------------- reduce
+// With a live table, only the live targets of a tile are written, from the
+// items before the group's live filament end (a tile's items cover increasing
+// filament ranges, so those come first).
 __global__ void bs_reduce(const Tile *__restrict__ tiles, const Group *__restrict__ groups,
                           const double *__restrict__ part, const int *__restrict__ perm,
-                          int tile_cap) {
-  const Tile tl = tiles[blockIdx.x];
+                          int tile_cap, const Item *__restrict__ items,
+                          const GroupLive *__restrict__ live) {
+  Tile tl = tiles[blockIdx.x];
   const Group g = groups[tl.group];
+  if (live) {
+    const GroupLive gl = live[tl.group];
+    const long long tn = gl.t_end - tl.t_begin;
+    if (tn <= 0) return;
+    if (tn < tl.t_count) tl.t_count = (int)tn;
+    int k = 0;
+    while (k < tl.n_items && items[tl.first_item + k].f_begin < gl.f_end) ++k;
+    tl.n_items = k;
+  }
   for (int l = threadIdx.x; l < tl.t_count; l += blockDim.x) {
     double s0 = 0.0, s1 = 0.0, s2 = 0.0;
 #pragma unroll 4
@@ -907,10 +937,12 @@ cudaError_t sort_target_keys(void *temp, size_t *temp_bytes, const unsigned long
 }
 
 cudaError_t launch_reduce(const Tile *tiles, int n_tiles, const Group *groups, const double *part,
-                          const int *perm, int tile_cap, cudaStream_t s) {
+                          const int *perm, int tile_cap, cudaStream_t s, const Item *items,
+                          const GroupLive *live) {
   if (n_tiles <= 0) return cudaSuccess;
+  if (live && !items) return cudaErrorInvalidValue;
   const int bs = tile_cap >= 256 ? 256 : (tile_cap + 31) / 32 * 32;  // one thread per target
-  bs_reduce<<<n_tiles, bs, 0, s>>>(tiles, groups, part, perm, tile_cap);
+  bs_reduce<<<n_tiles, bs, 0, s>>>(tiles, groups, part, perm, tile_cap, items, live);
   return cudaGetLastError();
 }
 

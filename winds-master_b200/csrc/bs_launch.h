@@ -45,8 +45,10 @@ cudaError_t sort_target_keys(void *temp, size_t *temp_bytes, const unsigned long
                              cudaStream_t s);
 cudaError_t launch_f32c(const F32cArgs &a, int model, int T, int KF, int grid, cudaStream_t s);
 cudaError_t launch_f64(const F32cArgs &a, int grid, cudaStream_t s);
+// live (with the plan's items): only each group's live part (GroupLive).
 cudaError_t launch_reduce(const Tile *tiles, int n_tiles, const Group *groups, const double *part,
-                          const int *perm, int tile_cap, cudaStream_t s);
+                          const int *perm, int tile_cap, cudaStream_t s,
+                          const Item *items = nullptr, const GroupLive *live = nullptr);
 cudaError_t launch_ffma_peak(float *out, int blocks, int iters, cudaStream_t s);
 cudaError_t launch_wait_selftest(unsigned *err, unsigned long long limit_ns, cudaStream_t s);
 cudaError_t launch_length(const double *F1, const double *F2, long long d0, long long nf, double *L,

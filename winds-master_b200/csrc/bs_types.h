@@ -56,6 +56,17 @@ struct Item {           // one tile against one filament chunk
   int pad;
 };
 
+// Live part of a group whose target and filament counts change on the device
+// (a growing wake inside a fixed plan): sorted targets [Group.t_begin, t_end)
+// and packed filaments [Group.f_begin, f_end) take part; tiles past t_end and
+// items from f_end on are skipped, items crossing f_end are cut there. f_end
+// is a multiple of the filament pad.
+struct GroupLive {
+  long long t_end;
+  int f_end;
+  int pad;
+};
+
 struct BBox {           // ordered-int keys of float bounds (see float_key)
   int tmin[3], tmax[3]; // targets
   int fmin[3], fmax[3]; // filament endpoints
@@ -69,6 +80,7 @@ struct F32cArgs {
   const Tile *tiles;
   const Item *items;
   const int *order;  // work queue: queue position -> item (nullptr: identity)
+  const GroupLive *live = nullptr;  // per group (nullptr: every tile and item is live)
   int n_items;
   int tile_cap;
   double *part;

@@ -127,14 +127,15 @@ __global__ void kj_features(const WakeCase *cases, const KJCase *kc, const int *
 
 // bound = base + out_scale * y, base Gamma_prev or, with *base != 0, its
 // extrapolation Gamma_prev + dGamma_prev (feature 9 of the row).
-__global__ void kj_apply_guess(const WakeCase *cases, const KJCase *kc, const float *y,
-                               const float *out_scale, const float *feat, const float *base,
-                               double *bound) {
+// Nothing before the step the iteration starts at (WakeCase::kj_from).
+__global__ void kj_apply_guess(const WakeCase *cases, const KJCase *kc, const int *step,
+                               const float *y, const float *out_scale, const float *feat,
+                               const float *base, double *bound) {
   const WakeCase c = cases[blockIdx.y];
   const KJCase k = kc[blockIdx.y];
   const int ns = c.nst - 1;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= ns * c.nb) return;
+  if (t >= ns * c.nb || *step < c.kj_from) return;
   const int i = t % ns, b = t / ns;
   double g = bound[c.bound_off + i + (long long)ns * b];
   if (*base != 0.f) g += (double)feat[(k.t_off + t) * kKJFeatures + 9];
@@ -245,6 +246,19 @@ __global__ void kj_check_cond(int ncases, double tol, int *converged, int *iters
   }
 }
 
+// Upstream of a graph's WHILE node: no iteration at a step before the one the
+// iteration starts at (WakeCase::kj_from, the same for every case; the
+// reference's first step is core/initials.m's, which has none).
+__global__ void kj_gate_cond(const WakeCase *cases, const int *step, cudaGraphConditionalHandle h) {
+  if (threadIdx.x == 0 && *step < cases[0].kj_from) cudaGraphSetConditional(h, 0u);
+}
+
+cudaError_t launch_kj_gate_cond(const WakeCase *cases, const int *step,
+                                cudaGraphConditionalHandle h, cudaStream_t s) {
+  kj_gate_cond<<<1, 32, 0, s>>>(cases, step, h);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_kj_check_cond(int ncases, double tol, int *converged, int *iters,
                                  unsigned long long *res_max, double *res_last, int *active,
                                  int *it_ctr, int maxiter, cudaGraphConditionalHandle h,
@@ -289,10 +303,11 @@ cudaError_t launch_kj_features(const WakeCase *cases, const KJCase *kc, int ncas
 }
 
 cudaError_t launch_kj_apply_guess(const WakeCase *cases, const KJCase *kc, int ncases, int max_st,
-                                  const float *y, const float *out_scale, const float *feat,
-                                  const float *base, double *bound, cudaStream_t s) {
-  kj_apply_guess<<<dim3((max_st + 127) / 128, ncases), 128, 0, s>>>(cases, kc, y, out_scale, feat,
-                                                                    base, bound);
+                                  const int *step, const float *y, const float *out_scale,
+                                  const float *feat, const float *base, double *bound,
+                                  cudaStream_t s) {
+  kj_apply_guess<<<dim3((max_st + 127) / 128, ncases), 128, 0, s>>>(cases, kc, step, y, out_scale,
+                                                                    feat, base, bound);
   return cudaGetLastError();
 }
 

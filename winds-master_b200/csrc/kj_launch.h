@@ -48,8 +48,9 @@ cudaError_t launch_kj_features(const WakeCase *cases, const KJCase *kc, int ncas
 // bound = base + out_scale * y (row order of the lifting-line targets); base
 // Gamma_prev, or Gamma_prev + feature 9 (its change) when *base != 0
 cudaError_t launch_kj_apply_guess(const WakeCase *cases, const KJCase *kc, int ncases, int max_st,
-                                  const float *y, const float *out_scale, const float *feat,
-                                  const float *base, double *bound, cudaStream_t s);
+                                  const int *step, const float *y, const float *out_scale,
+                                  const float *feat, const float *base, double *bound,
+                                  cudaStream_t s);
 // Rotor thrust, torque and power of every case at the step
 // (postproc/perform.m:18-62): out[3*case + {0,1,2}] = T, Q, P; dl [rows][3]
 // holds the spanwise terms.
@@ -59,6 +60,9 @@ cudaError_t launch_kj_loads(const WakeCase *cases, const KJCase *kc, int ncases,
                             const double *chord, const double *st_rr, const double *st_dr,
                             const double *rpm, const double *pitch, double *dl, double *out,
                             cudaStream_t s);
+// Clears a graph WHILE condition at a step before WakeCase::kj_from.
+cudaError_t launch_kj_gate_cond(const WakeCase *cases, const int *step,
+                                cudaGraphConditionalHandle h, cudaStream_t s);
 // kj_check that also sets a graph WHILE condition (see kj_kernels.cu).
 cudaError_t launch_kj_check_cond(int ncases, double tol, int *converged, int *iters,
                                  unsigned long long *res_max, double *res_last, int *active,

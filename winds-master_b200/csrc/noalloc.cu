@@ -12,8 +12,14 @@
 // holds until the process exits.
 //
 // Rules of use (also in include/winds_bs.h):
-//   * the first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress); make that first call before any stream capture;
+//   * every call looks up the array's device address on the current device
+//     (cudaGetSymbolAddress, a host-side lookup, so the address is never stale
+//     after a device reset); the first call on a device also loads the
+//     module, which commits the array: make that first call before any
+//     stream capture;
+//   * the work runs on the calling thread's current device and on `stream`
+//     (NULL: the legacy default stream), not on the library's own device
+//     choice and stream as winds_bs_eval_device does;
 //   * every call shares the one array and overwrites it: calls that overlap on
 //     the GPU (two streams, or two host threads) race and corrupt each other;
 //   * sizes are limited to WINDS_BS_NOALLOC_MAX_FILAMENTS filaments and
@@ -21,7 +27,6 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <mutex>
 
 #include "bs_launch.h"
 #include "engine.h"
@@ -38,22 +43,13 @@ constexpr size_t kPartBudget = (size_t)24 << 20;  // partial sums: 3 doubles per
 // symbol: the device address comes from cudaGetSymbolAddress below.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_addr_mu;
-unsigned char *g_addr[kMaxDevices] = {};
-
-// Device address of the scratch array on the current device (looked up once
-// per device, with that device current).
-int scratch_address(int dev, unsigned char **out) {
-  if (dev < 0 || dev >= kMaxDevices) return fail(WINDS_BS_ERR_ARG, "device %d out of range", dev);
-  std::lock_guard<std::mutex> g(g_addr_mu);
-  if (!g_addr[dev]) {
-    void *p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(noalloc scratch)");
-    g_addr[dev] = static_cast<unsigned char *>(p);
-  }
-  *out = g_addr[dev];
+// Device address of the scratch array on the current device, looked up on
+// every call: nothing is cached that a device reset could invalidate.
+int scratch_address(unsigned char **out) {
+  void *p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(noalloc scratch)");
+  *out = static_cast<unsigned char *>(p);
   return WINDS_BS_OK;
 }
 
@@ -145,9 +141,12 @@ extern "C" int winds_bs_eval_device_noalloc(const winds_bs_family *fams, int nfa
   int dev = 0;
   if ((e = cudaGetDevice(&dev)) != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
   unsigned char *base = nullptr;
-  if ((rc = scratch_address(dev, &base))) return rc;
+  if ((rc = scratch_address(&base))) return rc;
   int sms = 0;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
+      sms <= 0)
+    return e != cudaSuccess ? cuda_fail(e, "multiprocessor count")
+                            : fail(WINDS_BS_ERR_CUDA, "device %d reports no multiprocessors", dev);
 
   // ---- plan (sizes only; the tables are written by a kernel)
   const long long nfp = std::max<long long>((nf + kFilamentPad - 1) / kFilamentPad * kFilamentPad,
@@ -261,11 +260,12 @@ extern "C" int winds_bs_eval_device_noalloc(const winds_bs_family *fams, int nfa
   if (e == cudaSuccess) e = launch_reduce(tiles, n_tiles, groups, part, perm, tile_cap, s);
   if (e != cudaSuccess) return cuda_fail(e, "noalloc direct-sum launch");
 
-  // ---- synchronous: report a device-side timeout recorded in the error word
-  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "stream synchronize");
+  // ---- synchronous: report a device-side timeout recorded in the error word,
+  // read on the call's own stream (no wait on the device's other streams)
   unsigned word = 0;
-  if ((e = cudaMemcpy(&word, err, sizeof(word), cudaMemcpyDeviceToHost)) != cudaSuccess)
+  if ((e = cudaMemcpyAsync(&word, err, sizeof(word), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
     return cuda_fail(e, "error word read");
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "stream synchronize");
   if (word & kErrWaitTimeout)
     return fail(WINDS_BS_ERR_TIMEOUT, "a bounded device wait ran out (error word 0x%x)", word);
   if (word) return fail(WINDS_BS_ERR_CUDA, "device reported error word 0x%x", word);

@@ -5,10 +5,13 @@
 //   bookkeeping -> [pack filaments + targets -> sort -> direct sum -> reduce]
 //   -> convect (fe/ab2/ab4, or pcc predictor) -> (pcc: bookkeeping for p+1
 //   -> [direct sum at the predicted nodes] -> corrector) -> commit.
-// All sizes are fixed at creation (each wake keeps na columns), so the plan
-// tables of the persistent direct-sum kernel are built once and the whole
-// step can be captured once as a CUDA graph and replayed. The step counter
-// lives on the device, so a replayed graph reads the right kinematics row.
+// All sizes are fixed at creation (each wake has a capacity of na columns),
+// so the plan tables of the persistent direct-sum kernel are built once and
+// the whole step can be captured once as a CUDA graph and replayed. The step
+// counter lives on the device, so a replayed graph reads the right kinematics
+// row and the right live column count of a growing wake: every evaluation
+// first writes a live table (wake_live) that limits the direct sum and its
+// reduction to the live targets and filaments of each case.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -37,16 +40,19 @@ struct winds_wake_batch {
   cudaGraphExec_t exec = nullptr;
   std::vector<WakeCase> cases;
   long long nodes = 0, shed_n = 0, trail_n = 0, bound_n = 0, fil_pad = 0, kin_n = 0, wind_n = 0;
+  long long ser_n = 0;
   long long max_nodes = 0, max_cols = 0, max_fil = 0, max_slots = 0;
   int max_nb = 0;  // most blades of a case
-  long long interactions = 0;
+  long long interactions = 0;  // per step of the last winds_wake_step call
   int launches = 0;
+  int pcc_from = 0, kj_from = 0;  // first step of the corrector / the iteration (startup)
   // state and work buffers
   DevBuf cases_d, step_d;
   DevBuf dom, dom_pred, dom_new, vel, h1, h2, h3, uind, uind_pred;
   DevBuf bound, trail_prev, shed_cur, trail_cur, shed_next, trail_next;
   DevBuf rc_s, rc_t, len_old_s, len_old_t, len_s, len_t, len_ps, len_pt;
-  DevBuf quarter, trailing, wind;
+  DevBuf quarter, trailing, wind, ser;
+  DevBuf live_main, live_pred, live_kj;  // GroupLive per case, per evaluation kind
   // direct-sum buffers
   DevBuf pk, ra, rb, tp, tp_raw, tgroup, keys, vals, perm, sort_tmp;
   DevBuf groups_main, groups_pred, tiles, items, order, part, bbox, ctr, err, nearctr;
@@ -112,6 +118,10 @@ int alloc_all(winds_wake_batch *b) {
       (rc = b->quarter.ensure(b->kin_n * sizeof(double), s)) ||
       (rc = b->trailing.ensure(b->kin_n * sizeof(double), s)) ||
       (rc = b->wind.ensure(b->wind_n * sizeof(double), s)) ||
+      (rc = b->ser.ensure(std::max<long long>(b->ser_n, 1) * sizeof(double), s)) ||
+      (rc = b->live_main.ensure(b->ncases * sizeof(GroupLive), s)) ||
+      (rc = b->live_pred.ensure(b->ncases * sizeof(GroupLive), s)) ||
+      (rc = b->live_kj.ensure(b->ncases * sizeof(GroupLive), s)) ||
       (rc = b->cases_d.ensure(b->ncases * sizeof(WakeCase), s)) ||
       (rc = b->step_d.ensure(4 * sizeof(int), s)))
     return rc;
@@ -189,24 +199,29 @@ int build_plans(winds_wake_batch *b) {
   return WINDS_BS_OK;
 }
 
-// One induced-velocity evaluation of every case (nodes of `dom`, Γ, cores).
+// One induced-velocity evaluation of every case (nodes of `dom`, Γ, cores) at
+// step *step + step_add; live_mode kLiveNodes or kLivePredicted (wake_live).
 cudaError_t enqueue_eval(winds_wake_batch *b, const double *dom, const double *shed,
                          const double *trail, int step_add, const double *lold_s,
                          const double *lold_t, int have_old, double *lnew_s, double *lnew_t,
-                         double *rc_s, double *rc_t, DevBuf &groups, int &launches) {
+                         double *rc_s, double *rc_t, DevBuf &groups, int &launches,
+                         int live_mode = kLiveNodes) {
   cudaStream_t s = b->stream;
   const WakeCase *cd = P<const WakeCase>(b->cases_d);
+  const int *step = P<const int>(b->step_d);
   PackedFilaments pf{P<float4>(b->pk),
                      P<double4>(b->ra), P<double4>(b->rb)};
   BBox *bb = P<BBox>(b->bbox);
+  GroupLive *live = P<GroupLive>(live_mode == kLivePredicted ? b->live_pred : b->live_main);
   cudaError_t e = launch_bbox_init(bb, s);
+  if (e == cudaSuccess) e = launch_wake_live(cd, b->ncases, step, step_add, live_mode, live, s);
   if (e == cudaSuccess)
-    e = launch_wake_filaments(cd, b->ncases, b->max_fil, P<const int>(b->step_d), step_add, dom,
-                              shed, trail, lold_s, lold_t, have_old, b->prm.stretch, lnew_s, lnew_t,
-                              rc_s, rc_t, nullptr, nullptr, b->model, b->dcut, pf, bb, s);
+    e = launch_wake_filaments(cd, b->ncases, b->max_fil, step, step_add, P<const double>(b->ser),
+                              dom, shed, trail, lold_s, lold_t, have_old, b->prm.stretch, lnew_s,
+                              lnew_t, rc_s, rc_t, nullptr, nullptr, b->model, b->dcut, pf, bb, s);
   if (e == cudaSuccess)
-    e = launch_wake_targets(cd, b->ncases, b->max_nodes, dom, P<double4>(b->tp_raw),
-                            P<int>(b->tgroup), bb, s);
+    e = launch_wake_targets(cd, b->ncases, b->max_nodes, step, step_add, dom,
+                            P<double4>(b->tp_raw), P<int>(b->tgroup), bb, s);
   unsigned long long *k0 = P<unsigned long long>(b->keys), *k1 = k0 + std::max<long long>(b->nodes, 1);
   if (e == cudaSuccess)
     e = launch_target_keys(P<const double4>(b->tp_raw), P<const int>(b->tgroup), b->nodes, bb, k0,
@@ -239,13 +254,15 @@ cudaError_t enqueue_eval(winds_wake_batch *b, const double *dom, const double *s
   a.n = b->nidx;
   a.co = b->prm.co;
   a.wait_limit_ns = default_wait_limit_ns();
+  a.live = live;
   if (e == cudaSuccess)
     e = b->prec == WINDS_PREC_F64 ? launch_f64(a, b->grid, s)
                                   : launch_f32c(a, b->model, b->ch.T, b->ch.KF, b->grid, s);
   if (e == cudaSuccess)
     e = launch_reduce(P<const Tile>(b->tiles), b->n_tiles, P<const Group>(groups),
-                      P<const double>(b->part), P<const int>(b->perm), b->tile_cap, s);
-  launches += 12;  // bbox, filaments, targets, keys, sort (4), gather, memset, sum, reduce
+                      P<const double>(b->part), P<const int>(b->perm), b->tile_cap, s,
+                      P<const Item>(b->items), live);
+  launches += 13;  // bbox, live, filaments, targets, keys, sort (4), gather, memset, sum, reduce
   return e;
 }
 
@@ -255,12 +272,12 @@ cudaError_t enqueue_pre(winds_wake_batch *b, int &launches) {
   const int *step = P<const int>(b->step_d);
   launches = 0;
   const bool pcc = b->prm.integrator == WINDS_INTEG_PCC;
-  cudaError_t e = launch_wake_bookkeep(cd, b->ncases, b->max_cols, P<const double>(b->bound),
-                                       P<const double>(b->trail_prev), P<double>(b->shed_cur),
-                                       P<double>(b->trail_cur), s);
+  cudaError_t e = launch_wake_bookkeep(cd, b->ncases, b->max_cols, step, 0,
+                                       P<const double>(b->bound), P<const double>(b->trail_prev),
+                                       P<double>(b->shed_cur), P<double>(b->trail_cur), s);
   ++launches;
-  // have_old: lengths of a previous step exist from step 1 on (read on device
-  // through the counter would need a branch in the kernel; the host tracks it)
+  // previous lengths exist from creation on (the initial lengths: zero strain
+  // at step 0); the start-up's first stretching step is checked on the device
   if (e == cudaSuccess)
     e = enqueue_eval(b, P<const double>(b->dom), P<const double>(b->shed_cur),
                      P<const double>(b->trail_cur), 0, P<const double>(b->len_old_s),
@@ -279,7 +296,7 @@ cudaError_t enqueue_pre(winds_wake_batch *b, int &launches) {
   ++launches;
   if (pcc) {
     if (e == cudaSuccess)
-      e = launch_wake_bookkeep(cd, b->ncases, b->max_cols, P<const double>(b->bound),
+      e = launch_wake_bookkeep(cd, b->ncases, b->max_cols, step, 1, P<const double>(b->bound),
                                P<const double>(b->trail_cur), P<double>(b->shed_next),
                                P<double>(b->trail_next), s);
     ++launches;
@@ -287,7 +304,7 @@ cudaError_t enqueue_pre(winds_wake_batch *b, int &launches) {
       e = enqueue_eval(b, P<const double>(b->dom_pred), P<const double>(b->shed_next),
                        P<const double>(b->trail_next), 1, P<const double>(b->len_s),
                        P<const double>(b->len_t), 1, P<double>(b->len_ps), P<double>(b->len_pt),
-                       nullptr, nullptr, b->groups_pred, launches);
+                       nullptr, nullptr, b->groups_pred, launches, kLivePredicted);
     if (e == cudaSuccess)
       e = launch_wake_convect(cd, b->ncases, b->max_nodes, step, kConvectCorrector,
                               P<const double>(b->dom), nullptr, nullptr, P<const double>(b->dom_pred),
@@ -306,9 +323,9 @@ cudaError_t enqueue_post(winds_wake_batch *b, int &launches) {
   const WakeCase *cd = P<const WakeCase>(b->cases_d);
   cudaError_t e = cudaSuccess;
   if (b->kj) {
-    e = launch_wake_bookkeep(cd, b->ncases, b->max_cols, P<const double>(b->bound),
-                             P<const double>(b->trail_prev), P<double>(b->shed_cur),
-                             P<double>(b->trail_cur), s);
+    e = launch_wake_bookkeep(cd, b->ncases, b->max_cols, P<const int>(b->step_d), 0,
+                             P<const double>(b->bound), P<const double>(b->trail_prev),
+                             P<double>(b->shed_cur), P<double>(b->trail_cur), s);
     ++launches;
     if (e == cudaSuccess && b->loads) {
       e = launch_kj_loads(cd, P<const KJCase>(b->kjc_d), b->ncases, b->max_st,
@@ -355,20 +372,22 @@ cudaError_t enqueue_kj_iter(winds_wake_batch *b, int &launches, cudaStream_t s,
   // Γ of the bound iterate: columns 0-1 follow it (the others come from the
   // previous step); only those are recomputed and repacked (enqueue_kj_begin
   // did every column and every filament with the step's positions and cores)
-  cudaError_t e = launch_wake_bookkeep(cd, b->ncases, 2LL * b->max_nb, P<const double>(b->bound),
-                                       P<const double>(b->trail_prev), P<double>(b->shed_cur),
-                                       P<double>(b->trail_cur), s, 2);
+  const int *step = P<const int>(b->step_d);
+  cudaError_t e = launch_wake_bookkeep(cd, b->ncases, 2LL * b->max_nb, step, 0,
+                                       P<const double>(b->bound), P<const double>(b->trail_prev),
+                                       P<double>(b->shed_cur), P<double>(b->trail_cur), s, 2);
   if (e == cudaSuccess)
-    e = launch_wake_filaments_bound_cols(cd, b->ncases, b->max_bound_cols, P<const double>(b->dom),
-                                         P<const double>(b->shed_cur), P<const double>(b->trail_cur),
-                                         P<const double>(b->rc_s), P<const double>(b->rc_t),
-                                         b->model, b->dcut, pf, s);
+    e = launch_wake_filaments_bound_cols(cd, b->ncases, b->max_bound_cols, step,
+                                         P<const double>(b->dom), P<const double>(b->shed_cur),
+                                         P<const double>(b->trail_cur), P<const double>(b->rc_s),
+                                         P<const double>(b->rc_t), b->model, b->dcut, pf, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(b->ctr.p, 0, sizeof(unsigned), s);
   F32cArgs a;
   a.pk = pf.pk;
   a.ra = pf.ra;
   a.rb = pf.rb;
   a.tp = P<const double4>(b->tp_ll);
+  a.live = P<const GroupLive>(b->live_kj);
   a.groups = P<const Group>(b->kj_groups);
   a.tiles = P<const Tile>(b->kj_tiles);
   a.items = P<const Item>(b->kj_items);
@@ -390,7 +409,8 @@ cudaError_t enqueue_kj_iter(winds_wake_batch *b, int &launches, cudaStream_t s,
                                   : launch_f32c(a, b->model, b->kj_T, b->kj_KF, b->kj_grid, s);
   if (e == cudaSuccess)
     e = launch_reduce(P<const Tile>(b->kj_tiles), b->kj_ntiles, P<const Group>(b->kj_groups),
-                      P<const double>(b->kj_part), P<const int>(b->perm_ll), b->kj_tile_cap, s);
+                      P<const double>(b->kj_part), P<const int>(b->perm_ll), b->kj_tile_cap, s,
+                      P<const Item>(b->kj_items), P<const GroupLive>(b->live_kj));
   if (e == cudaSuccess)
     e = launch_kj_update(cd, kd, b->ncases, b->max_st, P<const int>(b->step_d),
                          P<const double>(b->uindb), P<const double>(b->bxn), P<const double>(b->byn),
@@ -415,6 +435,10 @@ cudaError_t enqueue_kj_iter(winds_wake_batch *b, int &launches, cudaStream_t s,
 cudaError_t enqueue_kj_begin(winds_wake_batch *b) {
   cudaStream_t s = b->stream;
   cudaError_t e = launch_bbox_init(P<BBox>(b->bbox), s);
+  // the step's live filaments; every lifting-line point is a target
+  if (e == cudaSuccess)
+    e = launch_wake_live(P<const WakeCase>(b->cases_d), b->ncases, P<const int>(b->step_d), 0,
+                         kLiveAll, P<GroupLive>(b->live_kj), s);
   if (e == cudaSuccess)
     e = launch_kj_targets(P<const WakeCase>(b->cases_d), P<const KJCase>(b->kjc_d), b->ncases,
                           b->max_st, P<const int>(b->step_d), P<const double>(b->ll),
@@ -444,9 +468,10 @@ cudaError_t enqueue_kj_begin(winds_wake_batch *b) {
         mlp_forward(b->mlp, P<__nv_bfloat16>(b->mw.X), b->n_ll, b->mw, P<float>(b->mw.y), s))
       e = cudaErrorLaunchFailure;
     if (e == cudaSuccess)
-      e = launch_kj_apply_guess(cd, kd, b->ncases, b->max_st, P<const float>(b->mw.y),
-                                mlp_out_scale_dev(b->mlp), P<const float>(b->feat),
-                                mlp_base_dev(b->mlp), P<double>(b->bound), s);
+      e = launch_kj_apply_guess(cd, kd, b->ncases, b->max_st, P<const int>(b->step_d),
+                                P<const float>(b->mw.y), mlp_out_scale_dev(b->mlp),
+                                P<const float>(b->feat), mlp_base_dev(b->mlp), P<double>(b->bound),
+                                s);
   }
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(b->guess.p, b->bound.p, b->bound_n * sizeof(double),
@@ -455,13 +480,14 @@ cudaError_t enqueue_kj_begin(winds_wake_batch *b) {
   // (as kj() does), Γ from the start value; the iterations repack only the
   // columns that follow the bound iterate
   if (e == cudaSuccess)
-    e = launch_wake_bookkeep(cd, b->ncases, b->max_cols, P<const double>(b->bound),
-                             P<const double>(b->trail_prev), P<double>(b->shed_cur),
-                             P<double>(b->trail_cur), s);
+    e = launch_wake_bookkeep(cd, b->ncases, b->max_cols, P<const int>(b->step_d), 0,
+                             P<const double>(b->bound), P<const double>(b->trail_prev),
+                             P<double>(b->shed_cur), P<double>(b->trail_cur), s);
   if (e == cudaSuccess) {
     PackedFilaments pf{P<float4>(b->pk), P<double4>(b->ra), P<double4>(b->rb)};
     e = launch_wake_filaments(cd, b->ncases, b->max_fil, P<const int>(b->step_d), 0,
-                              P<const double>(b->dom), P<const double>(b->shed_cur),
+                              P<const double>(b->ser), P<const double>(b->dom),
+                              P<const double>(b->shed_cur),
                               P<const double>(b->trail_cur), nullptr, nullptr, 0, 0, nullptr,
                               nullptr, nullptr, nullptr, P<const double>(b->rc_s),
                               P<const double>(b->rc_t), b->model, b->dcut, pf, P<BBox>(b->bbox), s);
@@ -493,6 +519,13 @@ int build_step_graph(winds_wake_batch *b) {
     size_t ndeps = 0;
     e = cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &ndeps);
     if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+    // no iteration at a step before the start-up's first (the condition is
+    // reset to 1 at every launch of the graph)
+    if (e == cudaSuccess && b->kj_from > 0) {
+      e = launch_kj_gate_cond(P<const WakeCase>(b->cases_d), P<const int>(b->step_d), h, s);
+      if (e == cudaSuccess) e = cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &ndeps);
+      ++l1;
+    }
     // zero-filled storage: the parameter union has no usable default constructor
     union NodeParams {
       cudaGraphNodeParams p;
@@ -540,6 +573,10 @@ int build_step_graph(winds_wake_batch *b) {
 }
 
 int run_kj(winds_wake_batch *b, bool use_graph) {
+  if (b->steps_done < b->kj_from) {  // the start-up's first step has no iteration
+    b->kj_evals = 0;
+    return WINDS_BS_OK;
+  }
   cudaError_t e = enqueue_kj_begin(b);
   if (e != cudaSuccess) return cuda_fail(e, "kj begin");
   if (use_graph && !b->exec_kj) {
@@ -585,6 +622,21 @@ int kj_step_errors(winds_wake_batch *b) {
   return WINDS_BS_OK;
 }
 
+// Interactions of step s over all cases and evaluations (the live columns'
+// nodes against the live filaments; the pcc prediction from its first step).
+long long step_interactions(const winds_wake_batch *b, long long s) {
+  long long n = 0;
+  for (const WakeCase &c : b->cases) {
+    const int m = live_cols(c, s);
+    n += (long long)c.nst * m * c.nb * live_filaments(c, m);
+    if (b->prm.integrator == WINDS_INTEG_PCC && s >= b->pcc_from) {
+      const int m1 = live_cols(c, s + 1);
+      n += (long long)c.nst * m1 * c.nb * live_filaments(c, m1);
+    }
+  }
+  return n;
+}
+
 }  // namespace
 
 extern "C" {
@@ -604,6 +656,8 @@ int winds_wake_create(const winds_wake_case *cases, int ncases, const winds_wake
   if ((rc = resolve_model(&bp, &model, &dcut, &nidx, &prec))) return rc;
   if (prm->integrator < WINDS_INTEG_FE || prm->integrator > WINDS_INTEG_PCC)
     return fail(WINDS_BS_ERR_ARG, "unknown integrator %d", prm->integrator);
+  if (prm->startup != WINDS_STARTUP_FULL && prm->startup != WINDS_STARTUP_REFERENCE)
+    return fail(WINDS_BS_ERR_ARG, "unknown start-up %d", prm->startup);
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0)
     return fail(WINDS_BS_ERR_NODEV, "no CUDA device is visible");
@@ -615,19 +669,28 @@ int winds_wake_create(const winds_wake_case *cases, int ncases, const winds_wake
   b->prec = prec;
   b->dcut = dcut;
   b->nidx = nidx;
+  const bool ref_startup = prm->startup == WINDS_STARTUP_REFERENCE;
+  // time index p = s + 1: corrector when p > 2 (pcc.m:40), stretching when
+  // p > 3 (filamentmod.m:26), no iteration at p = 1 (initials.m)
+  b->pcc_from = ref_startup ? 2 : 0;
+  b->kj_from = ref_startup ? 1 : 0;
   cudaError_t e;
   if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess ||
       (e = cudaEventCreate(&b->ev0)) != cudaSuccess || (e = cudaEventCreate(&b->ev1)) != cudaSuccess) {
     delete b;
     return cuda_fail(e, "wake stream/events");
   }
-  long long node = 0, sh = 0, tr = 0, bd = 0, fil = 0, kin = 0, wnd = 0;
+  long long node = 0, sh = 0, tr = 0, bd = 0, fil = 0, kin = 0, wnd = 0, ser = 0;
   for (int k = 0; k < ncases; ++k) {
     const winds_wake_case &h = cases[k];
     if (h.nst < 2 || h.nb < 1 || h.na < 3 || h.nsteps < 2 || !(h.dt > 0) || !h.quarter ||
         !h.trailing || !h.wind || !h.dom || !h.bound || !h.trail_gamma) {
       winds_wake_destroy(b);
       return fail(WINDS_BS_ERR_ARG, "case %d: bad sizes or null arrays", k);
+    }
+    if (h.na_start != 0 && (h.na_start < 2 || h.na_start > h.na)) {
+      winds_wake_destroy(b);
+      return fail(WINDS_BS_ERR_ARG, "case %d: na_start %d outside 2..na (%d)", k, h.na_start, h.na);
     }
     WakeCase c;
     std::memset(&c, 0, sizeof(c));
@@ -639,6 +702,14 @@ int winds_wake_create(const winds_wake_case *cases, int ncases, const winds_wake
     c.dt = h.dt, c.t0 = h.t0, c.shear = h.shear, c.hub = h.hub_height > 0 ? h.hub_height : 1.0;
     c.r0 = h.r0, c.rc0 = h.rc0, c.alpha = h.alpha, c.nu = h.nu, c.a1 = h.a1, c.delta = h.delta;
     c.core_mode = h.core_mode;
+    c.na0 = h.na_start ? h.na_start : h.na;
+    c.ser_off = ser;
+    c.has_time = h.time != nullptr;
+    c.has_r0 = h.r0_step != nullptr;
+    c.pcc_from = b->pcc_from;
+    c.stretch_from = ref_startup ? 3 : 0;
+    c.kj_from = b->kj_from;
+    ser += 2LL * h.nsteps;
     const long long nn = (long long)h.nst * h.na * h.nb;
     node += nn;
     sh += (long long)(h.nst - 1) * h.na * h.nb;
@@ -652,20 +723,22 @@ int winds_wake_create(const winds_wake_case *cases, int ncases, const winds_wake
     b->max_nb = std::max(b->max_nb, h.nb);
     b->max_fil = std::max(b->max_fil, c.fil_pad);
     b->max_slots = std::max(b->max_slots, nn);
-    b->interactions += nn * c.fil_count;
     b->min_nsteps = k == 0 ? h.nsteps : std::min<long long>(b->min_nsteps, h.nsteps);
     b->cases.push_back(c);
   }
   b->nodes = node, b->shed_n = sh, b->trail_n = tr, b->bound_n = bd, b->fil_pad = fil;
-  b->kin_n = kin, b->wind_n = wnd;
-  if (prm->integrator == WINDS_INTEG_PCC) b->interactions *= 2;
+  b->kin_n = kin, b->wind_n = wnd, b->ser_n = ser;
+  b->interactions = step_interactions(b, 0);
+  bool grows = false;
+  for (const WakeCase &c : b->cases) grows = grows || c.na0 < c.na;
   if (fil > (1ll << 30) || node > (1ll << 30)) {
     winds_wake_destroy(b);
     return fail(WINDS_BS_ERR_ARG, "batch too large");
   }
   b->ch = default_choice(node);
   b->ch.waves = 32.0;
-  if (prec == WINDS_PREC_F32C) b->tuned = lookup_tune(model, node, fil, &b->ch);
+  // a growing wake's first steps are no sample of its work: default tiling
+  if (prec == WINDS_PREC_F32C && !grows) b->tuned = lookup_tune(model, node, fil, &b->ch);
   if ((rc = alloc_all(b)) || (rc = build_plans(b))) {
     winds_wake_destroy(b);
     return rc;
@@ -693,6 +766,12 @@ int winds_wake_create(const winds_wake_case *cases, int ncases, const winds_wake
     if (e == cudaSuccess)
       e = cudaMemcpy(P<double>(b->wind) + c.wind_off, h.wind, 3 * h.nsteps * sizeof(double),
                      cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && h.time)
+      e = cudaMemcpy(P<double>(b->ser) + c.ser_off, h.time, h.nsteps * sizeof(double),
+                     cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && h.r0_step)
+      e = cudaMemcpy(P<double>(b->ser) + c.ser_off + h.nsteps, h.r0_step,
+                     h.nsteps * sizeof(double), cudaMemcpyHostToDevice);
     // the stored trailing columns are those of the step before: trail_prev(:,k) = trail(:,k+1)
     if (e == cudaSuccess) {
       tmp.assign(ntr, 0.0);
@@ -720,8 +799,9 @@ int winds_wake_create(const winds_wake_case *cases, int ncases, const winds_wake
     // initial lengths = current lengths (zero strain at the first step)
     int l = 0;
     cudaError_t e2 = launch_wake_bookkeep(P<const WakeCase>(b->cases_d), b->ncases, b->max_cols,
-                                          P<const double>(b->bound), P<const double>(b->trail_prev),
-                                          P<double>(b->shed_cur), P<double>(b->trail_cur), b->stream);
+                                          P<const int>(b->step_d), 0, P<const double>(b->bound),
+                                          P<const double>(b->trail_prev), P<double>(b->shed_cur),
+                                          P<double>(b->trail_cur), b->stream);
     if (e2 == cudaSuccess)
       e2 = enqueue_eval(b, P<const double>(b->dom), P<const double>(b->shed_cur),
                         P<const double>(b->trail_cur), 0, P<const double>(b->len_old_s),
@@ -754,8 +834,9 @@ static int autotune_batch(winds_wake_batch *b) {
   if (!c->autotune) return build_plans(b);
   cudaStream_t s = b->stream;
   cudaError_t e = launch_wake_bookkeep(P<const WakeCase>(b->cases_d), b->ncases, b->max_cols,
-                                       P<const double>(b->bound), P<const double>(b->trail_prev),
-                                       P<double>(b->shed_cur), P<double>(b->trail_cur), s);
+                                       P<const int>(b->step_d), 0, P<const double>(b->bound),
+                                       P<const double>(b->trail_prev), P<double>(b->shed_cur),
+                                       P<double>(b->trail_cur), s);
   if (e != cudaSuccess) return cuda_fail(e, "autotune bookkeeping");
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
@@ -806,8 +887,28 @@ static int device_error_word(winds_wake_batch *b) {
   return WINDS_BS_OK;
 }
 
+static int step_impl(winds_wake_batch *b, int nsteps, int use_graph);
+
 int winds_wake_step(winds_wake_batch *b, int nsteps, int use_graph) {
   if (!b || nsteps < 0) return fail(WINDS_BS_ERR_ARG, "bad step arguments");
+  const long long s0 = b->steps_done;
+  const int rc = step_impl(b, nsteps, use_graph);
+  if (rc == WINDS_BS_OK && b->steps_done > s0) {
+    long long n = 0;
+    for (long long s = s0; s < b->steps_done; ++s) n += step_interactions(b, s);
+    b->interactions = n / (b->steps_done - s0);
+  }
+  return rc;
+}
+
+int winds_wake_get_live(winds_wake_batch *b, int icase, int *na_live, long long *steps_done) {
+  if (!b || icase < 0 || icase >= b->ncases) return fail(WINDS_BS_ERR_ARG, "bad case index");
+  if (na_live) *na_live = live_cols(b->cases[icase], b->steps_done);
+  if (steps_done) *steps_done = b->steps_done;
+  return WINDS_BS_OK;
+}
+
+static int step_impl(winds_wake_batch *b, int nsteps, int use_graph) {
   if (b->steps_done + nsteps >= b->min_nsteps)
     return fail(WINDS_BS_ERR_ARG, "kinematics cover %lld steps; %lld done, %d more requested",
                 b->min_nsteps - 1, b->steps_done, nsteps);
@@ -1043,6 +1144,13 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
   if ((rc = b->kj_it.ensure(16, s))) return rc;
   for (DevBuf *x : {&b->cl_o, &b->cd_o, &b->aoa_o, &b->guess, &b->bound_last})
     if ((rc = x->ensure(b->bound_n * sizeof(double), s))) return rc;
+  // defined values before any iteration (a step without one reads them)
+  for (DevBuf *x : {&b->conv, &b->iters, &b->diverged, &b->res_max, &b->res_last, &b->active})
+    if (cudaError_t e0 = cudaMemset(x->p, 0, std::max(b->ncases, 1) * 8 + 8); e0 != cudaSuccess)
+      return cuda_fail(e0, "lifting-line counters");
+  for (DevBuf *x : {&b->cl_o, &b->cd_o, &b->aoa_o})
+    if (cudaError_t e0 = cudaMemset(x->p, 0, b->bound_n * sizeof(double)); e0 != cudaSuccess)
+      return cuda_fail(e0, "lifting-line outputs");
   // no change before the first step
   if (cudaError_t e0 = cudaMemcpy(b->bound_last.p, b->bound.p, b->bound_n * sizeof(double),
                                   cudaMemcpyDeviceToDevice);

@@ -20,6 +20,9 @@ cases built from them through the kinematics.
     ``WindV*i``, ``RotSpeed``), in the form ``operating_series`` returns.
   * ``cases(...)`` -- a ``winds_wake_case`` and a ``winds_kj_case`` (dicts for
     ``wake.WakeBatch`` / ``set_kj``) from the kinematics of that series.
+  * ``initial_cases(...)`` -- the same for a run from ``core/initials.m``'s
+    state: a wake of two columns that grows by one per step, the core of
+    ``core/vcore.m`` with ``wake.r0`` and ``fastout.Time`` per step.
 """
 from __future__ import annotations
 
@@ -184,7 +187,7 @@ def cases(model: dict, series: dict, kin: dict, rc0=0.1, delta=100.0, nu=1.5e-5,
     f = np.asfortranarray
     quarter = kin["quarter"][:, :, s0:, :]
     trail = kin["trail"][:, :, s0:, :]
-    dom = np.zeros((nst, 3, na, nb))
+    dom = np.zeros((nst, 3, max(na, 2), nb))  # initial_cases sets the capacity of na = 1 series
     dom[:, :, 0, :] = quarter[:, :, 0, :]
     dom[:, :, 1, :] = trail[:, :, 0, :]
     for j in range(2, na):
@@ -196,7 +199,7 @@ def cases(model: dict, series: dict, kin: dict, rc0=0.1, delta=100.0, nu=1.5e-5,
     wake = dict(nst=nst, nb=nb, na=na, nsteps=nsteps + 1, dt=dt, t0=0.0, quarter=f(quarter),
                 trailing=f(trail), wind=f(wind), shear=0.0, hub_height=float(model["tower_ht"]),
                 core_mode=1, r0=rc0, rc0=rc0, alpha=alpha, nu=nu, a1=0.0, delta=delta, dom=f(dom),
-                bound=f(np.zeros((ns, nb))), trail_gamma=f(np.zeros((nst, na - 1, nb))))
+                bound=f(np.zeros((ns, nb))), trail_gamma=f(np.zeros((nst, max(na, 2) - 1, nb))))
     st = stations(model["r_trail"], model["chord_trail"], model["twist_trail"], model["nfoil_trail"])
     tabs = model["tables"]
     R = float(model["r_trail"][-1])
@@ -217,6 +220,48 @@ def cases(model: dict, series: dict, kin: dict, rc0=0.1, delta=100.0, nu=1.5e-5,
     if per_step:  # blade pitch per step and blade for the loads (perform.m:22-33)
         kj["pitch"] = f(np.asarray(series["pitch"], np.float64)[s0:s0 + nsteps + 1])
     return wake, kj
+
+
+VCORE = dict(alpha=1.25643, nu=1e-5, delta=100.0, a1=6.5e-5)  # core/constants.m:22-25
+
+
+def initial_r0(tip_rad, tsr, wind_speed, alpha=VCORE["alpha"], nu=VCORE["nu"], delta=VCORE["delta"]):
+    """``wake.r0`` per step (core/initials.m:134-135):
+    ``sqrt(4 alpha nu delta T0)``, ``T0 = 2 pi R / (12 TSR |U|)``."""
+    T0 = 2 * np.pi * tip_rad / (12 * np.asarray(tsr, np.float64) * np.asarray(wind_speed, np.float64))
+    return np.sqrt(4 * alpha * nu * delta * T0)
+
+
+def initial_cases(model: dict, series: dict, kin: dict, cl0, na: int, rho=1.23) -> tuple:
+    """(wake case, lifting-line case) of a run from the state core/initials.m
+    sets up at time index 1 (step 0 of the series, ``series["_na"] == 1``):
+    ``wake.domain{1}`` = quarter-chord and trailing-edge nodes, capacity ``na``
+    columns; bound circulation ``0.5 |U(1)| chord cl0`` (``cl0``: BEM's Cl,
+    [ns] or [ns, nb]); ``tsr`` per step from ``series["tsr"]`` (else
+    omega R / |U|) for ``wake.r0``; the core of core/vcore.m (absolute time,
+    core/constants.m's values). Use with ``startup="reference"``."""
+    if series["_na"] != 1:
+        raise ValueError("a run from initials starts at the series' first sample (na = 1)")
+    wk, kj = cases(model, series, kin)
+    nst, nb, nsteps = wk["nst"], wk["nb"], wk["nsteps"]
+    ns = nst - 1
+    wind = np.asarray(series["wind"], np.float64)[:nsteps]
+    U = np.sqrt(np.sum(wind ** 2, axis=1))
+    R = float(model["r_trail"][-1])
+    tsr = np.asarray(series["tsr"], np.float64)[:nsteps] if "tsr" in series else series["_omega"] * R / U
+    dom = np.zeros((nst, 3, na, nb))
+    dom[:, :, :2, :] = wk["dom"][:, :, :2, :]
+    cl0 = np.asarray(cl0, np.float64)
+    if cl0.ndim == 1:
+        cl0 = np.repeat(cl0[:, None], nb, axis=1)
+    chord = np.asarray(kj["chord"], np.float64)
+    bound = 0.5 * U[0] * chord[:, None] * cl0
+    wk.update(na=na, na_start=2, dom=np.asfortranarray(dom), bound=np.asfortranarray(bound),
+              trail_gamma=np.asfortranarray(np.zeros((nst, na - 1, nb))), wind=np.asfortranarray(wind.T),
+              core_mode=0, r0=0.0, time=np.asarray(series["time"], np.float64)[:nsteps].copy(),
+              r0_step=initial_r0(R, tsr, U), **VCORE)
+    kj["rho"] = rho
+    return wk, kj
 
 
 def load_model(path: str) -> dict:

@@ -5,6 +5,13 @@ velocity, bookkeeping, core growth and convection: ``WInDS.m:127-179``).
 ``WakeBatch(cases, ...)`` takes case dicts as :func:`synth.make_wake_case`
 returns them (WInDS-layout arrays), ``step(n, graph=True)`` advances every
 case, ``state(i)`` reads one case back.
+
+A case dict may also give ``na_start`` (live age columns at step 0: 2 starts
+from the two columns of ``core/initials.m:84-86`` and grows one column per
+step up to ``na``), ``time`` (``fastout.Time`` per step) and ``r0_step``
+(``wake.r0`` per step, ``core/initials.m:134-135``). ``startup="reference"``
+applies the reference's time-index switches (``ab2.m:35``, ``ab4.m:35``,
+``pcc.m:40``, ``filamentmod.m:26``; no lifting-line iteration at step 0).
 """
 from __future__ import annotations
 
@@ -24,7 +31,8 @@ class WakeCaseC(C.Structure):
                 ("shear", C.c_double), ("hub_height", C.c_double), ("core_mode", C.c_int),
                 ("r0", C.c_double), ("rc0", C.c_double), ("alpha", C.c_double), ("nu", C.c_double),
                 ("a1", C.c_double), ("delta", C.c_double),
-                ("dom", C.c_void_p), ("bound", C.c_void_p), ("trail_gamma", C.c_void_p)]
+                ("dom", C.c_void_p), ("bound", C.c_void_p), ("trail_gamma", C.c_void_p),
+                ("na_start", C.c_int), ("time", C.c_void_p), ("r0_step", C.c_void_p)]
 
 
 class KJCaseC(C.Structure):
@@ -44,7 +52,9 @@ class KJParamsC(C.Structure):
 class WakeParamsC(C.Structure):
     _fields_ = [("integrator", C.c_int), ("core_model", C.c_int), ("d", C.c_double),
                 ("co", C.c_double), ("precision", C.c_int), ("pcc_double_add", C.c_int),
-                ("stretch", C.c_int)]
+                ("stretch", C.c_int), ("startup", C.c_int)]
+
+STARTUP = {"full": 0, "reference": 1}
 
 
 def _bind():
@@ -65,13 +75,15 @@ def _bind():
         L.winds_wake_get_kj_guess.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         L.winds_wake_get_kj_features.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         L.winds_wake_get_loads.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.winds_wake_get_live.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int),
+                                          C.POINTER(C.c_longlong)]
         L._wake_bound = True
     return L
 
 
 class WakeBatch:
     def __init__(self, cases, integrator="pcc", d="visc2", co=1000.0, precision="f32c",
-                 pcc_double_add=True, stretch=True):
+                 pcc_double_add=True, stretch=True, startup="full"):
         L = _bind()
         self._keep = []
         arr = (WakeCaseC * len(cases))()
@@ -85,9 +97,18 @@ class WakeBatch:
                 x = np.asfortranarray(c[f], dtype=np.float64)
                 self._keep.append(x)
                 setattr(a, f, x.ctypes.data)
+            a.na_start = int(c.get("na_start", 0))
+            for f in ("time", "r0_step"):
+                if c.get(f) is not None:
+                    x = np.ascontiguousarray(c[f], dtype=np.float64)
+                    if x.size < int(c["nsteps"]):
+                        raise ValueError(f"case {k}: {f} has {x.size} entries, nsteps is {c['nsteps']}")
+                    self._keep.append(x)
+                    setattr(a, f, x.ctypes.data)
         core, dv = parse_core(d)
         p = WakeParamsC(INTEG[integrator], core, dv, float(co),
-                        {"f32c": 0, "f64": 1}[precision], int(pcc_double_add), int(stretch))
+                        {"f32c": 0, "f64": 1}[precision], int(pcc_double_add), int(stretch),
+                        STARTUP[startup])
         h = C.c_void_p()
         _check(L.winds_wake_create(arr, len(cases), C.byref(p), C.byref(h)))
         self.h = h
@@ -95,6 +116,12 @@ class WakeBatch:
 
     def step(self, n=1, graph=False):
         _check(_bind().winds_wake_step(self.h, int(n), 1 if graph else 0))
+
+    def live(self, i=0):
+        """(live age columns of case ``i``'s wake now, steps run so far)."""
+        m, st = C.c_int(), C.c_longlong()
+        _check(_bind().winds_wake_get_live(self.h, i, C.byref(m), C.byref(st)))
+        return m.value, st.value
 
     def state(self, i):
         c = self.cases[i]
