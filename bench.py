@@ -52,13 +52,13 @@ def parse():
                     help="large: 3x41x720 (the metric's case); medium: 3x41x180 for profiling")
     ap.add_argument("--tiling", default=None,
                     help="force the FP32 tiling 'T,KF,waves' instead of the autotuner's choice")
-    ap.add_argument("--wake-steps", type=int, default=3,
+    ap.add_argument("--wake-steps", type=int, default=10,
                     help="timed pcc steps of the 64-case batched wake (0: skip)")
     ap.add_argument("--quick", action="store_true",
                     help="timed loop only (no FP64 comparison, e2e, CPU baseline or studies)")
     ap.add_argument("--no-studies", action="store_true",
                     help="skip the start-value study and the end-to-end run")
-    ap.add_argument("--e2e-steps", type=int, default=3,
+    ap.add_argument("--e2e-steps", type=int, default=20,
                     help="pcc steps of the 16-case end-to-end run (each path)")
     ap.add_argument("--wake-only", action="store_true",
                     help="profiling aid: only the 64-case batched wake (fast path, default "
@@ -141,6 +141,15 @@ def workload(seed, kind="large"):
     P = np.asfortranarray(pts.reshape(-1, 3, 1, 1))
     nf = sum(f[0].shape[0] * f[0].shape[2] * f[0].shape[3] for f in fams)
     return w, fams, P, nf, P.shape[0]
+
+
+def bench_config(kind, nt, nf, world):
+    """The workload description both arms print (the same dict on both)."""
+    return {"workload": f"helical wake 3x41x{720 if kind == 'large' else 180} (1 deg), Vatistas n=2, "
+            "all shed+trailing filaments onto all wake nodes + lifting-line points",
+            "targets": nt, "filaments": nf, "interactions_per_step": nt * nf,
+            "l2": "256 MB buffer written between timed steps (GPU arm)",
+            "parallelism": f"replicated wakes x{world}" if world > 1 else "single GPU"}
 
 
 def profiled_traffic(interactions):
@@ -235,8 +244,7 @@ def reference_arm(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total_t / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": "helical wake 3x41x720 (1 deg), Vatistas n=2, all shed+trailing "
-                   "filaments onto all wake nodes + lifting-line points", "targets": nt, "filaments": nf},
+        "config": bench_config(args.workload, nt, nf, int(os.environ.get("WORLD_SIZE", "1"))),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": f"{n} sampled targets x {nf} filaments per step"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -247,93 +255,192 @@ def reference_arm(args):
 
 
 # ------------------------------------------------------------------ batched wake
-def wake_bench(args, seed=2, ncases=64, plain=True):
+def timed_steps(b, n, graph):
+    """Steps ``b`` n times; mean device ms per step (CUDA events per call)."""
+    ms = []
+    for _ in range(n):
+        b.step(1, graph=graph)
+        ms.append(b.stats()[0])
+    return statistics.mean(ms)
+
+
+def wake_bench(args, seed=2, ncases=64, plain=True, mlp=None):
     """64 uneven rotor cases (wake steps 60-720, span nodes 17-41, U 5-25 m/s,
-    TSR 4-10, yaw 0-30 deg, shear 0-0.3), pcc predictor-corrector step: the
-    FP32-compensated batched engine replaying one CUDA graph per step, against
-    the plain FP64 path (each case on its own, eager, FP64 direct sum)."""
+    TSR 4-10, yaw 0-30 deg, shear 0-0.3), pcc predictor-corrector step. Three
+    paths: the FP32-compensated batch replaying one CUDA graph per step (the
+    product), the same batch in FP64 (batching and graphs without the FP32
+    direct sum), and the plain FP64 path (each case on its own, eager, FP64).
+    plain / batched FP64 is the batching-and-graph gain, batched FP64 / fast
+    the FP32c gain."""
     synth = importlib.import_module("winds-master_b200.synth")
     wake = importlib.import_module("winds-master_b200.wake")
     rcases = synth.batch_cases(ncases, seed=seed)
-    warm = 1
-    cases = [synth.make_wake_case(rc, nsteps=warm + args.wake_steps + 3, jitter=0.05)
+    warm, n_fast, n_b64 = 1, args.wake_steps, 3
+    cases = [synth.make_wake_case(rc, nsteps=warm + max(n_fast, n_b64) + 3, jitter=0.05)
              for rc in rcases]
     b = wake.WakeBatch(cases, integrator="pcc", precision="f32c")
     b.step(warm, graph=True)
-    b.step(args.wake_steps, graph=True)
-    ms, inter, launches = b.stats()
+    ms = timed_steps(b, n_fast, True)
+    _, inter, launches = b.stats()
     b.close()
+    nodes = int(sum(c["nst"] * c["na"] * c["nb"] for c in cases))
+    if not plain:
+        return {"cases": ncases, "integrator": "pcc", "graph": True, "steps_per_s": 1000.0 / ms,
+                "ms_per_step": ms, "launches_per_step": launches, "nodes": nodes}
+    b64 = wake.WakeBatch(cases, integrator="pcc", precision="f64")
+    b64.step(warm, graph=True)
+    ms64 = timed_steps(b64, n_b64, True)
+    b64.close()
     plain_ms = 0.0
-    for c in (cases if plain else []):
+    for c in cases:
         p = wake.WakeBatch([c], integrator="pcc", precision="f64")
         p.step(1)
         p.step(1)
         plain_ms += p.stats()[0]
         p.close()
-    if not plain:
-        return {"cases": ncases, "integrator": "pcc", "graph": True, "steps_per_s": 1000.0 / ms,
-                "ms_per_step": ms, "launches_per_step": launches,
-                "nodes": int(sum(c["nst"] * c["na"] * c["nb"] for c in cases))}
-    return {"cases": ncases, "integrator": "pcc", "graph": True,
+    return {"cases": ncases, "integrator": "pcc", "graph": True, "timed_steps": n_fast,
             "steps_per_s": 1000.0 / ms, "ms_per_step": ms,
             "interactions_per_step": inter, "gint_per_s": inter / (ms * 1e-3) / 1e9,
             "launches_per_step": launches,
+            "batched_fp64_steps_per_s": 1000.0 / ms64, "batched_fp64_timed_steps": n_b64,
             "plain_fp64_steps_per_s": 1000.0 / plain_ms,
             "speedup_vs_plain_fp64": plain_ms / ms,
-            "nodes": int(sum(c["nst"] * c["na"] * c["nb"] for c in cases)),
-            "lifting_line": wake_kj_bench(rcases, cases)}
+            "gain_batching_and_graphs": plain_ms / ms64, "gain_fp32c_over_fp64": ms64 / ms,
+            "nodes": nodes,
+            "lifting_line": wake_kj_bench(rcases, cases, mlp=mlp)}
 
 
-def wake_kj_bench(rcases, cases, tol=1e-6, relax=0.3, maxiter=200):
+def sharded_wake_bench(args, rank, world, seed=2, ncases=64):
+    """The 64-case batch split over the ranks by case (sharding.ShardedRun):
+    each rank steps the batch of its own cases with graph replay, with no
+    collective on the data path; per-case values are gathered on the host
+    after every step. The batch's step time is the slowest rank's (CUDA
+    events around each rank's steps, max over ranks)."""
+    import torch
+    import torch.distributed as dist
+    synth = importlib.import_module("winds-master_b200.synth")
+    sh = importlib.import_module("winds-master_b200.sharding")
+    rcases = synth.batch_cases(ncases, seed=seed)
+    cases = [synth.make_wake_case(rc, nsteps=1 + args.wake_steps + 3, jitter=0.05) for rc in rcases]
+    run = sh.ShardedRun(cases, rank=rank, world=world, integrator="pcc", precision="f32c")
+    run.step(1)  # capture
+    ms = 0.0
+    for _ in range(args.wake_steps):
+        run.step(1)
+        ms += run.local.step_ms() if run.local is not None else 0.0
+    parts = run.parts
+    run.close()
+    t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    costs = [sh.case_cost(c) for c in cases]
+    return {"cases": ncases, "ranks": world, "parallelism": "case-sharded", "integrator": "pcc",
+            "graph": True, "timed_steps": args.wake_steps,
+            "steps_per_s": 1000.0 * args.wake_steps / float(t.item()),
+            "cases_per_rank": [len(p) for p in parts], "imbalance": sh.imbalance(costs, parts),
+            "timing": "CUDA events around each rank's steps, max over ranks"}
+
+
+def batch_start_value(seed=12, n_train=48, n_val=8, steps=10, relax=0.3, tol=1e-6, maxiter=200):
+    """A start-value network for the 64-case mix: pairs from the plain solver
+    on other draws of the same case distribution (batch_cases, no root
+    cylinders), extrapolated base, output scale chosen on validation draws."""
+    synth = importlib.import_module("winds-master_b200.synth")
+    gi = importlib.import_module("winds-master_b200.gamma_init")
+    kw = dict(relax=relax, tol=tol, maxiter=maxiter, root_cut=0.0)
+    pts = [gi.OperatingPoint(rc, 0.0) for rc in synth.batch_cases(n_train + n_val, seed=seed)]
+    tr = gi.run(pts[:n_train], steps, record=True, **kw)
+    keep = (tr["step_case"][:, 0] >= 4) & tr["lift"]
+    m, _ = gi.train(tr["X"][keep], tr["dG"][keep], epochs=40, base="extrapolated")
+    gi.choose_shrink(m, pts[n_train:], steps, **kw)
+    return m
+
+
+def wake_kj_bench(rcases, cases, tol=1e-6, relax=0.3, maxiter=200, warm=3, timed=3, mlp=None):
     """The 64-case batch with the lifting line and rotor loads: every pcc step
-    runs the Kutta-Joukowski fixed point to the same tolerance on both paths.
-    Fast: FP32c, one CUDA graph per step (the iteration a conditional node).
-    Plain: each case alone, FP64, eager, the host waiting on the convergence
-    flag every iteration. One warm step, then one timed step each."""
+    runs the Kutta-Joukowski fixed point to the same tolerance on every path.
+    Fast: FP32c, one CUDA graph per step (the iteration a conditional node),
+    started from the previous step's circulation (the reference), from its
+    extrapolation alone, and from the extrapolation plus the network (when
+    given). Host loop: the same FP32c batch with the host reading the
+    convergence flag every iteration. Plain: each case alone, FP64, eager.
+    ``warm`` untimed steps, then ``timed`` steps; iterations are summed over
+    the timed steps and split by case subset: converged on both the fast and
+    the plain path at every timed step, and the rest (stations past the
+    synthetic polar's stall, whose relaxed iteration does not settle)."""
     synth = importlib.import_module("winds-master_b200.synth")
     wake = importlib.import_module("winds-master_b200.wake")
+    gi = importlib.import_module("winds-master_b200.gamma_init")
     kjs = [synth.make_kj_case(rc, nsteps=c["nsteps"], t0=c["t0"]) for rc, c in zip(rcases, cases)]
-    b = wake.WakeBatch(cases, integrator="pcc", precision="f32c")
-    b.set_kj(kjs, relax=relax, tol=tol, maxiter=maxiter)
-    b.step(1, graph=True)
-    b.step(1, graph=True)
-    ms = b.stats()[0]
-    it_f = b.kj_stats()[0].copy()
-    T_f = b.loads()[0].copy()
-    G_f = [b.bound(k) for k in range(len(cases))]
-    b.close()
-    # the same FP32c batch with the host driving the iteration (a 4-byte
-    # convergence flag read back after every iteration, no graphs)
-    h = wake.WakeBatch(cases, integrator="pcc", precision="f32c")
-    h.set_kj(kjs, relax=relax, tol=tol, maxiter=maxiter)
-    h.step(1)
-    h.step(1)
-    ms_host = h.stats()[0]
-    h.close()
-    plain_ms, it_p, T_p, G_p = 0.0, [], [], []
-    for c, kj in zip(cases, kjs):
-        p = wake.WakeBatch([c], integrator="pcc", precision="f64")
-        p.set_kj([kj], relax=relax, tol=tol, maxiter=maxiter)
-        p.step(1)
-        p.step(1)
-        plain_ms += p.stats()[0]
-        it_p.append(int(p.kj_stats()[0][0]))
-        T_p.append(float(p.loads()[0][0]))
-        G_p.append(p.bound(0))
-        p.close()
-    it_p = np.array(it_p)
-    both = (it_f < maxiter) & (it_p < maxiter)
-    dT = np.abs(T_f - np.array(T_p)) / np.abs(np.array(T_p))
-    dG = [float(np.abs(gf - gp).max() / np.abs(gp).max()) for gf, gp in zip(G_f, G_p)]
-    return {"tol": tol, "relax": relax, "maxiter": maxiter,
-            "steps_per_s": 1000.0 / ms, "ms_per_step": ms,
-            "host_loop_steps_per_s": 1000.0 / ms_host,
-            "plain_fp64_steps_per_s": 1000.0 / plain_ms, "speedup_vs_plain_fp64": plain_ms / ms,
-            "kj_iterations_fast": int(it_f.sum()), "kj_iterations_plain": int(it_p.sum()),
-            "converged_fast": float(np.mean(it_f < maxiter)),
-            "converged_plain": float(np.mean(it_p < maxiter)),
-            "thrust_rel_diff_max": float(dT[both].max()) if both.any() else None,
-            "bound_rel_diff_max": float(np.max(np.array(dG)[both])) if both.any() else None}
+    n = len(cases)
+
+    def run(prec, graph, net=None, one=None):
+        sel = range(n) if one is None else [one]
+        b = wake.WakeBatch([cases[k] for k in sel], integrator="pcc", precision=prec)
+        b.set_kj([kjs[k] for k in sel], relax=relax, tol=tol, maxiter=maxiter)
+        if net is not None:
+            b.set_mlp(net)
+        for _ in range(warm):
+            b.step(1, graph=graph)
+        its, ms, evals = 0, 0.0, 0
+        capped = np.zeros(len(sel), dtype=bool)
+        for _ in range(timed):
+            b.step(1, graph=graph)
+            ms += b.stats()[0]
+            it, _, ev = b.kj_stats()
+            its = its + it.astype(np.int64)
+            capped |= it >= maxiter
+            evals += ev
+        out = dict(ms=ms / timed, iters=its, evals=evals, capped=capped, T=b.loads()[0].copy(),
+                   G=[b.bound(k) for k in range(len(sel))])
+        b.close()
+        return out
+
+    fast = run("f32c", True)
+    host = run("f32c", False)
+    plain = dict(ms=0.0, iters=[], T=[], G=[], capped=[])
+    for k in range(n):
+        r = run("f64", False, one=k)
+        plain["ms"] += r["ms"]
+        plain["iters"].append(int(r["iters"][0]))
+        plain["T"].append(float(r["T"][0]))
+        plain["G"].append(r["G"][0])
+        plain["capped"].append(bool(r["capped"][0]))
+    it_f, it_p = fast["iters"], np.array(plain["iters"])
+    # cases whose every timed step converged on both paths
+    conv = ~fast["capped"] & ~np.array(plain["capped"])
+    dT = np.abs(fast["T"] - np.array(plain["T"])) / np.abs(np.array(plain["T"]))
+    dG = np.array([float(np.abs(gf - gp).max() / np.abs(gp).max()) for gf, gp in zip(fast["G"], plain["G"])])
+    out = {"tol": tol, "relax": relax, "maxiter": maxiter, "warm_steps": warm, "timed_steps": timed,
+           "steps_per_s": 1000.0 / fast["ms"], "ms_per_step": fast["ms"],
+           "host_loop_steps_per_s": 1000.0 / host["ms"],
+           "plain_fp64_steps_per_s": 1000.0 / plain["ms"], "speedup_vs_plain_fp64": plain["ms"] / fast["ms"],
+           "kj_iterations_fast": int(it_f.sum()), "kj_iterations_plain": int(it_p.sum()),
+           "converged_cases": int(conv.sum()), "stalled_cases": int((~conv).sum()),
+           "converged_subset": {
+               "kj_iterations_fast": int(it_f[conv].sum()), "kj_iterations_plain": int(it_p[conv].sum()),
+               "iterations_ratio_fast_over_plain": float(it_f[conv].sum() / max(it_p[conv].sum(), 1)),
+               "cases_iterations_equal": int((it_f[conv] == it_p[conv]).sum()),
+               "thrust_rel_diff_max": float(dT[conv].max()) if conv.any() else None,
+               "bound_rel_diff_max": float(dG[conv].max()) if conv.any() else None},
+           "stalled_subset": {"kj_iterations_fast": int(it_f[~conv].sum()),
+                              "kj_iterations_plain": int(it_p[~conv].sum())}}
+    # start-value arms on the fast path
+    arms = {"previous": fast}
+    xo = gi.extrapolation_only()
+    arms["extrapolated"] = run("f32c", True, net=xo)
+    xo.close()
+    if mlp is not None:
+        arms["network"] = run("f32c", True, net=mlp)
+    ref = arms["previous"]
+    out["start_value_arms"] = {}
+    for name, r in arms.items():
+        ok = conv & ~r["capped"]
+        dTa = np.abs(r["T"] - ref["T"]) / np.abs(ref["T"])
+        out["start_value_arms"][name] = {
+            "kj_iterations_converged_subset": int(r["iters"][conv].sum()),
+            "lifting_line_evaluations": int(r["evals"]), "steps_per_s": 1000.0 / r["ms"],
+            "thrust_rel_diff_vs_previous_max": float(dTa[ok].max()) if ok.any() else None}
+    return out
 
 
 # ------------------------------------------------------------------ start value
@@ -341,24 +448,37 @@ def kj_mlp_bench():
     """Learned Kutta-Joukowski start value: pairs from the plain solver on the
     attached-flow points among 800 seeded operating points (U 5-25 m/s, pitch
     0-15 deg, yaw 0-30 deg, TSR 5-9, 10 deg steps), trained on the GPU, then
-    iterations with and without it at tol 1e-6 on held-out points."""
+    the iteration from the previous step's circulation, from its
+    extrapolation alone and from the network on held-out points at tol 1e-6,
+    and the converged results of the starts at tol 1e-6 and 1e-10."""
     gi = importlib.import_module("winds-master_b200.gamma_init")
     r = gi.study(n_train=800, n_test=120, epochs=60)
     r.pop("model").close()
-    return {k: (round(v, 6) if isinstance(v, float) else v) for k, v in r.items()}
+
+    def rnd(v):
+        if isinstance(v, float):
+            return round(v, 6)
+        if isinstance(v, dict):
+            return {k: rnd(x) for k, x in v.items()}
+        return v
+    return rnd(r)
 
 
 # ------------------------------------------------------------------ end to end
-def e2e_run_bench(steps, ncases=16, ages=1440, seed=5):
+def e2e_run_bench(steps, ncases=16, ages=1440, seed=5, plain_cases=4):
     """16 rotor cases, 3 blades x 41 nodes, wake truncated at 1440 steps of
     1 deg, U = 11.4 m/s, shear 0.2, yaw 0-30 deg, pcc with the lifting-line
-    iteration (tol 1e-6) and rotor loads every step: the FP32-compensated
-    batch with graph replay and the MLP start value on the previous-step base
-    (trained here on plain-solver pairs of the same conditions with 120-step
-    wakes, its output scale chosen on validation runs that must keep the
-    reference start's fixed point) against the
-    plain FP64 path (FP64 direct sum, previous-step start, no graphs).
-    Thrust and power histories are compared step by step."""
+    iteration (tol 1e-6) and rotor loads every step, ``steps`` steps per path.
+    Fast: the FP32-compensated batch with graph replay, started from the
+    network (previous-step base, trained here on plain-solver pairs of the
+    same conditions with 120-step wakes, its output scale chosen on
+    validation runs that must keep the reference start's fixed point), from
+    the previous step's circulation, and from its extrapolation alone.
+    Plain FP64 (FP64 direct sum, previous-step start, each case alone, no
+    graphs) runs ``plain_cases`` of the 16 cases (every 16/plain_cases-th:
+    the same size as every other case, so its time per case scales to the
+    batch) for the same steps; thrust and power histories are compared step
+    by step on those cases."""
     synth = importlib.import_module("winds-master_b200.synth")
     wake = importlib.import_module("winds-master_b200.wake")
     gi = importlib.import_module("winds-master_b200.gamma_init")
@@ -373,7 +493,7 @@ def e2e_run_bench(steps, ncases=16, ages=1440, seed=5):
 
     t0 = time.perf_counter()
     tr = gi.run(points(120, rng.uniform(0.0, 30.0, 64), 900), 48, record=True, maxiter=200)
-    keep = tr["step_case"][:, 0] >= 4
+    keep = (tr["step_case"][:, 0] >= 4) & tr["lift"]
     # the previous-step base: these cases have stations past stall, where a
     # start far from the reference's can select another fixed point
     m, _ = gi.train(tr["X"][keep], tr["dG"][keep], epochs=40, base="previous")
@@ -383,42 +503,81 @@ def e2e_run_bench(steps, ncases=16, ages=1440, seed=5):
     train_s = time.perf_counter() - t0
     pts = points(ages, yaws, 100)
     cases, kjs = gi.build(pts, steps + 1)
+    sub = list(range(0, ncases, ncases // plain_cases))
+    xo = gi.extrapolation_only()
     out = {}
-    for name, prec, mlp, graph in (("fast", "f32c", m, True), ("plain_fp64", "f64", None, False)):
-        b = wake.WakeBatch(cases, integrator="pcc", precision=prec)
-        b.set_kj(kjs, relax=0.3, tol=1e-6, maxiter=200)
-        if mlp is not None:
-            b.set_mlp(mlp)
+    for name, prec, mlp, graph, sel in (("fast", "f32c", m, True, None),
+                                        ("fast_previous_start", "f32c", None, True, None),
+                                        ("fast_extrapolated_start", "f32c", xo, True, None),
+                                        ("plain_fp64", "f64", None, False, sub)):
+        idx = list(range(ncases)) if sel is None else sel
         T, P, its, ms = [], [], [], []
+        if sel is None:
+            batches = [wake.WakeBatch([cases[k] for k in idx], integrator="pcc", precision=prec)]
+            batches[0].set_kj([kjs[k] for k in idx], relax=0.3, tol=1e-6, maxiter=200)
+            if mlp is not None:
+                batches[0].set_mlp(mlp)
+        else:  # each case alone
+            batches = []
+            for k in idx:
+                b = wake.WakeBatch([cases[k]], integrator="pcc", precision=prec)
+                b.set_kj([kjs[k]], relax=0.3, tol=1e-6, maxiter=200)
+                batches.append(b)
         for s in range(steps):
-            b.step(1, graph=graph)
-            t_, _, p_ = b.loads()
-            T.append(t_)
-            P.append(p_)
-            its.append(int(b.kj_stats()[0].sum()))
-            ms.append(b.stats()[0])
-        inter = b.stats()[1]
-        b.close()
-        out[name] = dict(T=np.array(T), P=np.array(P), iters=its, ms=ms, inter=inter)
+            t_row, p_row, it_row, ms_s = [], [], [], 0.0
+            for b in batches:
+                b.step(1, graph=graph)
+                t_, _, p_ = b.loads()
+                t_row += list(t_)
+                p_row += list(p_)
+                it_row += list(b.kj_stats()[0])
+                ms_s += b.stats()[0]
+            T.append(t_row)
+            P.append(p_row)
+            its.append(int(np.sum(it_row)))
+            ms.append(ms_s)
+        inter = sum(b.stats()[1] for b in batches)
+        for b in batches:
+            b.close()
+        out[name] = dict(T=np.array(T), P=np.array(P), iters=its, ms=ms, inter=inter, idx=idx)
     m.close()
+    xo.close()
     f, p = out["fast"], out["plain_fp64"]
-    relT = np.abs(f["T"] - p["T"]) / np.abs(p["T"])
-    relP = np.abs(f["P"] - p["P"]) / np.maximum(np.abs(p["P"]), 1e-9 * np.abs(p["T"]))
-    fast_ms, plain_ms = statistics.mean(f["ms"]), statistics.mean(p["ms"])
+
+    def rel(x, y, idx):
+        a, b_ = x["T"][:, idx], y["T"]
+        c, d = x["P"][:, idx], y["P"]
+        return (float((np.abs(a - b_) / np.abs(b_)).max()),
+                float((np.abs(c - d) / np.maximum(np.abs(d), 1e-9 * np.abs(b_))).max()))
+    relT, relP = rel(f, p, p["idx"])
+    fast_ms = statistics.mean(f["ms"])
+    plain_ms = statistics.mean(p["ms"]) * ncases / len(p["idx"])
+    arms = {}
+    for name in ("fast", "fast_previous_start", "fast_extrapolated_start"):
+        a = out[name]
+        tT, tP = rel(a, p, p["idx"])
+        dT = np.abs(a["T"] - out["fast_previous_start"]["T"]) / np.abs(out["fast_previous_start"]["T"])
+        arms[name] = {"steps_per_s": 1000.0 / statistics.mean(a["ms"]), "kj_iterations": a["iters"],
+                      "kj_iterations_total": int(sum(a["iters"])),
+                      "thrust_rel_diff_vs_plain_max": tT, "power_rel_diff_vs_plain_max": tP,
+                      "thrust_rel_diff_vs_previous_start_max": float(dT.max())}
     return {"cases": ncases, "nodes_per_case": 41 * (ages + 1) * 3,
             "filaments_per_case": (40 * (ages + 1) + 41 * ages) * 3, "steps": steps,
             "steps_per_s": 1000.0 / fast_ms, "plain_fp64_steps_per_s": 1000.0 / plain_ms,
+            "plain_fp64_cases_run": len(p["idx"]),
             "speedup_vs_plain_fp64": plain_ms / fast_ms,
             "interactions_per_step": f["inter"],
-            "kj_iterations_fast": f["iters"], "kj_iterations_plain": p["iters"],
-            "thrust_rel_diff_max": float(relT.max()), "power_rel_diff_max": float(relP.max()),
+            "kj_iterations_fast": f["iters"], "kj_iterations_plain_on_subset": p["iters"],
+            "thrust_rel_diff_max": relT, "power_rel_diff_max": relP,
+            "start_value_arms": arms,
             "thrust_history_N": f["T"].sum(1).round(1).tolist(),
             "power_history_W": f["P"].sum(1).round(1).tolist(),
             "mlp_training_s": round(train_s, 2), "mlp_base": mlp_base, "mlp_output_shrink": mlp_shrink,
             "mlp_validation": mlp_val,
-            "timing": "CUDA events around each step "
-            "(fast path: the lifting-line loop runs inside the step's graph; plain path: the "
-            "host waits on a per-iteration convergence flag)"}
+            "timing": "CUDA events around each step (fast paths: the lifting-line loop runs inside "
+            "the step's graph; plain path: the host waits on a per-iteration convergence flag, its "
+            f"time per step measured on {len(p['idx'])} of the {ncases} equal-size cases and scaled "
+            "to all of them)"}
 
 
 # ------------------------------------------------------------------ our arm
@@ -563,7 +722,13 @@ def ours(args):
     # would wait at the final barrier for minutes, past the group's timeout
     wake_line = None
     if rank == 0 and world == 1 and args.wake_steps > 0 and not args.quick:
-        wake_line = wake_bench(args)
+        net = batch_start_value() if not args.no_studies else None
+        wake_line = wake_bench(args, mlp=net)
+        if net is not None:
+            net.close()
+    sharded_line = None
+    if world > 1 and args.wake_steps > 0 and not args.quick:
+        sharded_line = sharded_wake_bench(args, rank, world)
     mlp_line = e2e_line_run = None
     if rank == 0 and world == 1 and not (args.quick or args.no_studies):
         mlp_line = kj_mlp_bench()
@@ -575,12 +740,7 @@ def ours(args):
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic",
-            "config": {"workload": f"helical wake 3x41x{720 if args.workload == 'large' else 180} (1 deg), "
-                       "Vatistas n=2, all shed+trailing filaments onto all wake nodes + lifting-line "
-                       "points", "targets": nt,
-                       "filaments": nf, "interactions_per_step": interactions,
-                       "l2": "256 MB buffer written between timed steps",
-                       "parallelism": f"replicated wakes x{world}" if world > 1 else "single GPU"},
+            "config": bench_config(args.workload, nt, nf, world),
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                          "frac": achieved / peak.value if peak.value else None, "traffic": traffic,
                          "peak_source": "FFMA probe measured in this run (winds_bs_fp32_peak)",
@@ -597,6 +757,7 @@ def ours(args):
             "tiling": dict(zip(("targets_per_thread", "filaments_per_tile", "waves"),
                                wb.get_tuning(core, nt, nf))),
             "wake_batch": wake_line,
+            "wake_batch_sharded": sharded_line,
             "kj_start_value": mlp_line,
             "e2e_run": e2e_line_run,
         }

@@ -197,10 +197,14 @@ int winds_wake_get_perf(winds_wake_batch *b, int icase, double *cl, double *cd, 
  * (3 components: vblade at the step plus the previous step's induced
  * velocity at the lifting line, transformed as kj() does), previous bound
  * circulation, its change over the previous step; the start value is
- * Gamma_prev + out_scale * network(features). The network must have 10 inputs
- * and live on the batch's device; the iteration and its tolerance are
- * unchanged. No reference counterpart (WInDS.m:131 always starts from the
- * previous step). */
+ * Gamma_prev + out_scale * network(features) (on the extrapolated base:
+ * Gamma_prev + its change + out_scale * network) at stations whose airfoil
+ * table has lift, and Gamma_prev at the others (e.g. cylinder root sections:
+ * Cl = 0 at every AoA, so their fixed point is Gamma = 0, and the relaxed
+ * iteration damps a start error there by only 1 - relax per iteration).
+ * The network must have 10 inputs and live on the batch's device; the
+ * iteration and its tolerance are unchanged. No reference counterpart
+ * (WInDS.m:131 always starts from the previous step). */
 struct winds_mlp;
 int winds_wake_set_mlp(winds_wake_batch *b, struct winds_mlp *m);
 

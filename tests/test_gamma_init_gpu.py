@@ -19,7 +19,15 @@ def _mods():
     return gi, mlp, wake, synth
 
 
+def _lift(gi, kj, nb):
+    """[ns*nb] row mask of the stations the start value applies to."""
+    return np.tile(gi.lifting_stations(kj), nb)
+
+
 def test_features_and_start_value_match_host(wb):
+    """Device features equal the host's; the start value is Gamma_prev +
+    out_scale * network at lifting stations and Gamma_prev at the others
+    (the cylinder root sections, whose table has no lift)."""
     gi, mlp, wake, synth = _mods()
     pts = gi.operating_points(3, seed=7, nst=13, wake_steps=10)
     cases, kjs = gi.build(pts, 4)
@@ -36,7 +44,9 @@ def test_features_and_start_value_match_host(wb):
         xh = synth.kj_features(kjs[k], 0, prev[k])
         np.testing.assert_allclose(x, xh, rtol=2e-6, atol=1e-6)
         g = b.kj_guess(k)
-        gh = prev[k].ravel(order="F") + float(np.float32(0.7)) * m.forward(x).astype(np.float64)
+        lift = _lift(gi, kjs[k], cases[k]["nb"])
+        assert lift.any() and not lift.all()
+        gh = prev[k].ravel(order="F") + lift * float(np.float32(0.7)) * m.forward(x).astype(np.float64)
         np.testing.assert_allclose(g.ravel(order="F"), gh, rtol=1e-12, atol=1e-9)
     # later steps carry the change of the converged circulation
     prev1 = [b.bound(k) for k in range(3)]
@@ -69,8 +79,9 @@ def test_extrapolated_base_start_value(wb):
         b.step(1, graph=True)
         for k in range(3):
             x = b.kj_features(k)
-            gh = ((prev[k].ravel(order="F") + x[:, 9].astype(np.float64))
-                  + float(np.float32(0.05)) * m.forward(x).astype(np.float64))
+            lift = _lift(gi, kjs[k], cases[k]["nb"])
+            gh = prev[k].ravel(order="F") + lift * (
+                x[:, 9].astype(np.float64) + float(np.float32(0.05)) * m.forward(x).astype(np.float64))
             np.testing.assert_allclose(b.kj_guess(k).ravel(order="F"), gh, rtol=1e-12, atol=1e-9)
     xo = gi.extrapolation_only()
     b.set_mlp(xo)
@@ -78,8 +89,10 @@ def test_extrapolated_base_start_value(wb):
     b.step(1)
     for k in range(3):
         x = b.kj_features(k)
+        lift = _lift(gi, kjs[k], cases[k]["nb"])
         np.testing.assert_array_equal(b.kj_guess(k).ravel(order="F"),
-                                      prev[k].ravel(order="F") + x[:, 9].astype(np.float64))
+                                      np.where(lift, prev[k].ravel(order="F") + x[:, 9].astype(np.float64),
+                                               prev[k].ravel(order="F")))
     b.close()
     m.close()
     xo.close()
@@ -110,7 +123,8 @@ def test_graph_with_network_matches_host_loop(wb):
     b.step(1, graph=True)
     for k in range(3):
         x = b.kj_features(k)
-        gh = prev[k].ravel(order="F") + float(np.float32(0.3)) * m.forward(x).astype(np.float64)
+        lift = _lift(gi, kjs[k], cases[k]["nb"])
+        gh = prev[k].ravel(order="F") + lift * float(np.float32(0.3)) * m.forward(x).astype(np.float64)
         np.testing.assert_allclose(b.kj_guess(k).ravel(order="F"), gh, rtol=1e-12, atol=1e-9)
     b.close()
     m.close()

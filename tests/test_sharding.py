@@ -31,39 +31,96 @@ def test_partition_covers_every_case_once_and_balances(synth):
     assert sorted(i for p in parts for i in p) == [0, 1, 2]
 
 
-def _worker(rank, world, port, costs, q):
+class OracleStepper:
+    """The FP64 step oracle with the lifting line and loads (oracle/kj_ref.py)
+    in place of the device batch: one KJWakeRef per case of this rank."""
+
+    def __init__(self, cases, kjs, **kw):
+        import kj_ref
+        import wake_ref
+        self.refs = [kj_ref.KJWakeRef(wake_ref.WakeCaseRef(**{k: c[k] for k in
+                                                               wake_ref.WakeCaseRef.__dataclass_fields__}),
+                                      kj, integrator="pcc", relax=0.3, tol=1e-6, maxiter=60)
+                     for c, kj in zip(cases, kjs)]
+
+    def step(self, graph=True):
+        for r in self.refs:
+            r.step()
+
+    def values(self):
+        return np.array([[r.T, r.Q, r.P, float(r.kj_iters)] for r in self.refs])
+
+    def close(self):
+        pass
+
+
+def _small_cases(n, seed=4):
+    import importlib
+    synth = importlib.import_module("winds-master_b200.synth")
+    rcs = synth.batch_cases(n, seed=seed, steps_range=(5, 9), nodes_range=(7, 9))
+    cases = [synth.make_wake_case(rc, nsteps=4) for rc in rcs]
+    kjs = [synth.make_kj_case(rc, nsteps=4, t0=c["t0"]) for rc, c in zip(rcs, cases)]
+    return cases, kjs
+
+
+def _run_worker(rank, world, port, ncases, steps, q):
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    for p in (root, os.path.join(root, "oracle"), os.path.join(root, "tests")):
+        sys.path.insert(0, p)
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
                       WORLD_SIZE=str(world))
     import datetime
     import torch.distributed as dist
-    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
     try:
+        from test_sharding import OracleStepper, _small_cases
         sh = _mod()
-        parts = sh.partition(costs, world)
-        # each rank "steps" its own cases: per-case values computed locally
-        local = [[float(i), float(costs[i]) * 2.0] for i in parts[rank]]
-        full = sh.gather_case_values(local, parts, rank, world)
-        q.put((rank, full.tolist()))
+        cases, kjs = _small_cases(ncases)
+        run = sh.ShardedRun(cases, kjs, rank=rank, world=world, stepper=OracleStepper)
+        hist = [run.step().tolist() for _ in range(steps)]
+        q.put((rank, run.mine, [len(x.refs) for x in [run.local] if x is not None], hist))
+        run.close()
     finally:
         dist.destroy_process_group()
 
 
-def test_gloo_two_ranks_gather_in_case_order():
-    import sys
-    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
-    costs = [5, 3, 9, 1, 7, 2, 8]
+def _spawn(world, ncases, steps):
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
         port = s.getsockname()[1]
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    procs = [ctx.Process(target=_worker, args=(r, 2, port, costs, q)) for r in range(2)]
+    procs = [ctx.Process(target=_run_worker, args=(r, world, port, ncases, steps, q))
+             for r in range(world)]
     for p in procs:
         p.start()
-    res = [q.get(timeout=120) for _ in range(2)]
+    res = sorted(q.get(timeout=300) for _ in range(world))
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    want = [[float(i), 2.0 * c] for i, c in enumerate(costs)]
-    for _, full in res:
-        assert full == want
+    return res
+
+
+def test_sharded_steps_match_a_single_rank_run():
+    """Two gloo ranks each step their own cases (FP64 step oracle with the
+    lifting line and loads); the gathered thrust, torque, power and iteration
+    counts of every case, every step, equal those of one rank stepping all
+    cases, on both ranks. A third layout puts more ranks than cases: the empty
+    rank still takes part in every gather."""
+    sh = _mod()
+    cases, kjs = _small_cases(5)
+    one = sh.ShardedRun(cases, kjs, rank=0, world=1, stepper=OracleStepper)
+    want = [one.step().tolist() for _ in range(3)]
+    res = _spawn(2, 5, 3)
+    parts = sh.partition([sh.case_cost(c) for c in cases], 2)
+    for rank, mine, local_n, hist in res:
+        assert mine == parts[rank] and local_n == [len(parts[rank])]
+        assert hist == want
+    assert sorted(res[0][1] + res[1][1]) == list(range(5))
+    few = _spawn(3, 2, 1)
+    assert sum(len(m) for _, m, _, _ in few) == 2 and any(not m for _, m, _, _ in few)
+    one2 = sh.ShardedRun(*_small_cases(2), rank=0, world=1, stepper=OracleStepper)
+    ref2 = one2.step().tolist()
+    for _, _, _, hist in few:
+        assert hist == [ref2]

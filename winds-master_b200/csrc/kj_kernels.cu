@@ -126,17 +126,22 @@ __global__ void kj_features(const WakeCase *cases, const KJCase *kc, const int *
 }
 
 // bound = base + out_scale * y, base Gamma_prev or, with *base != 0, its
-// extrapolation Gamma_prev + dGamma_prev (feature 9 of the row).
+// extrapolation Gamma_prev + dGamma_prev (feature 9 of the row). Stations
+// whose airfoil table has no lift (st_lift 0: Cl = 0 at every AoA, e.g. the
+// cylinder root sections) keep Gamma_prev: their fixed point is Gamma = 0,
+// the previous step already sits there, and the relaxed iteration damps any
+// start error at such a station only by (1 - relax) per iteration.
 // Nothing before the step the iteration starts at (WakeCase::kj_from).
 __global__ void kj_apply_guess(const WakeCase *cases, const KJCase *kc, const int *step,
-                               const float *y, const float *out_scale, const float *feat,
-                               const float *base, double *bound) {
+                               const int *st_lift, const float *y, const float *out_scale,
+                               const float *feat, const float *base, double *bound) {
   const WakeCase c = cases[blockIdx.y];
   const KJCase k = kc[blockIdx.y];
   const int ns = c.nst - 1;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ns * c.nb || *step < c.kj_from) return;
   const int i = t % ns, b = t / ns;
+  if (!st_lift[k.station_off + i]) return;
   double g = bound[c.bound_off + i + (long long)ns * b];
   if (*base != 0.f) g += (double)feat[(k.t_off + t) * kKJFeatures + 9];
   bound[c.bound_off + i + (long long)ns * b] = g + (double)*out_scale * (double)y[k.t_off + t];
@@ -303,11 +308,11 @@ cudaError_t launch_kj_features(const WakeCase *cases, const KJCase *kc, int ncas
 }
 
 cudaError_t launch_kj_apply_guess(const WakeCase *cases, const KJCase *kc, int ncases, int max_st,
-                                  const int *step, const float *y, const float *out_scale,
-                                  const float *feat, const float *base, double *bound,
-                                  cudaStream_t s) {
-  kj_apply_guess<<<dim3((max_st + 127) / 128, ncases), 128, 0, s>>>(cases, kc, step, y, out_scale,
-                                                                    feat, base, bound);
+                                  const int *step, const int *st_lift, const float *y,
+                                  const float *out_scale, const float *feat, const float *base,
+                                  double *bound, cudaStream_t s) {
+  kj_apply_guess<<<dim3((max_st + 127) / 128, ncases), 128, 0, s>>>(cases, kc, step, st_lift, y,
+                                                                    out_scale, feat, base, bound);
   return cudaGetLastError();
 }
 

@@ -80,6 +80,7 @@ struct winds_wake_batch {
   bool loads = false;           // every case gave the loads inputs
   DevBuf st_rr, st_dr, rpm, pitch, dl, loads_out;
   DevBuf st_r, st_c, st_tw, azim, guess, feat, bound_last;
+  DevBuf st_lift;  // per station: 1 when its airfoil table has lift (start value applies)
   winds_mlp *mlp = nullptr;
   MlpWork mw;
   cudaGraphExec_t exec_pre = nullptr, exec_kj = nullptr, exec_post = nullptr;
@@ -469,7 +470,8 @@ cudaError_t enqueue_kj_begin(winds_wake_batch *b) {
       e = cudaErrorLaunchFailure;
     if (e == cudaSuccess)
       e = launch_kj_apply_guess(cd, kd, b->ncases, b->max_st, P<const int>(b->step_d),
-                                P<const float>(b->mw.y), mlp_out_scale_dev(b->mlp),
+                                P<const int>(b->st_lift), P<const float>(b->mw.y),
+                                mlp_out_scale_dev(b->mlp),
                                 P<const float>(b->feat), mlp_base_dev(b->mlp), P<double>(b->bound),
                                 s);
   }
@@ -1075,7 +1077,7 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
   b->kjc.clear();
   long long fr = 0, tt = 0, st = 0, tab = 0, az = 0, rp = 0;
   bool all_inputs = true, have_twist = true, all_loads = true, any_pitch = false;
-  std::vector<int> foil_off, foils;
+  std::vector<int> foil_off, foils, lift;
   std::vector<double> aoa, cl, cd, chord;
   b->max_st = 0;
   b->max_bound_cols = 0;
@@ -1112,10 +1114,17 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
       cl.push_back(h.cl[j]);
       cd.push_back(h.cd[j]);
     }
+    // tables with lift (some Cl != 0); a station on a table without keeps its
+    // previous circulation as the start value
+    std::vector<int> has_lift(h.n_foils, 0);
+    for (int f = 0, j = 0; f < h.n_foils; ++f)
+      for (int e = 0; e < h.foil_points[f]; ++e, ++j)
+        if (h.cl[j] != 0.0) has_lift[f] = 1;
     for (int i = 0; i < ns; ++i) {
       if (h.foil[i] < 0 || h.foil[i] >= h.n_foils)
         return fail(WINDS_BS_ERR_ARG, "case %d: station %d uses airfoil %d of %d", k, i, h.foil[i], h.n_foils);
       foils.push_back(h.foil[i]);
+      lift.push_back(has_lift[h.foil[i]]);
       chord.push_back(h.chord[i]);
     }
     tab += o;
@@ -1134,6 +1143,7 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
     if ((rc = x->ensure(fr * sizeof(double), s))) return rc;
   if ((rc = b->kjc_d.ensure(b->ncases * sizeof(KJCase), s)) ||
       (rc = b->chord.ensure(st * sizeof(double), s)) || (rc = b->foil.ensure(st * sizeof(int), s)) ||
+      (rc = b->st_lift.ensure(st * sizeof(int), s)) ||
       (rc = b->foil_off.ensure(foil_off.size() * sizeof(int), s)) ||
       (rc = b->aoa_t.ensure(tab * sizeof(double), s)) || (rc = b->cl_t.ensure(tab * sizeof(double), s)) ||
       (rc = b->cd_t.ensure(tab * sizeof(double), s)) || (rc = b->tp_ll.ensure(tt * sizeof(double4), s)) ||
@@ -1228,6 +1238,7 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
   for (long long i = 0; i < tt; ++i) ident[i] = (int)i;
   if (e == cudaSuccess) e = cudaMemcpy(b->chord.p, chord.data(), st * sizeof(double), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(b->foil.p, foils.data(), st * sizeof(int), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->st_lift.p, lift.data(), st * sizeof(int), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(b->foil_off.p, foil_off.data(), foil_off.size() * sizeof(int), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(b->aoa_t.p, aoa.data(), tab * sizeof(double), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(b->cl_t.p, cl.data(), tab * sizeof(double), cudaMemcpyHostToDevice);
@@ -1385,6 +1396,7 @@ void winds_wake_destroy(winds_wake_batch *b) {
     if (x) cudaGraphDestroy(x);
   if (b->body_stream) cudaStreamDestroy(b->body_stream);
   b->kj_it.release();
+  b->st_lift.release();
   for (DevBuf *x : {&b->kjc_d, &b->ll, &b->bxn, &b->byn, &b->bzn, &b->vblade, &b->chord, &b->foil,
                     &b->foil_off, &b->aoa_t, &b->cl_t, &b->cd_t, &b->tp_ll, &b->perm_ll, &b->uindb,
                     &b->kj_groups, &b->kj_tiles, &b->kj_items, &b->kj_order, &b->kj_part,

@@ -24,7 +24,11 @@ Features (device-computed, ``winds_wake_get_kj_features``): r/R, chord/R,
 twist, sin and cos of the azimuth, the local inflow in the blade frame
 (kinematic inflow plus the previous step's induced velocity at the lifting
 line), the previous bound circulation and its change over the previous step.
-Training pairs come only from (case, step) whose plain iteration converged.
+Training pairs come only from (case, step) whose plain iteration converged,
+and only from lifting stations: a station whose airfoil table has no lift
+(the cylinder root sections) converges to Gamma = 0, the engine keeps its
+previous value as the start, and any other start there costs iterations
+(the relaxed iteration damps it by only 1 - relax per iteration).
 """
 from __future__ import annotations
 
@@ -65,23 +69,33 @@ def operating_points(n: int, seed: int, nst: int = 41, wake_steps: int = 36,
     return out
 
 
-def build(points, run_steps: int):
+def lifting_stations(kj: dict) -> np.ndarray:
+    """[ns] bool: the stations whose airfoil table has some Cl != 0 (the
+    stations the engine's start value applies to)."""
+    offs = np.concatenate([[0], np.cumsum(kj["foil_points"])])
+    lift = np.array([np.any(np.asarray(kj["cl"])[offs[f]:offs[f + 1]] != 0.0)
+                     for f in range(len(kj["foil_points"]))])
+    return lift[np.asarray(kj["foil"])]
+
+
+def build(points, run_steps: int, root_cut: float = ROOT_CUT):
     """Wake and lifting-line inputs of every point for ``run_steps`` steps."""
     cases, kjs = [], []
     for p in points:
         cases.append(synth.make_wake_case(p.case, nsteps=run_steps + 1, pitch_deg=p.pitch_deg))
         kjs.append(synth.make_kj_case(p.case, nsteps=run_steps + 1, pitch_deg=p.pitch_deg,
-                                      root_cut=ROOT_CUT))
+                                      root_cut=root_cut))
     return cases, kjs
 
 
 def run(points, run_steps: int, relax=0.3, tol=1e-6, maxiter=100, mlp=None, precision="f32c",
-        record=False, graph=True):
+        record=False, graph=True, root_cut: float = ROOT_CUT):
     """Runs every point for ``run_steps`` pcc steps with the lifting line.
     Returns per-step, per-case iterations, the lifting-line evaluations per
     step (the batch iterates until its slowest case converged), the bound
-    circulation after every step and, with ``record``, the training pairs."""
-    cases, kjs = build(points, run_steps)
+    circulation, rotor thrust and power after every step and, with
+    ``record``, the training pairs."""
+    cases, kjs = build(points, run_steps, root_cut)
     b = WakeBatch(cases, integrator="pcc", precision=precision)
     b.set_kj(kjs, relax=relax, tol=tol, maxiter=maxiter)
     if mlp is not None:
@@ -91,14 +105,19 @@ def run(points, run_steps: int, relax=0.3, tol=1e-6, maxiter=100, mlp=None, prec
     aoa_max = np.zeros(n)
     iters = np.zeros((run_steps, n), dtype=np.int64)
     evals = np.zeros(run_steps, dtype=np.int64)
+    thrust = np.zeros((run_steps, n))
+    power = np.zeros((run_steps, n))
     bounds = []
-    X, dG, tag = [], [], []
+    X, dG, tag, lrows = [], [], [], []
+    nbs = [c["nb"] for c in cases]
+    lift_rows = [np.tile(lifting_stations(kj), nb) for kj, nb in zip(kjs, nbs)]
     t0 = time.perf_counter()
     for s in range(run_steps):
         b.step(1, graph=graph)
         it, _, ev = b.kj_stats()
         iters[s] = it
         evals[s] = ev
+        thrust[s], _, power[s] = b.loads()
         conv = [b.bound(k) for k in range(n)]
         for k in range(n):
             aoa = b.perf(k)[2]
@@ -110,14 +129,17 @@ def run(points, run_steps: int, relax=0.3, tol=1e-6, maxiter=100, mlp=None, prec
                     X.append(x)
                     dG.append(conv[k].ravel(order="F") - x[:, 8].astype(np.float64))
                     tag.append(np.full((x.shape[0], 2), (s, k), dtype=np.int32))
+                    lrows.append(lift_rows[k])
         bounds.append(conv)
     wall = time.perf_counter() - t0
     b.close()
-    out = dict(iters=iters, evals=evals, bounds=bounds, wall_s=wall, aoa_max=aoa_max)
+    out = dict(iters=iters, evals=evals, bounds=bounds, wall_s=wall, aoa_max=aoa_max,
+               thrust=thrust, power=power)
     if record:
         out["X"] = np.concatenate(X).astype(np.float32) if X else np.zeros((0, N_FEATURES), np.float32)
         out["dG"] = np.concatenate(dG).astype(np.float32) if dG else np.zeros(0, np.float32)
         out["step_case"] = np.concatenate(tag) if tag else np.zeros((0, 2), np.int32)
+        out["lift"] = np.concatenate(lrows) if lrows else np.zeros(0, bool)
     return out
 
 
@@ -219,23 +241,33 @@ def extrapolation_only():
 
 def study(n_train: int = 400, n_test: int = 120, train_steps: int = 42, test_steps: int = 30,
           skip: int = 4, epochs: int = 60, relax: float = 0.3, tol: float = 1e-6,
-          maxiter: int = 200, seed: int = 1, precision: str = "f32c", base: str = "extrapolated"):
+          maxiter: int = 200, seed: int = 1, precision: str = "f32c", base: str = "extrapolated",
+          weight_decay: float = 0.0, tight_points: int = 6, tight_steps: int = 10,
+          tight_tol: float = 1e-10):
     """Trains the start value on the attached-flow points among ``n_train``
     seeded candidates (pairs from steps >= ``skip``, past the start-up
     transient of the synthetic initial circulation) and compares the
     iteration with and without it on the attached points among ``n_test``
     other candidates; also the extrapolation alone (no network), so the
-    network's own share shows. Returns a dict of the measurements."""
+    network's own share shows (``arms``: previous-step start, extrapolation
+    alone, network, over the steps past the start-up that converged in all
+    three). Converged results: thrust, power and bound circulation of each
+    start against the previous-step start at the study's tolerance, and again
+    on ``tight_points`` test points at ``tight_tol`` -- the iteration's
+    stopping rule bounds the residual, not the distance to the fixed point,
+    so the differences must shrink with the tolerance when every start
+    reaches the same fixed point. Returns a dict of the measurements."""
     t0 = time.perf_counter()
     kw = dict(relax=relax, tol=tol, maxiter=maxiter, precision=precision)
     train_pts = attached(operating_points(n_train, seed=seed), **kw)
     d = run(train_pts, train_steps, record=True, **kw)
-    keep = d["step_case"][:, 0] >= skip
+    keep = (d["step_case"][:, 0] >= skip) & d["lift"]
     t1 = time.perf_counter()
     # pairs from most points; the rest validate the network's output scale
     n_val = max(1, len(train_pts) // 5)
     fit_rows = keep & (d["step_case"][:, 1] < len(train_pts) - n_val)
-    m, losses = train(d["X"][fit_rows], d["dG"][fit_rows], epochs=epochs, seed=seed, base=base)
+    m, losses = train(d["X"][fit_rows], d["dG"][fit_rows], epochs=epochs, seed=seed, base=base,
+                      weight_decay=weight_decay)
     choose_shrink(m, train_pts[-n_val:], test_steps, skip=skip, **kw)
     t2 = time.perf_counter()
     test_pts = attached(operating_points(n_test, seed=seed + 1), **kw)
@@ -256,8 +288,37 @@ def study(n_train: int = 400, n_test: int = 120, train_steps: int = 42, test_ste
     rel = [float(np.abs(np.asarray(x) - np.asarray(y)).max() / (np.abs(np.asarray(x)).max() + 1.0))
            for k, (x, y) in enumerate(zip(a["bounds"][-1], b["bounds"][-1])) if ok_case[k]]
     ms, nsteps = m.train_stats()
+
+    def loads_diff(x, y, mask):
+        dT = np.abs(x["thrust"] - y["thrust"]) / np.abs(y["thrust"])
+        dP = np.abs(x["power"] - y["power"]) / np.maximum(np.abs(y["power"]), 1e-9 * np.abs(y["thrust"]))
+        return (float(dT[mask].max()) if mask.any() else 0.0,
+                float(dP[mask].max()) if mask.any() else 0.0)
+
+    def arm(r):
+        return dict(iterations=int(r["iters"][all3].sum()), evals=int(r["evals"].sum()),
+                    converged=float((r["iters"] < maxiter).mean()))
+
+    arms = dict(previous=arm(a), extrapolated=arm(e), network=arm(b))
+    for name, r in (("extrapolated", e), ("network", b)):
+        arms[name]["thrust_rel_diff_max"], arms[name]["power_rel_diff_max"] = loads_diff(r, a, all3)
+    # the same comparison at a tight tolerance: every start must reach the same fixed point
+    tight = {}
+    if tight_points > 0 and test_pts:
+        kt = dict(kw, tol=tight_tol, maxiter=max(maxiter, 600))
+        pts_t = test_pts[:tight_points]
+        ta = run(pts_t, tight_steps, **kt)
+        tb = run(pts_t, tight_steps, mlp=m, **kt)
+        ok = (ta["iters"] < kt["maxiter"]) & (tb["iters"] < kt["maxiter"])
+        dT, dP = loads_diff(tb, ta, ok)
+        dGt = max(float(np.abs(np.asarray(x) - np.asarray(y)).max() / (np.abs(np.asarray(y)).max() + 1.0))
+                  for x, y in zip(tb["bounds"][-1], ta["bounds"][-1]))
+        tight = dict(tol=tight_tol, points=len(pts_t), steps=tight_steps,
+                     converged=float(ok.mean()), thrust_rel_diff_max=dT, power_rel_diff_max=dP,
+                     bound_rel_diff_max=dGt, iterations_previous=int(ta["iters"][ok].sum()),
+                     iterations_network=int(tb["iters"][ok].sum()))
     return dict(
-        model=m, train_points=len(train_pts), test_points=len(test_pts),
+        model=m, train_points=len(train_pts), test_points=len(test_pts), arms=arms, tight=tight,
         pairs=int(keep.sum()), loss_first=float(losses[0]), loss_last=float(losses[-1]),
         data_s=t1 - t0, train_s=t2 - t1, train_device_ms=ms, adam_steps=nsteps,
         iters_plain=int(ia[both].sum()), iters_mlp=int(ib[both].sum()),

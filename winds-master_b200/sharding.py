@@ -7,6 +7,13 @@ iteration counts) cross ranks, gathered on the host after the step. The
 split balances the per-step direct-sum work: greedy longest-processing-time
 assignment of each case's interactions per evaluation (nodes x filaments
 plus the lifting line), heaviest first, ties to the lowest rank.
+
+``ShardedRun`` is the driver: every rank builds the batch of its own cases
+(``partition(...)[rank]``) through a stepper factory -- ``BatchStepper`` (the
+device engine, ``wake.WakeBatch``) by default -- steps it, and after every
+step gathers thrust, torque, power and iteration counts of all cases in case
+order on every rank. A rank without cases (more ranks than cases) steps
+nothing and still joins every gather.
 """
 from __future__ import annotations
 
@@ -55,11 +62,77 @@ def gather_case_values(values_local, parts, rank: int, world: int, group=None):
     if world == 1:
         return local
     got = [None] * world
-    dist.all_gather_object(got, (rank, local.tolist()), group=group)
+    dist.all_gather_object(got, (rank, local.shape[1:], local.tolist()), group=group)
     n = sum(len(p) for p in parts)
-    first = np.asarray(got[0][1])
-    out = np.zeros((n,) + first.shape[1:], dtype=first.dtype if first.size else np.float64)
-    for r, vals in got:
+    tail = next((shp for _, shp, v in got if len(v)), local.shape[1:])
+    dtype = next((np.asarray(v).dtype for _, _, v in got if len(v)), np.float64)
+    out = np.zeros((n,) + tuple(tail), dtype=dtype)
+    for r, _, vals in got:
         for j, i in enumerate(parts[r]):
             out[i] = vals[j]
     return out
+
+
+class BatchStepper:
+    """The device engine for one rank's cases: a ``wake.WakeBatch`` (with the
+    lifting lines when ``kjs`` is given). ``step`` advances one step;
+    ``values`` returns per-case rows (thrust, torque, power, iterations)."""
+
+    def __init__(self, cases, kjs=None, kj_params=None, **batch_kw):
+        from .wake import WakeBatch
+        self.b = WakeBatch(cases, **batch_kw)
+        self.kj = kjs is not None
+        if self.kj:
+            self.b.set_kj(kjs, **(kj_params or {}))
+        self.n = len(cases)
+
+    def step(self, graph=True):
+        self.b.step(1, graph=graph)
+
+    def values(self):
+        if not self.kj:
+            return np.zeros((self.n, 4))
+        T, Q, P = self.b.loads()
+        it = self.b.kj_stats()[0]
+        return np.stack([T, Q, P, it.astype(np.float64)], 1)
+
+    def step_ms(self):
+        return self.b.stats()[0]
+
+    def close(self):
+        self.b.close()
+
+
+class ShardedRun:
+    """Steps ``cases`` (wake-case dicts, with ``kjs`` lifting lines when given)
+    split over ``world`` ranks; this process is ``rank``. ``stepper`` builds
+    the local stepper from (cases, kjs, **kw); after every ``step`` the
+    per-case rows of ``values()`` of all ranks are in ``history`` (one
+    [ncases, columns] array per step, case order), the same on every rank."""
+
+    def __init__(self, cases, kjs=None, rank=0, world=1, stepper=BatchStepper, group=None,
+                 **kw):
+        self.rank, self.world, self.group = rank, world, group
+        self.parts = partition([case_cost(c) for c in cases], world)
+        self.mine = self.parts[rank]
+        self.ncases = len(cases)
+        self.local = None
+        if self.mine:
+            self.local = stepper([cases[i] for i in self.mine],
+                                 None if kjs is None else [kjs[i] for i in self.mine], **kw)
+        self.history = []
+
+    def step(self, n=1, graph=True):
+        for _ in range(n):
+            if self.local is not None:
+                self.local.step(graph=graph)
+                vals = self.local.values()
+            else:
+                vals = np.zeros((0, 4))
+            self.history.append(gather_case_values(vals, self.parts, self.rank, self.world, self.group))
+        return self.history[-1]
+
+    def close(self):
+        if self.local is not None:
+            self.local.close()
+            self.local = None
