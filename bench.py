@@ -373,10 +373,10 @@ def wake_kj_bench(rcases, cases, tol=1e-6, relax=0.3, maxiter=200, warm=3, timed
     kjs = [synth.make_kj_case(rc, nsteps=c["nsteps"], t0=c["t0"]) for rc, c in zip(rcases, cases)]
     n = len(cases)
 
-    def run(prec, graph, net=None, one=None):
+    def run(prec, graph, net=None, one=None, ll_fp64=False):
         sel = range(n) if one is None else [one]
         b = wake.WakeBatch([cases[k] for k in sel], integrator="pcc", precision=prec)
-        b.set_kj([kjs[k] for k in sel], relax=relax, tol=tol, maxiter=maxiter)
+        b.set_kj([kjs[k] for k in sel], relax=relax, tol=tol, maxiter=maxiter, ll_fp64=ll_fp64)
         if net is not None:
             b.set_mlp(net)
         for _ in range(warm):
@@ -397,6 +397,7 @@ def wake_kj_bench(rcases, cases, tol=1e-6, relax=0.3, maxiter=200, warm=3, timed
 
     fast = run("f32c", True)
     host = run("f32c", False)
+    fast_ll64 = run("f32c", True, ll_fp64=True)
     plain = dict(ms=0.0, iters=[], T=[], G=[], capped=[])
     for k in range(n):
         r = run("f64", False, one=k)
@@ -423,7 +424,14 @@ def wake_kj_bench(rcases, cases, tol=1e-6, relax=0.3, maxiter=200, warm=3, timed
                "thrust_rel_diff_max": float(dT[conv].max()) if conv.any() else None,
                "bound_rel_diff_max": float(dG[conv].max()) if conv.any() else None},
            "stalled_subset": {"kj_iterations_fast": int(it_f[~conv].sum()),
-                              "kj_iterations_plain": int(it_p[~conv].sum())}}
+                              "kj_iterations_plain": int(it_p[~conv].sum())},
+           # the same FP32c batch with the lifting-line evaluations in FP64
+           "fast_lifting_line_fp64": {
+               "steps_per_s": 1000.0 / fast_ll64["ms"],
+               "kj_iterations_converged_subset": int(fast_ll64["iters"][conv].sum()),
+               "iterations_ratio_over_plain": float(fast_ll64["iters"][conv].sum()
+                                                    / max(it_p[conv].sum(), 1)),
+               "cases_iterations_equal_plain": int((fast_ll64["iters"][conv] == it_p[conv]).sum())}}
     # start-value arms on the fast path
     arms = {"previous": fast}
     xo = gi.extrapolation_only()

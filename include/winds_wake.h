@@ -176,6 +176,8 @@ typedef struct {
   double relax;  /* fixed-point relaxation (user.relax) */
   double tol;    /* convergence tolerance (user.tol)   */
   int maxiter;   /* iteration cap (user.maxiter)       */
+  int ll_fp64;   /* 1: the iteration's induced velocity at the lifting lines in FP64 (the
+                    plain FP64 direct sum) whatever the batch's precision; 0: the batch's */
 } winds_kj_params;
 
 /* Attaches one lifting line per case (host arrays copied) and enables the
@@ -196,13 +198,14 @@ int winds_wake_get_perf(winds_wake_batch *b, int icase, double *cl, double *cd, 
  * twist, sin(azimuth), cos(azimuth), the local inflow in the blade frame
  * (3 components: vblade at the step plus the previous step's induced
  * velocity at the lifting line, transformed as kj() does), previous bound
- * circulation, its change over the previous step; the start value is
+ * circulation, its change over the previous step, the change over the step
+ * before that; the start value is
  * Gamma_prev + out_scale * network(features) (on the extrapolated base:
  * Gamma_prev + its change + out_scale * network) at stations whose airfoil
  * table has lift, and Gamma_prev at the others (e.g. cylinder root sections:
  * Cl = 0 at every AoA, so their fixed point is Gamma = 0, and the relaxed
  * iteration damps a start error there by only 1 - relax per iteration).
- * The network must have 10 inputs and live on the batch's device; the
+ * The network must have 11 inputs and live on the batch's device; the
  * iteration and its tolerance are unchanged. No reference counterpart
  * (WInDS.m:131 always starts from the previous step). */
 struct winds_mlp;
@@ -216,7 +219,7 @@ int winds_wake_get_loads(winds_wake_batch *b, double *thrust, double *torque, do
 /* The start value [ns,nb] of the last step's iteration for one case. */
 int winds_wake_get_kj_guess(winds_wake_batch *b, int icase, double *guess);
 
-/* The MLP features [ns*nb][10] (rows i + ns*b) of one case at the last step,
+/* The MLP features [ns*nb][11] (rows i + ns*b) of one case at the last step,
  * computed whenever the lifting lines carry the station inputs (training
  * pairs: these rows with the converged bound circulation). */
 int winds_wake_get_kj_features(winds_wake_batch *b, int icase, float *x);

@@ -14,7 +14,7 @@ class FakeMlp:
         self.base, self.full_out_scale, self.out = base, 2.0, 2.0
 
     def scaling(self):
-        return np.zeros(10, np.float32), np.ones(10, np.float32), self.out
+        return np.zeros(11, np.float32), np.ones(11, np.float32), self.out
 
     def set_scaling(self, shift, scale, out_scale):
         self.out = out_scale

@@ -34,7 +34,7 @@ def test_features_and_start_value_match_host(wb):
     b = wake.WakeBatch(cases, integrator="pcc")
     b.set_kj(kjs, relax=0.3, tol=1e-6, maxiter=100)
     m = mlp.Mlp(gi.N_FEATURES, seed=3)
-    m.set_scaling(np.zeros(10, np.float32), np.full(10, 0.2, np.float32), 0.7)
+    m.set_scaling(np.zeros(gi.N_FEATURES, np.float32), np.full(gi.N_FEATURES, 0.2, np.float32), 0.7)
     b.set_mlp(m)
     prev = [b.bound(k) for k in range(3)]
     b.step(1)
@@ -48,13 +48,20 @@ def test_features_and_start_value_match_host(wb):
         assert lift.any() and not lift.all()
         gh = prev[k].ravel(order="F") + lift * float(np.float32(0.7)) * m.forward(x).astype(np.float64)
         np.testing.assert_allclose(g.ravel(order="F"), gh, rtol=1e-12, atol=1e-9)
-    # later steps carry the change of the converged circulation
+    # later steps carry the changes of the converged circulation
     prev1 = [b.bound(k) for k in range(3)]
     b.step(1)
     for k in range(3):
         x = b.kj_features(k)
         np.testing.assert_allclose(x[:, 8], prev1[k].ravel(order="F"), rtol=1e-6, atol=1e-5)
         np.testing.assert_allclose(x[:, 9], (prev1[k] - prev[k]).ravel(order="F"), rtol=1e-5, atol=1e-4)
+        np.testing.assert_array_equal(x[:, 10], 0.0)  # no change before the first step
+    prev2 = [b.bound(k) for k in range(3)]
+    b.step(1)
+    for k in range(3):
+        x = b.kj_features(k)
+        np.testing.assert_allclose(x[:, 9], (prev2[k] - prev1[k]).ravel(order="F"), rtol=1e-5, atol=1e-4)
+        np.testing.assert_allclose(x[:, 10], (prev1[k] - prev[k]).ravel(order="F"), rtol=1e-5, atol=1e-4)
     b.close()
     m.close()
 
@@ -69,7 +76,7 @@ def test_extrapolated_base_start_value(wb):
     b = wake.WakeBatch(cases, integrator="pcc")
     b.set_kj(kjs, relax=0.3, tol=1e-6, maxiter=100)
     m = mlp.Mlp(gi.N_FEATURES, seed=3)
-    m.set_scaling(np.zeros(10, np.float32), np.full(10, 0.2, np.float32), 0.05)
+    m.set_scaling(np.zeros(gi.N_FEATURES, np.float32), np.full(gi.N_FEATURES, 0.2, np.float32), 0.05)
     m.set_base("extrapolated")
     assert m.base == "extrapolated"
     b.step(1)
@@ -105,7 +112,7 @@ def test_graph_with_network_matches_host_loop(wb):
     gi, mlp, wake, synth = _mods()
     pts = gi.operating_points(3, seed=7, nst=13, wake_steps=10)
     m = mlp.Mlp(gi.N_FEATURES, seed=3)
-    m.set_scaling(np.zeros(10, np.float32), np.full(10, 0.2, np.float32), 0.02)
+    m.set_scaling(np.zeros(gi.N_FEATURES, np.float32), np.full(gi.N_FEATURES, 0.2, np.float32), 0.02)
     ra = gi.run(pts, 3, mlp=m, graph=False)
     rb = gi.run(pts, 3, mlp=m, graph=True)
     np.testing.assert_array_equal(ra["iters"], rb["iters"])
@@ -119,7 +126,7 @@ def test_graph_with_network_matches_host_loop(wb):
     b.set_mlp(m)
     b.step(1, graph=True)
     prev = [b.bound(k) for k in range(3)]
-    m.set_scaling(np.zeros(10, np.float32), np.full(10, 0.2, np.float32), 0.3)
+    m.set_scaling(np.zeros(gi.N_FEATURES, np.float32), np.full(gi.N_FEATURES, 0.2, np.float32), 0.3)
     b.step(1, graph=True)
     for k in range(3):
         x = b.kj_features(k)
@@ -137,7 +144,7 @@ def test_attach_detach_between_graph_steps(wb):
     gi, mlp, wake, synth = _mods()
     pts = gi.operating_points(3, seed=7, nst=13, wake_steps=10)
     m = mlp.Mlp(gi.N_FEATURES, seed=5)
-    m.set_scaling(np.zeros(10, np.float32), np.full(10, 0.2, np.float32), 0.02)
+    m.set_scaling(np.zeros(gi.N_FEATURES, np.float32), np.full(gi.N_FEATURES, 0.2, np.float32), 0.02)
     out = []
     for graph in (False, True):
         cases, kjs = gi.build(pts, 5)

@@ -103,3 +103,26 @@ def test_first_step_autotunes_the_batch_tiling(wb, synth):
     T, KF, waves = wb.get_tuning(wb.bs.CORE_VATISTAS, nodes, fil)
     assert T in (3, 4) and KF in (32, 64) and waves in (32.0, 64.0)
     b.close()
+
+
+def test_sharded_run_device_stepper_matches_the_batch(wb, synth):
+    """sharding.ShardedRun on one rank with the device stepper gives the
+    batch's own thrust, torque, power and iteration counts every step."""
+    import importlib
+    sh = importlib.import_module("winds-master_b200.sharding")
+    wake = importlib.import_module("winds-master_b200.wake")
+    rcs = synth.batch_cases(3, seed=8, steps_range=(20, 40), nodes_range=(9, 13))
+    cases = [synth.make_wake_case(rc, nsteps=4) for rc in rcs]
+    kjs = [synth.make_kj_case(rc, nsteps=4, t0=c["t0"]) for rc, c in zip(rcs, cases)]
+    kp = dict(relax=0.3, tol=1e-6, maxiter=100)
+    run = sh.ShardedRun(cases, kjs, rank=0, world=1, integrator="pcc", precision="f32c", kj_params=kp)
+    b = wake.WakeBatch(cases, integrator="pcc", precision="f32c")
+    b.set_kj(kjs, **kp)
+    for _ in range(2):
+        got = run.step(1, graph=True)
+        b.step(1, graph=True)
+        T, Q, P = b.loads()
+        want = np.stack([T, Q, P, b.kj_stats()[0].astype(np.float64)], 1)
+        np.testing.assert_array_equal(got, want)
+    run.close()
+    b.close()

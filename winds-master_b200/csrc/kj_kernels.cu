@@ -93,8 +93,11 @@ __global__ void kj_update(const WakeCase *cases, const KJCase *kc, const int *st
 // this step with the induced velocity of the previous step's last iteration
 // (uindb, zero before the first step): vblade + [bxn; byn; bzn] uindb, the
 // velocity the first iteration of kj() would see (core/KuttaJoukowski.m:241-249).
+// The history: bound (the last converged value), bound_last and bound_last2
+// (the two before it; equal to bound before there were any).
 __global__ void kj_features(const WakeCase *cases, const KJCase *kc, const int *step,
                             const double *bound, const double *bound_last,
+                            const double *bound_last2,
                             const double *vblade, const double *bxn,
                             const double *byn, const double *bzn, const double *uindb,
                             const double *st_r, const double *st_c, const double *st_tw,
@@ -123,6 +126,7 @@ __global__ void kj_features(const WakeCase *cases, const KJCase *kc, const int *
   const long long q = c.bound_off + i + (long long)ns * b;
   f[8] = (float)bound[q];
   f[9] = (float)(bound[q] - bound_last[q]);
+  f[10] = (float)(bound_last[q] - bound_last2[q]);
 }
 
 // bound = base + out_scale * y, base Gamma_prev or, with *base != 0, its
@@ -297,13 +301,14 @@ cudaError_t launch_kj_update(const WakeCase *cases, const KJCase *kc, int ncases
 
 cudaError_t launch_kj_features(const WakeCase *cases, const KJCase *kc, int ncases, int max_st,
                                const int *step, const double *bound, const double *bound_last,
-                               const double *vblade, const double *bxn, const double *byn,
-                               const double *bzn, const double *uindb, const double *st_r,
+                               const double *bound_last2, const double *vblade,
+                               const double *bxn, const double *byn, const double *bzn,
+                               const double *uindb, const double *st_r,
                                const double *st_c, const double *st_tw, const double *azim,
                                float *x, cudaStream_t s) {
   kj_features<<<dim3((max_st + 127) / 128, ncases), 128, 0, s>>>(
-      cases, kc, step, bound, bound_last, vblade, bxn, byn, bzn, uindb, st_r, st_c, st_tw, azim,
-      x);
+      cases, kc, step, bound, bound_last, bound_last2, vblade, bxn, byn, bzn, uindb, st_r, st_c,
+      st_tw, azim, x);
   return cudaGetLastError();
 }
 

@@ -24,9 +24,9 @@ struct KJCase {
 // r/R, chord/R, twist, sin and cos of the blade azimuth, the three
 // blade-frame components of the local inflow (vblade at the step plus the
 // previous step's induced velocity at the lifting line), the current bound
-// circulation (the previous step's converged value) and its change over the
-// previous step.
-constexpr int kKJFeatures = 10;
+// circulation (the previous step's converged value), its change over the
+// previous step and the change over the step before that.
+constexpr int kKJFeatures = 11;
 
 cudaError_t launch_kj_targets(const WakeCase *cases, const KJCase *kc, int ncases, int max_st,
                               const int *step, const double *ll, double4 *tp, BBox *bb,
@@ -41,6 +41,7 @@ cudaError_t launch_kj_update(const WakeCase *cases, const KJCase *kc, int ncases
                              double *cd_out, double *aoa_out, cudaStream_t s);
 cudaError_t launch_kj_features(const WakeCase *cases, const KJCase *kc, int ncases, int max_st,
                                const int *step, const double *bound, const double *bound_last,
+                               const double *bound_last2,
                                const double *vblade, const double *bxn, const double *byn,
                                const double *bzn, const double *uindb, const double *st_r,
                                const double *st_c, const double *st_tw, const double *azim,

@@ -79,7 +79,7 @@ struct winds_wake_batch {
   bool mlp_inputs = false;      // every case gave the station arrays
   bool loads = false;           // every case gave the loads inputs
   DevBuf st_rr, st_dr, rpm, pitch, dl, loads_out;
-  DevBuf st_r, st_c, st_tw, azim, guess, feat, bound_last;
+  DevBuf st_r, st_c, st_tw, azim, guess, feat, bound_last, bound_last2;
   DevBuf st_lift;  // per station: 1 when its airfoil table has lift (start value applies)
   winds_mlp *mlp = nullptr;
   MlpWork mw;
@@ -406,7 +406,7 @@ cudaError_t enqueue_kj_iter(winds_wake_batch *b, int &launches, cudaStream_t s,
   a.co = b->prm.co;
   a.wait_limit_ns = default_wait_limit_ns();
   if (e == cudaSuccess)
-    e = b->prec == WINDS_PREC_F64 ? launch_f64(a, b->kj_grid, s)
+    e = b->prec == WINDS_PREC_F64 || b->kjp.ll_fp64 ? launch_f64(a, b->kj_grid, s)
                                   : launch_f32c(a, b->model, b->kj_T, b->kj_KF, b->kj_grid, s);
   if (e == cudaSuccess)
     e = launch_reduce(P<const Tile>(b->kj_tiles), b->kj_ntiles, P<const Group>(b->kj_groups),
@@ -452,12 +452,16 @@ cudaError_t enqueue_kj_begin(winds_wake_batch *b) {
   if (e == cudaSuccess && b->mlp_inputs)
     e = launch_kj_features(cd, kd, b->ncases, b->max_st, P<const int>(b->step_d),
                            P<const double>(b->bound), P<const double>(b->bound_last),
-                           P<const double>(b->vblade), P<const double>(b->bxn), P<const double>(b->byn),
+                           P<const double>(b->bound_last2), P<const double>(b->vblade),
+                           P<const double>(b->bxn), P<const double>(b->byn),
                            P<const double>(b->bzn), P<const double>(b->uindb),
                            P<const double>(b->st_r), P<const double>(b->st_c),
                            P<const double>(b->st_tw), P<const double>(b->azim), P<float>(b->feat),
                            s);
-  // the previous step's converged value, for the next step's change feature
+  // the history one step on, for the next step's change features
+  if (e == cudaSuccess && b->mlp_inputs)
+    e = cudaMemcpyAsync(b->bound_last2.p, b->bound_last.p, b->bound_n * sizeof(double),
+                        cudaMemcpyDeviceToDevice, s);
   if (e == cudaSuccess && b->mlp_inputs)
     e = cudaMemcpyAsync(b->bound_last.p, b->bound.p, b->bound_n * sizeof(double),
                         cudaMemcpyDeviceToDevice, s);
@@ -1152,7 +1156,7 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
   for (DevBuf *x : {&b->conv, &b->iters, &b->diverged, &b->res_max, &b->res_last, &b->active})
     if ((rc = x->ensure(std::max(b->ncases, 1) * 8 + 8, s))) return rc;
   if ((rc = b->kj_it.ensure(16, s))) return rc;
-  for (DevBuf *x : {&b->cl_o, &b->cd_o, &b->aoa_o, &b->guess, &b->bound_last})
+  for (DevBuf *x : {&b->cl_o, &b->cd_o, &b->aoa_o, &b->guess, &b->bound_last, &b->bound_last2})
     if ((rc = x->ensure(b->bound_n * sizeof(double), s))) return rc;
   // defined values before any iteration (a step without one reads them)
   for (DevBuf *x : {&b->conv, &b->iters, &b->diverged, &b->res_max, &b->res_last, &b->active})
@@ -1162,10 +1166,11 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
     if (cudaError_t e0 = cudaMemset(x->p, 0, b->bound_n * sizeof(double)); e0 != cudaSuccess)
       return cuda_fail(e0, "lifting-line outputs");
   // no change before the first step
-  if (cudaError_t e0 = cudaMemcpy(b->bound_last.p, b->bound.p, b->bound_n * sizeof(double),
-                                  cudaMemcpyDeviceToDevice);
-      e0 != cudaSuccess)
-    return cuda_fail(e0, "bound copy");
+  for (DevBuf *x : {&b->bound_last, &b->bound_last2})
+    if (cudaError_t e0 = cudaMemcpy(x->p, b->bound.p, b->bound_n * sizeof(double),
+                                    cudaMemcpyDeviceToDevice);
+        e0 != cudaSuccess)
+      return cuda_fail(e0, "bound copy");
   all_loads = all_loads && have_twist;
   b->mlp_inputs = all_inputs;
   b->loads = all_loads;
@@ -1262,7 +1267,7 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
   int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->dev);
   int resident, quantum;
-  if (b->prec == WINDS_PREC_F64) {
+  if (b->prec == WINDS_PREC_F64 || b->kjp.ll_fp64) {
     b->kj_tile_cap = f64_threads();
     resident = f64_occupancy() * sms;
     quantum = f64_tile();
@@ -1403,7 +1408,7 @@ void winds_wake_destroy(winds_wake_batch *b) {
                     &b->conv, &b->iters,
                     &b->res_max, &b->res_last, &b->active, &b->diverged, &b->cl_o, &b->cd_o,
                     &b->aoa_o, &b->st_r, &b->st_c, &b->st_tw, &b->azim, &b->guess, &b->feat,
-                    &b->bound_last, &b->st_rr, &b->st_dr, &b->rpm, &b->pitch, &b->dl,
+                    &b->bound_last, &b->bound_last2, &b->st_rr, &b->st_dr, &b->rpm, &b->pitch, &b->dl,
                     &b->loads_out})
     x->release();
   b->mw.release();

@@ -23,7 +23,9 @@ synthetic blade and polar (chord 3.5 -> 1.4 m, twist 13 -> 0 deg, Cl =
 Features (device-computed, ``winds_wake_get_kj_features``): r/R, chord/R,
 twist, sin and cos of the azimuth, the local inflow in the blade frame
 (kinematic inflow plus the previous step's induced velocity at the lifting
-line), the previous bound circulation and its change over the previous step.
+line), the previous bound circulation, its change over the previous step and
+the change over the step before that (with which the network can form a
+second-order extrapolation).
 Training pairs come only from (case, step) whose plain iteration converged,
 and only from lifting stations: a station whose airfoil table has no lift
 (the cylinder root sections) converges to Gamma = 0, the engine keeps its
@@ -41,7 +43,7 @@ from . import synth
 from .mlp import Mlp
 from .wake import WakeBatch
 
-N_FEATURES = 10
+N_FEATURES = 11
 
 
 @dataclasses.dataclass

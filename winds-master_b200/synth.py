@@ -401,13 +401,14 @@ def make_kj_case(case: RotorCase, nsteps: int, t0: float = 0.0, pitch_deg: float
     return res
 
 
-def kj_features(kj: dict, s: int, bound, bound_last=None, uind=None) -> np.ndarray:
+def kj_features(kj: dict, s: int, bound, bound_last=None, uind=None, bound_last2=None) -> np.ndarray:
     """Inputs of the bound-circulation MLP at step ``s`` (rows i + ns*b), the
     device's feature order, as float32: r/R, chord/R, twist, sin/cos azimuth,
     local inflow in the blade frame (vblade plus ``uind`` [ns,3,nb], the
     previous step's induced velocity at the lifting line, rotated with
-    bxn/byn/bzn; zero when None), bound circulation and its change since
-    ``bound_last`` (zero when None)."""
+    bxn/byn/bzn; zero when None), bound circulation, its change since
+    ``bound_last`` and the change from ``bound_last2`` to ``bound_last``
+    (zero when None)."""
     ns, _, _, nb = kj["vblade"].shape
     az = kj["azimuth"][s]                                   # [nb]
     vb = kj["vblade"][:, :, s, :].copy()                    # [ns, 3, nb]
@@ -415,10 +416,12 @@ def kj_features(kj: dict, s: int, bound, bound_last=None, uind=None) -> np.ndarr
         for a, key in enumerate(("bxn", "byn", "bzn")):
             vb[:, a, :] += (kj[key][:, :, s, :] * uind).sum(1)
     bound = np.asarray(bound, dtype=np.float64)
-    d = bound - (np.asarray(bound_last) if bound_last is not None else bound)
+    last = np.asarray(bound_last, dtype=np.float64) if bound_last is not None else bound
+    d = bound - last
+    d2 = last - (np.asarray(bound_last2, dtype=np.float64) if bound_last2 is not None else last)
     cols = [np.repeat(kj["r_over_R"][:, None], nb, 1), np.repeat(kj["chord_over_R"][:, None], nb, 1),
             np.repeat(kj["twist"][:, None], nb, 1), np.repeat(np.sin(az)[None, :], ns, 0),
-            np.repeat(np.cos(az)[None, :], ns, 0), vb[:, 0], vb[:, 1], vb[:, 2], bound, d]
+            np.repeat(np.cos(az)[None, :], ns, 0), vb[:, 0], vb[:, 1], vb[:, 2], bound, d, d2]
     return np.stack([c.ravel(order="F") for c in cols], axis=1).astype(np.float32)
 
 

@@ -46,7 +46,8 @@ class KJCaseC(C.Structure):
 
 
 class KJParamsC(C.Structure):
-    _fields_ = [("relax", C.c_double), ("tol", C.c_double), ("maxiter", C.c_int)]
+    _fields_ = [("relax", C.c_double), ("tol", C.c_double), ("maxiter", C.c_int),
+                ("ll_fp64", C.c_int)]
 
 
 class WakeParamsC(C.Structure):
@@ -148,9 +149,10 @@ class WakeBatch:
         b = np.asfortranarray(bound, dtype=np.float64)
         _check(_bind().winds_wake_set_bound(self.h, i, b.ctypes.data))
 
-    def set_kj(self, kjs, relax=0.25, tol=1e-6, maxiter=30):
+    def set_kj(self, kjs, relax=0.25, tol=1e-6, maxiter=30, ll_fp64=False):
         """Attaches one lifting line per case (dicts as :func:`synth.make_kj_case`
-        returns them): every later step runs the Kutta-Joukowski iteration."""
+        returns them): every later step runs the Kutta-Joukowski iteration
+        (``ll_fp64``: its lifting-line evaluations in FP64 in an FP32c batch)."""
         arr = (KJCaseC * len(kjs))()
         for k, j in enumerate(kjs):
             a = arr[k]
@@ -171,7 +173,7 @@ class WakeBatch:
                     self._keep.append(x)
                     setattr(a, f, x.ctypes.data)
             a.rho = float(j.get("rho", 0.0))
-        p = KJParamsC(float(relax), float(tol), int(maxiter))
+        p = KJParamsC(float(relax), float(tol), int(maxiter), int(bool(ll_fp64)))
         _check(_bind().winds_wake_set_kj(self.h, arr, C.byref(p)))
 
     def set_mlp(self, mlp):
@@ -196,9 +198,9 @@ class WakeBatch:
         return T, Q, P
 
     def kj_features(self, i):
-        """MLP features [ns*nb, 10] of case ``i`` at the last step."""
+        """MLP features [ns*nb, 11] of case ``i`` at the last step."""
         c = self.cases[i]
-        x = np.zeros(((c["nst"] - 1) * c["nb"], 10), dtype=np.float32)
+        x = np.zeros(((c["nst"] - 1) * c["nb"], 11), dtype=np.float32)
         _check(_bind().winds_wake_get_kj_features(self.h, i, x.ctypes.data))
         return x
 
