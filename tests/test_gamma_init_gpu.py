@@ -165,18 +165,30 @@ def test_attach_detach_between_graph_steps(wb):
 
 
 def test_trained_start_value_saves_iterations(wb):
-    """Trained on plain-solver pairs (~4.5e5) of the attached-flow operating
-    points among 400 candidates, the network's start value needs fewer
-    iterations on held-out attached points at the same tolerance and leaves
-    the converged circulation unchanged (the fixed point is unique there)."""
+    """Trained on plain-solver pairs (~3e5, lifting stations) of the
+    attached-flow operating points among 400 candidates, on held-out attached
+    points at the same tolerance: the previous-step start (the reference),
+    the extrapolation alone, and the extrapolation plus the network. The
+    network needs fewer iterations than the extrapolation alone (by at least
+    3%; measured 5.4%) and than the previous-step start (at least 12%;
+    measured 19%). Converged results: at the study's tolerance (1e-6 on the
+    relative residual, which bounds the residual and not the distance to the
+    fixed point) the starts' thrust differs by a few 1e-4; iterated to 1e-10
+    in FP64 every start reaches the same fixed point."""
     gi, *_ = _mods()
     r = gi.study(n_train=400, n_test=120, epochs=60)
-    assert r["pairs"] > 300000 and r["test_points"] >= 10
+    assert r["pairs"] > 200000 and r["test_points"] >= 10
     assert r["loss_last"] < 0.1 * r["loss_first"]
-    # attached-flow points converge (a borderline step may reach maxiter in
-    # either run; iterations are compared where both converged)
-    assert r["converged_plain"] >= 0.99 and r["converged_mlp"] >= 0.99
-    assert r["saved_steady"] > 0.03, r
-    assert r["cases_improved"] >= 0.6 * r["test_points"], r
-    assert r["bound_rel_diff_max"] <= 2e-3, r
+    arms = r["arms"]
+    for name in ("previous", "extrapolated", "network"):
+        assert arms[name]["converged"] >= 0.99, (name, arms[name])
+    it_p, it_e, it_n = (arms[k]["iterations"] for k in ("previous", "extrapolated", "network"))
+    assert it_e < it_p, arms
+    assert it_n <= 0.97 * it_e, arms
+    assert it_n <= 0.88 * it_p, arms
+    assert arms["network"]["thrust_rel_diff_max"] <= 2e-3, arms
+    t = r["tight"]
+    assert t["converged"] >= 0.9, t
+    assert t["bound_rel_diff_max"] <= 1e-7, t
+    assert t["thrust_rel_diff_max"] <= 1e-7 and t["power_rel_diff_max"] <= 1e-7, t
     r["model"].close()
