@@ -465,7 +465,7 @@ def kj_mlp_bench():
 
     def rnd(v):
         if isinstance(v, float):
-            return round(v, 6)
+            return float(f"{v:.6g}")
         if isinstance(v, dict):
             return {k: rnd(x) for k, x in v.items()}
         return v

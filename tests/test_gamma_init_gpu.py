@@ -171,10 +171,11 @@ def test_trained_start_value_saves_iterations(wb):
     the extrapolation alone, and the extrapolation plus the network. The
     network needs fewer iterations than the extrapolation alone (by at least
     3%; measured 5.4%) and than the previous-step start (at least 12%;
-    measured 19%). Converged results: at the study's tolerance (1e-6 on the
-    relative residual, which bounds the residual and not the distance to the
-    fixed point) the starts' thrust differs by a few 1e-4; iterated to 1e-10
-    in FP64 every start reaches the same fixed point."""
+    measured 19%). Converged results: over a run at the study's tolerance
+    (1e-6 on the relative residual, which bounds the residual and not the
+    distance to the fixed point; each step's difference carries into the
+    wake) the starts' thrust differs by a few 1e-4; from one and the same wake
+    state, iterated to 1e-10 in FP64, every start reaches the same fixed point."""
     gi, *_ = _mods()
     r = gi.study(n_train=400, n_test=120, epochs=60)
     assert r["pairs"] > 200000 and r["test_points"] >= 10
@@ -188,7 +189,8 @@ def test_trained_start_value_saves_iterations(wb):
     assert it_n <= 0.88 * it_p, arms
     assert arms["network"]["thrust_rel_diff_max"] <= 2e-3, arms
     t = r["tight"]
-    assert t["converged"] >= 0.9, t
-    assert t["bound_rel_diff_max"] <= 1e-7, t
-    assert t["thrust_rel_diff_max"] <= 1e-7 and t["power_rel_diff_max"] <= 1e-7, t
+    assert t["same_state_before"] and t["converged"] >= 0.8, t
+    for name in ("extrapolated", "network"):
+        assert t[name]["bound_rel_diff_max"] <= 1e-7, t
+        assert t[name]["thrust_rel_diff_max"] <= 1e-7 and t[name]["power_rel_diff_max"] <= 1e-7, t
     r["model"].close()

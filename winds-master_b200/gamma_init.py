@@ -254,11 +254,12 @@ def study(n_train: int = 400, n_test: int = 120, train_steps: int = 42, test_ste
     network's own share shows (``arms``: previous-step start, extrapolation
     alone, network, over the steps past the start-up that converged in all
     three). Converged results: thrust, power and bound circulation of each
-    start against the previous-step start at the study's tolerance, and again
-    on ``tight_points`` test points at ``tight_tol`` in FP64 -- the
-    iteration's stopping rule bounds the residual, not the distance to the
-    fixed point, so the differences must shrink with the tolerance when every
-    start reaches the same fixed point. Returns a dict of the measurements."""
+    start against the previous-step start over the run at the study's
+    tolerance (the stopping rule bounds the residual, not the distance to the
+    fixed point, and each step's difference carries into the wake), and
+    (``tight``) from one and the same wake state on ``tight_points`` test
+    points at ``tight_tol`` in FP64, where every start must reach the same
+    fixed point. Returns a dict of the measurements."""
     t0 = time.perf_counter()
     kw = dict(relax=relax, tol=tol, maxiter=maxiter, precision=precision)
     train_pts = attached(operating_points(n_train, seed=seed), **kw)
@@ -304,22 +305,48 @@ def study(n_train: int = 400, n_test: int = 120, train_steps: int = 42, test_ste
     arms = dict(previous=arm(a), extrapolated=arm(e), network=arm(b))
     for name, r in (("extrapolated", e), ("network", b)):
         arms[name]["thrust_rel_diff_max"], arms[name]["power_rel_diff_max"] = loads_diff(r, a, all3)
-    # the same comparison at a tight tolerance: every start must reach the same fixed point
+    # the same wake state, three starts, a tight tolerance: every start must
+    # reach the same fixed point. Three identical FP64 batches (the FP32c
+    # sums' rounding keeps the residual above ~1e-7) step `tight_steps` steps
+    # from the previous-step start, then one more step from the previous step,
+    # the extrapolation alone and the network.
     tight = {}
     if tight_points > 0 and test_pts:
-        # FP64: the FP32c sums' rounding keeps the residual above ~1e-7
-        kt = dict(kw, tol=tight_tol, maxiter=max(maxiter, 600), precision="f64")
         pts_t = test_pts[:tight_points]
-        ta = run(pts_t, tight_steps, **kt)
-        tb = run(pts_t, tight_steps, mlp=m, **kt)
-        ok = (ta["iters"] < kt["maxiter"]) & (tb["iters"] < kt["maxiter"])
-        dT, dP = loads_diff(tb, ta, ok)
-        dGt = max(float(np.abs(np.asarray(x) - np.asarray(y)).max() / (np.abs(np.asarray(y)).max() + 1.0))
-                  for x, y in zip(tb["bounds"][-1], ta["bounds"][-1]))
-        tight = dict(tol=tight_tol, points=len(pts_t), steps=tight_steps,
-                     converged=float(ok.mean()), thrust_rel_diff_max=dT, power_rel_diff_max=dP,
-                     bound_rel_diff_max=dGt, iterations_previous=int(ta["iters"][ok].sum()),
-                     iterations_network=int(tb["iters"][ok].sum()))
+        cases_t, kjs_t = build(pts_t, tight_steps + 1)
+        maxit = max(maxiter, 600)
+        bs = []
+        for _ in range(3):
+            bt = WakeBatch(cases_t, integrator="pcc", precision="f64")
+            bt.set_kj(kjs_t, relax=relax, tol=tight_tol, maxiter=maxit)
+            bs.append(bt)
+        for _ in range(tight_steps):
+            for bt in bs:
+                bt.step(1, graph=True)
+        same_state = all(np.array_equal(bs[0].bound(k), bt.bound(k)) for bt in bs[1:]
+                         for k in range(len(pts_t)))
+        xo2 = extrapolation_only()
+        bs[1].set_mlp(xo2)
+        bs[2].set_mlp(m)
+        for bt in bs:
+            bt.step(1, graph=True)
+        its = [bt.kj_stats()[0] for bt in bs]
+        ok = np.all([it < maxit for it in its], axis=0)
+        G = [[bt.bound(k) for k in range(len(pts_t))] for bt in bs]
+        L = [bt.loads() for bt in bs]
+        tight = dict(tol=tight_tol, points=len(pts_t), step=tight_steps, same_state_before=bool(same_state),
+                     converged=float(ok.mean()),
+                     iterations={n: int(it[ok].sum()) for n, it in zip(("previous", "extrapolated",
+                                                                          "network"), its)})
+        for a_i, name in ((1, "extrapolated"), (2, "network")):
+            dG = max(float(np.abs(G[a_i][k] - G[0][k]).max() / (np.abs(G[0][k]).max() + 1.0))
+                     for k in range(len(pts_t)) if ok[k])
+            dT = float((np.abs(L[a_i][0] - L[0][0]) / np.abs(L[0][0]))[ok].max())
+            dP = float((np.abs(L[a_i][2] - L[0][2]) / np.abs(L[0][2]))[ok].max())
+            tight[name] = dict(bound_rel_diff_max=dG, thrust_rel_diff_max=dT, power_rel_diff_max=dP)
+        for bt in bs:
+            bt.close()
+        xo2.close()
     return dict(
         model=m, train_points=len(train_pts), test_points=len(test_pts), arms=arms, tight=tight,
         pairs=int(keep.sum()), loss_first=float(losses[0]), loss_last=float(losses[-1]),
