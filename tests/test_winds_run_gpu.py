@@ -114,3 +114,66 @@ def test_growing_wake_fills_its_capacity_then_truncates(wb):
     assert np.abs(a - c).max() < 1e-2 * np.abs(c).max()
     small.close()
     full.close()
+
+
+def test_start_value_waits_for_the_first_iteration(wb):
+    """With the reference start-up the network attached before step 0 changes
+    nothing at step 0 (core/initials.m's step has no iteration: the bound
+    circulation stays BEM's) and graph replay equals the host loop bit for
+    bit over the following steps."""
+    md = importlib.import_module("winds-master_b200.modeldata")
+    kin = importlib.import_module("winds-master_b200.kin")
+    wake = importlib.import_module("winds-master_b200.wake")
+    mlp = importlib.import_module("winds-master_b200.mlp")
+    import kin_ref
+    m, ser = nrel_series(nsteps=5)
+    cl0 = cl0_geometric(m, ser, kin_ref.kinematics(ser))
+    net = mlp.Mlp(11, seed=2)
+    net.set_scaling(np.zeros(11, np.float32), np.full(11, 0.05, np.float32), 0.5)
+    out = []
+    for graph in (False, True):
+        wc, kj = md.initial_cases(m, ser, kin.kinematics(ser), cl0, na=8)
+        b = wake.WakeBatch([wc], integrator="pcc", d=1e-4, precision="f32c", startup="reference")
+        b.set_kj([kj], relax=0.25, tol=1e-6, maxiter=60)
+        b.set_mlp(net)
+        g0 = b.bound(0)
+        b.step(1, graph=graph)
+        np.testing.assert_array_equal(b.bound(0), g0)
+        assert int(b.kj_stats()[0][0]) == 0
+        rec = []
+        for _ in range(3):
+            b.step(1, graph=graph)
+            rec.append((b.bound(0).copy(), int(b.kj_stats()[0][0]), b.kj_guess(0).copy()))
+        out.append(rec)
+        b.close()
+    for (ga, ia, sa), (gb, ib, sb) in zip(*out):
+        np.testing.assert_array_equal(ga, gb)
+        np.testing.assert_array_equal(sa, sb)
+        assert ia == ib
+    net.close()
+
+
+def test_lifting_line_in_fp64_gives_fp64_iterations(wb, synth):
+    """An FP32c batch whose lifting-line sums run in FP64 (ll_fp64) takes the
+    FP64 batch's iteration counts (tol 1e-6) and its bound circulation to
+    the FP32c wake's accuracy."""
+    wake = importlib.import_module("winds-master_b200.wake")
+    rcs = synth.batch_cases(4, seed=21, steps_range=(30, 60), nodes_range=(13, 17))
+    cases = [synth.make_wake_case(rc, nsteps=4) for rc in rcs]
+    kjs = [synth.make_kj_case(rc, nsteps=4, t0=c["t0"]) for rc, c in zip(rcs, cases)]
+    res = []
+    for prec, ll64 in (("f64", False), ("f32c", True)):
+        b = wake.WakeBatch(cases, integrator="pcc", precision=prec)
+        b.set_kj(kjs, relax=0.3, tol=1e-6, maxiter=200, ll_fp64=ll64)
+        its = []
+        for _ in range(3):
+            b.step(1, graph=True)
+            its.append(b.kj_stats()[0].copy())
+        res.append((its, [b.bound(k) for k in range(len(cases))]))
+        b.close()
+    for a, c in zip(res[0][0], res[1][0]):
+        conv = (a < 200) & (c < 200)
+        assert conv.sum() >= 2
+        np.testing.assert_array_equal(a[conv], c[conv])
+    for ga, gc in zip(res[0][1], res[1][1]):
+        assert np.abs(ga - gc).max() <= 1e-4 * (np.abs(ga).max() + 1.0)
