@@ -480,7 +480,8 @@ def e2e_run_bench(steps, ncases=16, ages=1440, seed=5, plain_cases=4):
     Fast: the FP32-compensated batch with graph replay, started from the
     network (previous-step base, trained here on plain-solver pairs of the
     same conditions with 120-step wakes, its output scale chosen on
-    validation runs that must keep the reference start's fixed point), from
+    validation runs that must keep the reference start's fixed point; the
+    start applies only at stations inside their polar's stall bounds), from
     the previous step's circulation, and from its extrapolation alone.
     Plain FP64 (FP64 direct sum, previous-step start, each case alone, no
     graphs) runs ``plain_cases`` of the 16 cases (every 16/plain_cases-th:
@@ -502,8 +503,9 @@ def e2e_run_bench(steps, ncases=16, ages=1440, seed=5, plain_cases=4):
     t0 = time.perf_counter()
     tr = gi.run(points(120, rng.uniform(0.0, 30.0, 64), 900), 48, record=True, maxiter=200)
     keep = (tr["step_case"][:, 0] >= 4) & tr["lift"]
-    # the previous-step base: these cases have stations past stall, where a
-    # start far from the reference's can select another fixed point
+    # the previous-step base: these cases have stations past stall, where the
+    # extrapolated start moves some cases to another fixed point (thrust
+    # percent off the plain path) even with the stall mask
     m, _ = gi.train(tr["X"][keep], tr["dG"][keep], epochs=40, base="previous")
     # output scale from solver runs on validation points of the same conditions
     gi.choose_shrink(m, points(120, rng.uniform(0.0, 30.0, 8), 950), 16, maxiter=200)

@@ -28,8 +28,10 @@ def _fake_run(table):
     scale (None: the reference's previous-step start)."""
     def run(points, steps, mlp=None, **kw):
         key = None if mlp is None else round(mlp.out / mlp.full_out_scale, 2)
-        its, bound = table[key]
-        return {"iters": np.array(its), "bounds": [[np.array(bound)]]}
+        its, bound = table[key][:2]
+        thrust = table[key][2] if len(table[key]) > 2 else 1.0
+        return {"iters": np.array(its), "bounds": [[np.array(bound)]],
+                "thrust": np.array([[thrust]])}
     return run
 
 
@@ -69,3 +71,39 @@ def test_choose_shrink_falls_back_to_the_reference_start(monkeypatch):
     m = FakeMlp()
     assert gi.choose_shrink(m, [], 6, skip=4) == 0.0
     assert m.base == "previous" and m.out == 0.0
+
+
+def test_start_rows_follow_the_stall_bounds():
+    """The synthetic polar's highest Cl in [0, 45] deg is at its 12 deg stall
+    (and the lowest in [-45, 0] at -12 deg); the start value applies at
+    lifting stations whose last AoA is more than 2 deg inside those bounds."""
+    gi = importlib.import_module("winds-master_b200.gamma_init")
+    synth = importlib.import_module("winds-master_b200.synth")
+    rc = synth.RotorCase(nst=9, nsteps=4, seed=1)
+    kj = synth.make_kj_case(rc, nsteps=4, root_cut=0.2)
+    sb = gi.stall_bounds(kj)
+    lift = gi.lifting_stations(kj)
+    assert lift.any() and not lift.all()
+    np.testing.assert_allclose(sb[lift], np.tile([-12.0, 12.0], (lift.sum(), 1)), atol=0.3)
+    ns, nb = len(lift), rc.nb
+    aoa = np.zeros((ns, nb))
+    aoa[:, 1] = 11.0  # past stall less the margin on blade 1
+    aoa[:, 2] = -9.0
+    rows = gi.start_rows(kj, nb, aoa).reshape(ns, nb, order="F")
+    np.testing.assert_array_equal(rows[:, 0], lift)
+    assert not rows[:, 1].any()
+    np.testing.assert_array_equal(rows[:, 2], lift)
+
+
+def test_choose_shrink_rejects_a_thrust_jump(monkeypatch):
+    """Circulation within the guard but thrust 2% off the previous-step
+    start's: another fixed point, rejected."""
+    gi = importlib.import_module("winds-master_b200.gamma_init")
+    ref = [10.0, 20.0]
+    table = {None: ([[9], [9], [9], [9], [9], [40]], ref, 1.0)}
+    for a, it, t in zip((0.0, 0.25, 0.5, 0.75, 1.0), (30, 20, 25, 35, 50),
+                        (1.0, 1.02, 1.0001, 1.0, 1.0)):
+        table[a] = ([[9], [9], [9], [9], [9], [it]], ref, t)
+    monkeypatch.setattr(gi, "run", _fake_run(table))
+    m = FakeMlp()
+    assert gi.choose_shrink(m, [], 6, skip=4) == 0.5

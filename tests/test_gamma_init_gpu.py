@@ -19,15 +19,17 @@ def _mods():
     return gi, mlp, wake, synth
 
 
-def _lift(gi, kj, nb):
-    """[ns*nb] row mask of the stations the start value applies to."""
-    return np.tile(gi.lifting_stations(kj), nb)
+def _lift(gi, kj, nb, aoa_prev):
+    """[ns*nb] row mask of the stations the start value applies to at a step
+    whose previous converged AoA is ``aoa_prev`` [ns, nb]."""
+    return gi.start_rows(kj, nb, aoa_prev)
 
 
 def test_features_and_start_value_match_host(wb):
     """Device features equal the host's; the start value is Gamma_prev +
-    out_scale * network at lifting stations and Gamma_prev at the others
-    (the cylinder root sections, whose table has no lift)."""
+    out_scale * network at lifting stations whose last AoA is inside their
+    table's stall bounds and Gamma_prev at the others (the cylinder root
+    sections, whose table has no lift)."""
     gi, mlp, wake, synth = _mods()
     pts = gi.operating_points(3, seed=7, nst=13, wake_steps=10)
     cases, kjs = gi.build(pts, 4)
@@ -37,6 +39,7 @@ def test_features_and_start_value_match_host(wb):
     m.set_scaling(np.zeros(gi.N_FEATURES, np.float32), np.full(gi.N_FEATURES, 0.2, np.float32), 0.7)
     b.set_mlp(m)
     prev = [b.bound(k) for k in range(3)]
+    ap = [b.perf(k)[2] for k in range(3)]
     b.step(1)
     for k in range(3):
         x = b.kj_features(k)
@@ -44,7 +47,7 @@ def test_features_and_start_value_match_host(wb):
         xh = synth.kj_features(kjs[k], 0, prev[k])
         np.testing.assert_allclose(x, xh, rtol=2e-6, atol=1e-6)
         g = b.kj_guess(k)
-        lift = _lift(gi, kjs[k], cases[k]["nb"])
+        lift = _lift(gi, kjs[k], cases[k]["nb"], ap[k])
         assert lift.any() and not lift.all()
         gh = prev[k].ravel(order="F") + lift * float(np.float32(0.7)) * m.forward(x).astype(np.float64)
         np.testing.assert_allclose(g.ravel(order="F"), gh, rtol=1e-12, atol=1e-9)
@@ -83,20 +86,22 @@ def test_extrapolated_base_start_value(wb):
     b.set_mlp(m)
     for _ in range(2):
         prev = [b.bound(k) for k in range(3)]
+        ap = [b.perf(k)[2] for k in range(3)]
         b.step(1, graph=True)
         for k in range(3):
             x = b.kj_features(k)
-            lift = _lift(gi, kjs[k], cases[k]["nb"])
+            lift = _lift(gi, kjs[k], cases[k]["nb"], ap[k])
             gh = prev[k].ravel(order="F") + lift * (
                 x[:, 9].astype(np.float64) + float(np.float32(0.05)) * m.forward(x).astype(np.float64))
             np.testing.assert_allclose(b.kj_guess(k).ravel(order="F"), gh, rtol=1e-12, atol=1e-9)
     xo = gi.extrapolation_only()
     b.set_mlp(xo)
     prev = [b.bound(k) for k in range(3)]
+    ap = [b.perf(k)[2] for k in range(3)]
     b.step(1)
     for k in range(3):
         x = b.kj_features(k)
-        lift = _lift(gi, kjs[k], cases[k]["nb"])
+        lift = _lift(gi, kjs[k], cases[k]["nb"], ap[k])
         np.testing.assert_array_equal(b.kj_guess(k).ravel(order="F"),
                                       np.where(lift, prev[k].ravel(order="F") + x[:, 9].astype(np.float64),
                                                prev[k].ravel(order="F")))
@@ -126,11 +131,12 @@ def test_graph_with_network_matches_host_loop(wb):
     b.set_mlp(m)
     b.step(1, graph=True)
     prev = [b.bound(k) for k in range(3)]
+    ap = [b.perf(k)[2] for k in range(3)]
     m.set_scaling(np.zeros(gi.N_FEATURES, np.float32), np.full(gi.N_FEATURES, 0.2, np.float32), 0.3)
     b.step(1, graph=True)
     for k in range(3):
         x = b.kj_features(k)
-        lift = _lift(gi, kjs[k], cases[k]["nb"])
+        lift = _lift(gi, kjs[k], cases[k]["nb"], ap[k])
         gh = prev[k].ravel(order="F") + lift * float(np.float32(0.3)) * m.forward(x).astype(np.float64)
         np.testing.assert_allclose(b.kj_guess(k).ravel(order="F"), gh, rtol=1e-12, atol=1e-9)
     b.close()

@@ -130,14 +130,20 @@ __global__ void kj_features(const WakeCase *cases, const KJCase *kc, const int *
 }
 
 // bound = base + out_scale * y, base Gamma_prev or, with *base != 0, its
-// extrapolation Gamma_prev + dGamma_prev (feature 9 of the row). Stations
-// whose airfoil table has no lift (st_lift 0: Cl = 0 at every AoA, e.g. the
-// cylinder root sections) keep Gamma_prev: their fixed point is Gamma = 0,
-// the previous step already sits there, and the relaxed iteration damps any
-// start error at such a station only by (1 - relax) per iteration.
+// extrapolation Gamma_prev + dGamma_prev (feature 9 of the row). Two kinds of
+// station keep Gamma_prev: those whose airfoil table has no lift (st_lift 0:
+// Cl = 0 at every AoA, e.g. the cylinder root sections; their fixed point is
+// Gamma = 0, the previous step already sits there, and the relaxed iteration
+// damps any start error there by only 1 - relax per iteration), and those
+// whose last converged AoA (aoa_prev) lies outside their table's stall bounds
+// st_stall (the AoA of its lowest and highest Cl) less kStallMargin degrees:
+// past stall a station can have more than one fixed point, and the previous
+// step's value is the start that keeps the branch it is on.
 // Nothing before the step the iteration starts at (WakeCase::kj_from).
+constexpr double kStallMargin = 2.0;  // degrees
 __global__ void kj_apply_guess(const WakeCase *cases, const KJCase *kc, const int *step,
-                               const int *st_lift, const float *y, const float *out_scale,
+                               const int *st_lift, const double2 *st_stall,
+                               const double *aoa_prev, const float *y, const float *out_scale,
                                const float *feat, const float *base, double *bound) {
   const WakeCase c = cases[blockIdx.y];
   const KJCase k = kc[blockIdx.y];
@@ -146,6 +152,9 @@ __global__ void kj_apply_guess(const WakeCase *cases, const KJCase *kc, const in
   if (t >= ns * c.nb || *step < c.kj_from) return;
   const int i = t % ns, b = t / ns;
   if (!st_lift[k.station_off + i]) return;
+  const double2 sb = st_stall[k.station_off + i];
+  const double ap = aoa_prev[c.bound_off + i + (long long)ns * b];
+  if (!(ap > sb.x + kStallMargin && ap < sb.y - kStallMargin)) return;
   double g = bound[c.bound_off + i + (long long)ns * b];
   if (*base != 0.f) g += (double)feat[(k.t_off + t) * kKJFeatures + 9];
   bound[c.bound_off + i + (long long)ns * b] = g + (double)*out_scale * (double)y[k.t_off + t];
@@ -313,11 +322,12 @@ cudaError_t launch_kj_features(const WakeCase *cases, const KJCase *kc, int ncas
 }
 
 cudaError_t launch_kj_apply_guess(const WakeCase *cases, const KJCase *kc, int ncases, int max_st,
-                                  const int *step, const int *st_lift, const float *y,
-                                  const float *out_scale, const float *feat, const float *base,
-                                  double *bound, cudaStream_t s) {
-  kj_apply_guess<<<dim3((max_st + 127) / 128, ncases), 128, 0, s>>>(cases, kc, step, st_lift, y,
-                                                                    out_scale, feat, base, bound);
+                                  const int *step, const int *st_lift, const double2 *st_stall,
+                                  const double *aoa_prev, const float *y, const float *out_scale,
+                                  const float *feat, const float *base, double *bound,
+                                  cudaStream_t s) {
+  kj_apply_guess<<<dim3((max_st + 127) / 128, ncases), 128, 0, s>>>(
+      cases, kc, step, st_lift, st_stall, aoa_prev, y, out_scale, feat, base, bound);
   return cudaGetLastError();
 }
 

@@ -48,11 +48,13 @@ cudaError_t launch_kj_features(const WakeCase *cases, const KJCase *kc, int ncas
                                float *x, cudaStream_t s);
 // bound = base + out_scale * y (row order of the lifting-line targets); base
 // Gamma_prev, or Gamma_prev + feature 9 (its change) when *base != 0;
-// stations with st_lift 0 (no lift in their table) keep Gamma_prev
+// stations with st_lift 0 (no lift in their table), or whose last AoA
+// (aoa_prev) is outside their table's stall bounds st_stall, keep Gamma_prev
 cudaError_t launch_kj_apply_guess(const WakeCase *cases, const KJCase *kc, int ncases, int max_st,
-                                  const int *step, const int *st_lift, const float *y,
-                                  const float *out_scale, const float *feat, const float *base,
-                                  double *bound, cudaStream_t s);
+                                  const int *step, const int *st_lift, const double2 *st_stall,
+                                  const double *aoa_prev, const float *y, const float *out_scale,
+                                  const float *feat, const float *base, double *bound,
+                                  cudaStream_t s);
 // Rotor thrust, torque and power of every case at the step
 // (postproc/perform.m:18-62): out[3*case + {0,1,2}] = T, Q, P; dl [rows][3]
 // holds the spanwise terms.

@@ -80,7 +80,8 @@ struct winds_wake_batch {
   bool loads = false;           // every case gave the loads inputs
   DevBuf st_rr, st_dr, rpm, pitch, dl, loads_out;
   DevBuf st_r, st_c, st_tw, azim, guess, feat, bound_last, bound_last2;
-  DevBuf st_lift;  // per station: 1 when its airfoil table has lift (start value applies)
+  DevBuf st_lift;   // per station: 1 when its airfoil table has lift (start value applies)
+  DevBuf st_stall;  // per station: AoA (deg) of its table's lowest and highest Cl
   winds_mlp *mlp = nullptr;
   MlpWork mw;
   cudaGraphExec_t exec_pre = nullptr, exec_kj = nullptr, exec_post = nullptr;
@@ -474,7 +475,8 @@ cudaError_t enqueue_kj_begin(winds_wake_batch *b) {
       e = cudaErrorLaunchFailure;
     if (e == cudaSuccess)
       e = launch_kj_apply_guess(cd, kd, b->ncases, b->max_st, P<const int>(b->step_d),
-                                P<const int>(b->st_lift), P<const float>(b->mw.y),
+                                P<const int>(b->st_lift), P<const double2>(b->st_stall),
+                                P<const double>(b->aoa_o), P<const float>(b->mw.y),
                                 mlp_out_scale_dev(b->mlp),
                                 P<const float>(b->feat), mlp_base_dev(b->mlp), P<double>(b->bound),
                                 s);
@@ -1082,6 +1084,7 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
   long long fr = 0, tt = 0, st = 0, tab = 0, az = 0, rp = 0;
   bool all_inputs = true, have_twist = true, all_loads = true, any_pitch = false;
   std::vector<int> foil_off, foils, lift;
+  std::vector<double2> stall;
   std::vector<double> aoa, cl, cd, chord;
   b->max_st = 0;
   b->max_bound_cols = 0;
@@ -1120,15 +1123,26 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
     }
     // tables with lift (some Cl != 0); a station on a table without keeps its
     // previous circulation as the start value
+    // and the stall bounds of each table: the AoA of its highest Cl above
+    // 0 deg and of its lowest Cl below (within +-45 deg)
     std::vector<int> has_lift(h.n_foils, 0);
-    for (int f = 0, j = 0; f < h.n_foils; ++f)
-      for (int e = 0; e < h.foil_points[f]; ++e, ++j)
+    std::vector<double2> bounds(h.n_foils);
+    for (int f = 0, j = 0; f < h.n_foils; ++f) {
+      double hi_cl = -1e300, lo_cl = 1e300, hi_a = 45.0, lo_a = -45.0;
+      for (int e = 0; e < h.foil_points[f]; ++e, ++j) {
         if (h.cl[j] != 0.0) has_lift[f] = 1;
+        const double a = h.aoa[j];
+        if (a >= 0.0 && a <= 45.0 && h.cl[j] > hi_cl) hi_cl = h.cl[j], hi_a = a;
+        if (a <= 0.0 && a >= -45.0 && h.cl[j] < lo_cl) lo_cl = h.cl[j], lo_a = a;
+      }
+      bounds[f] = make_double2(lo_a, hi_a);
+    }
     for (int i = 0; i < ns; ++i) {
       if (h.foil[i] < 0 || h.foil[i] >= h.n_foils)
         return fail(WINDS_BS_ERR_ARG, "case %d: station %d uses airfoil %d of %d", k, i, h.foil[i], h.n_foils);
       foils.push_back(h.foil[i]);
       lift.push_back(has_lift[h.foil[i]]);
+      stall.push_back(bounds[h.foil[i]]);
       chord.push_back(h.chord[i]);
     }
     tab += o;
@@ -1148,6 +1162,7 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
   if ((rc = b->kjc_d.ensure(b->ncases * sizeof(KJCase), s)) ||
       (rc = b->chord.ensure(st * sizeof(double), s)) || (rc = b->foil.ensure(st * sizeof(int), s)) ||
       (rc = b->st_lift.ensure(st * sizeof(int), s)) ||
+      (rc = b->st_stall.ensure(st * sizeof(double2), s)) ||
       (rc = b->foil_off.ensure(foil_off.size() * sizeof(int), s)) ||
       (rc = b->aoa_t.ensure(tab * sizeof(double), s)) || (rc = b->cl_t.ensure(tab * sizeof(double), s)) ||
       (rc = b->cd_t.ensure(tab * sizeof(double), s)) || (rc = b->tp_ll.ensure(tt * sizeof(double4), s)) ||
@@ -1244,6 +1259,8 @@ int winds_wake_set_kj(winds_wake_batch *b, const winds_kj_case *kj, const winds_
   if (e == cudaSuccess) e = cudaMemcpy(b->chord.p, chord.data(), st * sizeof(double), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(b->foil.p, foils.data(), st * sizeof(int), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(b->st_lift.p, lift.data(), st * sizeof(int), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(b->st_stall.p, stall.data(), st * sizeof(double2), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(b->foil_off.p, foil_off.data(), foil_off.size() * sizeof(int), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(b->aoa_t.p, aoa.data(), tab * sizeof(double), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(b->cl_t.p, cl.data(), tab * sizeof(double), cudaMemcpyHostToDevice);
@@ -1402,6 +1419,7 @@ void winds_wake_destroy(winds_wake_batch *b) {
   if (b->body_stream) cudaStreamDestroy(b->body_stream);
   b->kj_it.release();
   b->st_lift.release();
+  b->st_stall.release();
   for (DevBuf *x : {&b->kjc_d, &b->ll, &b->bxn, &b->byn, &b->bzn, &b->vblade, &b->chord, &b->foil,
                     &b->foil_off, &b->aoa_t, &b->cl_t, &b->cd_t, &b->tp_ll, &b->perm_ll, &b->uindb,
                     &b->kj_groups, &b->kj_tiles, &b->kj_items, &b->kj_order, &b->kj_part,

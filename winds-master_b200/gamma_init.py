@@ -27,10 +27,13 @@ line), the previous bound circulation, its change over the previous step and
 the change over the step before that (with which the network can form a
 second-order extrapolation).
 Training pairs come only from (case, step) whose plain iteration converged,
-and only from lifting stations: a station whose airfoil table has no lift
-(the cylinder root sections) converges to Gamma = 0, the engine keeps its
-previous value as the start, and any other start there costs iterations
-(the relaxed iteration damps it by only 1 - relax per iteration).
+and only from the stations the start value applies to (``start_rows``):
+lifting stations whose previous converged AoA is inside their table's stall
+bounds. A station whose airfoil table has no lift (the cylinder root
+sections) converges to Gamma = 0, and any start there but the previous value
+costs iterations (the relaxed iteration damps it by only 1 - relax per
+iteration); a station past stall can have more than one fixed point, and the
+previous value keeps the branch it is on.
 """
 from __future__ import annotations
 
@@ -71,13 +74,41 @@ def operating_points(n: int, seed: int, nst: int = 41, wake_steps: int = 36,
     return out
 
 
+STALL_MARGIN = 2.0  # degrees inside the stall bounds (kj_kernels.cu: kStallMargin)
+
+
 def lifting_stations(kj: dict) -> np.ndarray:
-    """[ns] bool: the stations whose airfoil table has some Cl != 0 (the
-    stations the engine's start value applies to)."""
+    """[ns] bool: the stations whose airfoil table has some Cl != 0."""
     offs = np.concatenate([[0], np.cumsum(kj["foil_points"])])
     lift = np.array([np.any(np.asarray(kj["cl"])[offs[f]:offs[f + 1]] != 0.0)
                      for f in range(len(kj["foil_points"]))])
     return lift[np.asarray(kj["foil"])]
+
+
+def stall_bounds(kj: dict) -> np.ndarray:
+    """[ns, 2]: per station, the AoA (deg) of its table's lowest Cl in
+    [-45, 0] and highest Cl in [0, 45] deg, as the engine computes them."""
+    offs = np.concatenate([[0], np.cumsum(kj["foil_points"])])
+    out = []
+    for f in range(len(kj["foil_points"])):
+        a = np.asarray(kj["aoa"])[offs[f]:offs[f + 1]]
+        c = np.asarray(kj["cl"])[offs[f]:offs[f + 1]]
+        hi, lo = (a >= 0) & (a <= 45), (a <= 0) & (a >= -45)
+        ahi = a[hi][np.argmax(c[hi])] if hi.any() else 45.0
+        alo = a[lo][np.argmin(c[lo])] if lo.any() else -45.0
+        out.append((alo, ahi))
+    return np.asarray(out)[np.asarray(kj["foil"])]
+
+
+def start_rows(kj: dict, nb: int, aoa_prev) -> np.ndarray:
+    """[ns*nb] bool (rows i + ns*b): where the engine's start value applies
+    -- lifting stations whose last converged AoA ``aoa_prev`` [ns, nb] lies
+    inside their table's stall bounds less STALL_MARGIN; elsewhere the start
+    is the previous step's circulation."""
+    sb = stall_bounds(kj)
+    ap = np.asarray(aoa_prev, np.float64)
+    inside = (ap > sb[:, :1] + STALL_MARGIN) & (ap < sb[:, 1:] - STALL_MARGIN)
+    return (inside & lifting_stations(kj)[:, None]).ravel(order="F")
 
 
 def build(points, run_steps: int, root_cut: float = ROOT_CUT):
@@ -112,7 +143,7 @@ def run(points, run_steps: int, relax=0.3, tol=1e-6, maxiter=100, mlp=None, prec
     bounds = []
     X, dG, tag, lrows = [], [], [], []
     nbs = [c["nb"] for c in cases]
-    lift_rows = [np.tile(lifting_stations(kj), nb) for kj, nb in zip(kjs, nbs)]
+    aoa_prev = [np.zeros((c["nst"] - 1, c["nb"])) for c in cases]  # the engine's before step 0
     t0 = time.perf_counter()
     for s in range(run_steps):
         b.step(1, graph=graph)
@@ -121,9 +152,9 @@ def run(points, run_steps: int, relax=0.3, tol=1e-6, maxiter=100, mlp=None, prec
         evals[s] = ev
         thrust[s], _, power[s] = b.loads()
         conv = [b.bound(k) for k in range(n)]
+        aoas = [b.perf(k)[2] for k in range(n)]
         for k in range(n):
-            aoa = b.perf(k)[2]
-            aoa_max[k] = max(aoa_max[k], float(np.nanmax(np.abs(aoa[lifting[k]]))))
+            aoa_max[k] = max(aoa_max[k], float(np.nanmax(np.abs(aoas[k][lifting[k]]))))
         if record:
             for k in range(n):
                 if it[k] < maxiter:  # converged pairs only
@@ -131,7 +162,8 @@ def run(points, run_steps: int, relax=0.3, tol=1e-6, maxiter=100, mlp=None, prec
                     X.append(x)
                     dG.append(conv[k].ravel(order="F") - x[:, 8].astype(np.float64))
                     tag.append(np.full((x.shape[0], 2), (s, k), dtype=np.int32))
-                    lrows.append(lift_rows[k])
+                    lrows.append(start_rows(kjs[k], nbs[k], aoa_prev[k]))
+        aoa_prev = aoas
         bounds.append(conv)
     wall = time.perf_counter() - t0
     b.close()
@@ -182,7 +214,7 @@ def train(X, dG, epochs=30, batch=4096, lr=2e-3, seed=0, weight_decay=0.0, base=
 
 
 def choose_shrink(m, points, run_steps, skip=4, alphas=(0.0, 0.25, 0.5, 0.75, 1.0), guard=1e-2,
-                  **kw):
+                  guard_thrust=1e-3, **kw):
     """Scales the network's output by the alpha of ``alphas`` whose start
     value needs the fewest iterations (steps >= ``skip``, (step, case) pairs
     converged under every alpha) when the solver actually runs on
@@ -194,10 +226,11 @@ def choose_shrink(m, points, run_steps, skip=4, alphas=(0.0, 0.25, 0.5, 0.75, 1.
 
     A candidate counts only if, at the last step, every case ends within
     ``guard`` (relative to its largest |Gamma| + 1) of the bound circulation
-    that the reference's previous-step start reaches: past stall a station
+    that the reference's previous-step start reaches, and its rotor thrust
+    within ``guard_thrust`` (relative) of that run's: past stall a station
     can have two fixed points and another start may select the other one
-    (a difference of percent, where converged starts otherwise agree to
-    ~1e-4). If no candidate passes, the network falls back to the
+    (thrust percent apart, where starts on the same branch drift apart by a
+    few 1e-4 over a run at tol 1e-6). If no candidate passes, the network falls back to the
     previous-step base with alpha = 0 (the reference's start). Sets
     ``m.shrink`` (and ``m.base``); ``m.validation`` lists (alpha, iterations,
     largest difference) per candidate."""
@@ -210,13 +243,16 @@ def choose_shrink(m, points, run_steps, skip=4, alphas=(0.0, 0.25, 0.5, 0.75, 1.
         return max(float(np.abs(np.asarray(x) - np.asarray(y)).max() / (np.abs(np.asarray(y)).max() + 1.0))
                    for x, y in zip(r["bounds"][-1], ref["bounds"][-1]))
 
+    def thrust_difference(r):
+        return float(np.max(np.abs(r["thrust"][-1] - ref["thrust"][-1]) / np.abs(ref["thrust"][-1])))
+
     its, valid, diffs = [], [], []
     for a in alphas:
         m.set_scaling(shift, scale, full * a)
         r = run(points, run_steps, mlp=m, **kw)
         its.append(r["iters"])
         diffs.append(largest_difference(r))
-        valid.append(diffs[-1] <= guard)
+        valid.append(diffs[-1] <= guard and thrust_difference(r) <= guard_thrust)
     ok = np.ones_like(its[0], dtype=bool)
     for it in its:
         ok &= it < maxiter
