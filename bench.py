@@ -473,7 +473,7 @@ def kj_mlp_bench():
 
 
 # ------------------------------------------------------------------ end to end
-def e2e_run_bench(steps, ncases=16, ages=1440, seed=5, plain_cases=4):
+def e2e_run_bench(steps, ncases=16, ages=1440, seed=5, plain_cases=2):
     """16 rotor cases, 3 blades x 41 nodes, wake truncated at 1440 steps of
     1 deg, U = 11.4 m/s, shear 0.2, yaw 0-30 deg, pcc with the lifting-line
     iteration (tol 1e-6) and rotor loads every step, ``steps`` steps per path.
