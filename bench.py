@@ -343,16 +343,16 @@ def sharded_wake_bench(args, rank, world, seed=2, ncases=64):
 def batch_start_value(seed=12, n_train=48, n_val=8, steps=10, relax=0.3, tol=1e-6, maxiter=200):
     """A start-value network for the 64-case mix: pairs from the plain solver
     on other draws of the same case distribution (batch_cases, no root
-    cylinders), extrapolated base, output scale chosen on validation draws."""
+    cylinders); of a network on the previous-step base and one on the
+    extrapolated base, each with its output scale chosen on validation draws,
+    the one that saves more iterations there."""
     synth = importlib.import_module("winds-master_b200.synth")
     gi = importlib.import_module("winds-master_b200.gamma_init")
     kw = dict(relax=relax, tol=tol, maxiter=maxiter, root_cut=0.0)
     pts = [gi.OperatingPoint(rc, 0.0) for rc in synth.batch_cases(n_train + n_val, seed=seed)]
     tr = gi.run(pts[:n_train], steps, record=True, **kw)
     keep = (tr["step_case"][:, 0] >= 4) & tr["lift"]
-    m, _ = gi.train(tr["X"][keep], tr["dG"][keep], epochs=40, base="extrapolated")
-    gi.choose_shrink(m, pts[n_train:], steps, **kw)
-    return m
+    return gi.fit_start_value(tr["X"][keep], tr["dG"][keep], pts[n_train:], steps, **kw)
 
 
 def wake_kj_bench(rcases, cases, tol=1e-6, relax=0.3, maxiter=200, warm=3, timed=3, mlp=None):
@@ -478,11 +478,12 @@ def e2e_run_bench(steps, ncases=16, ages=1440, seed=5, plain_cases=2):
     1 deg, U = 11.4 m/s, shear 0.2, yaw 0-30 deg, pcc with the lifting-line
     iteration (tol 1e-6) and rotor loads every step, ``steps`` steps per path.
     Fast: the FP32-compensated batch with graph replay, started from the
-    network (previous-step base, trained here on plain-solver pairs of the
-    same conditions with 120-step wakes, its output scale chosen on
-    validation runs that must keep the reference start's fixed point; the
-    start applies only at stations inside their polar's stall bounds), from
-    the previous step's circulation, and from its extrapolation alone.
+    network (trained here on plain-solver pairs of the same conditions with
+    120-step wakes; of a network on the previous-step base and one on the
+    extrapolated base, the one that saves more on validation runs that must
+    keep the reference start's fixed point; the start applies only at
+    stations inside their polar's stall bounds), from the previous step's
+    circulation, and from its extrapolation alone.
     Plain FP64 (FP64 direct sum, previous-step start, each case alone, no
     graphs) runs ``plain_cases`` of the 16 cases (every 16/plain_cases-th:
     the same size as every other case, so its time per case scales to the
@@ -503,13 +504,12 @@ def e2e_run_bench(steps, ncases=16, ages=1440, seed=5, plain_cases=2):
     t0 = time.perf_counter()
     tr = gi.run(points(120, rng.uniform(0.0, 30.0, 64), 900), 48, record=True, maxiter=200)
     keep = (tr["step_case"][:, 0] >= 4) & tr["lift"]
-    # the previous-step base: these cases have stations past stall, where the
-    # extrapolated start moves some cases to another fixed point (thrust
-    # percent off the plain path) even with the stall mask
-    m, _ = gi.train(tr["X"][keep], tr["dG"][keep], epochs=40, base="previous")
-    # output scale from solver runs on validation points of the same conditions
-    gi.choose_shrink(m, points(120, rng.uniform(0.0, 30.0, 8), 950), 16, maxiter=200)
-    mlp_base, mlp_shrink, mlp_val = m.base, m.shrink, m.validation
+    # a network per base, output scales from solver runs on validation points
+    # of the same conditions (whose guards reject a start that selects another
+    # fixed point at stalled stations); the one that saves more is kept
+    m = gi.fit_start_value(tr["X"][keep], tr["dG"][keep], points(120, rng.uniform(0.0, 30.0, 8), 950),
+                           16, maxiter=200)
+    mlp_base, mlp_shrink, mlp_val, mlp_tried = m.base, m.shrink, m.validation, m.bases_tried
     train_s = time.perf_counter() - t0
     pts = points(ages, yaws, 100)
     cases, kjs = gi.build(pts, steps + 1)
@@ -583,7 +583,7 @@ def e2e_run_bench(steps, ncases=16, ages=1440, seed=5, plain_cases=2):
             "thrust_history_N": f["T"].sum(1).round(1).tolist(),
             "power_history_W": f["P"].sum(1).round(1).tolist(),
             "mlp_training_s": round(train_s, 2), "mlp_base": mlp_base, "mlp_output_shrink": mlp_shrink,
-            "mlp_validation": mlp_val,
+            "mlp_validation": mlp_val, "mlp_bases_tried": mlp_tried,
             "timing": "CUDA events around each step (fast paths: the lifting-line loop runs inside "
             "the step's graph; plain path: the host waits on a per-iteration convergence flag, its "
             f"time per step measured on {len(p['idx'])} of the {ncases} equal-size cases and scaled "

@@ -107,3 +107,30 @@ def test_choose_shrink_rejects_a_thrust_jump(monkeypatch):
     monkeypatch.setattr(gi, "run", _fake_run(table))
     m = FakeMlp()
     assert gi.choose_shrink(m, [], 6, skip=4) == 0.5
+
+
+def test_fit_start_value_keeps_the_base_that_saves_more(monkeypatch):
+    """One network per base; the one whose chosen output scale saves more
+    validation iterations is kept, the other is closed."""
+    gi = importlib.import_module("winds-master_b200.gamma_init")
+    closed = []
+
+    class Net(FakeMlp):
+        def close(self):
+            closed.append(self.base)
+
+    def train(X, dG, epochs=30, base="previous", seed=0, **kw):
+        return Net(base), None
+
+    def choose_shrink(m, points, steps, **kw):
+        m.validation_reference = 100
+        m.validation_chosen = {"previous": 90, "extrapolated": 80}[m.base]
+        m.shrink = 0.5
+        return m.shrink
+
+    monkeypatch.setattr(gi, "train", train)
+    monkeypatch.setattr(gi, "choose_shrink", choose_shrink)
+    m = gi.fit_start_value(None, None, [], 6)
+    assert m.base == "extrapolated" and closed == ["previous"]
+    assert [(b, round(s, 6)) for b, _, _, s in m.bases_tried] == [("previous", 0.1),
+                                                                   ("extrapolated", 0.2)]

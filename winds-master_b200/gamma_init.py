@@ -253,19 +253,48 @@ def choose_shrink(m, points, run_steps, skip=4, alphas=(0.0, 0.25, 0.5, 0.75, 1.
         its.append(r["iters"])
         diffs.append(largest_difference(r))
         valid.append(diffs[-1] <= guard and thrust_difference(r) <= guard_thrust)
-    ok = np.ones_like(its[0], dtype=bool)
+    ok = ref["iters"] < maxiter
     for it in its:
         ok &= it < maxiter
     ok[:skip] = False
     tot = [int(it[ok].sum()) if v else np.iinfo(np.int64).max for it, v in zip(its, valid)]
     m.validation = [(float(a), int(it[ok].sum()), d) for a, it, d in zip(alphas, its, diffs)]
+    # iterations of the previous-step start over the same steps, and the chosen start's
+    m.validation_reference = int(ref["iters"][ok].sum())
     if any(valid):
-        m.shrink = float(alphas[int(np.argmin(tot))])
+        k = int(np.argmin(tot))
+        m.shrink = float(alphas[k])
+        m.validation_chosen = tot[k]
     else:
         m.set_base("previous")
         m.shrink = 0.0
+        m.validation_chosen = m.validation_reference
     m.set_scaling(shift, scale, full * m.shrink)
     return m.shrink
+
+
+def fit_start_value(X, dG, val_points, val_steps, bases=("previous", "extrapolated"), epochs=40,
+                    seed=0, **kw):
+    """One network per base trained on the pairs (X, dG), each output scale
+    chosen on ``val_points`` (``choose_shrink``, with its guards); keeps the
+    network whose chosen start saves the most iterations against the
+    previous-step start on those validation runs. Returns it with
+    ``m.bases_tried`` = [(base trained, base kept after the guards, output
+    scale, fraction of validation iterations saved)]."""
+    best, tried = None, []
+    for base in bases:
+        m, _ = train(X, dG, epochs=epochs, base=base, seed=seed)
+        choose_shrink(m, val_points, val_steps, **kw)
+        saving = 1.0 - m.validation_chosen / max(m.validation_reference, 1)
+        tried.append((base, m.base, m.shrink, saving))
+        if best is None or saving > best[1]:
+            if best is not None:
+                best[0].close()
+            best = (m, saving)
+        else:
+            m.close()
+    best[0].bases_tried = tried
+    return best[0]
 
 
 def extrapolation_only():
