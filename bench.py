@@ -448,6 +448,10 @@ def wake_kj_bench(rcases, cases, tol=1e-6, relax=0.3, maxiter=200, warm=3, timed
             "kj_iterations_converged_subset": int(r["iters"][conv].sum()),
             "lifting_line_evaluations": int(r["evals"]), "steps_per_s": 1000.0 / r["ms"],
             "thrust_rel_diff_vs_previous_max": float(dTa[ok].max()) if ok.any() else None}
+    if mlp is not None:
+        out["start_value_arms"]["network"].update(
+            {"base": mlp.base, "output_shrink": mlp.shrink,
+             "bases_tried": getattr(mlp, "bases_tried", None)})
     return out
 
 
