@@ -217,21 +217,24 @@ def choose_shrink(m, points, run_steps, skip=4, alphas=(0.0, 0.25, 0.5, 0.75, 1.
                   guard_thrust=1e-3, **kw):
     """Scales the network's output by the alpha of ``alphas`` whose start
     value needs the fewest iterations (steps >= ``skip``, (step, case) pairs
-    converged under every alpha) when the solver actually runs on
+    converged under the reference and every valid alpha) when the solver actually runs on
     ``points`` -- validation points kept out of the training pairs. The
     stopping rule sees the largest spanwise residual, and how fast the fixed
     point damps a start error depends on its spanwise shape, so no error
     norm of the start value predicts this as well as the iteration itself.
     alpha = 0 leaves the base alone.
 
-    A candidate counts only if, at the last step, every case ends within
-    ``guard`` (relative to its largest |Gamma| + 1) of the bound circulation
-    that the reference's previous-step start reaches, and its rotor thrust
-    within ``guard_thrust`` (relative) of that run's: past stall a station
-    can have two fixed points and another start may select the other one
-    (thrust percent apart, where starts on the same branch drift apart by a
-    few 1e-4 over a run at tol 1e-6). If no candidate passes, the network falls back to the
-    previous-step base with alpha = 0 (the reference's start). Sets
+    A candidate counts only if, at the last step, every case that reached
+    its fixed point under the reference's previous-step start reaches one
+    under the candidate too, within ``guard`` (relative to its largest
+    |Gamma| + 1) of the reference's bound circulation and with its rotor
+    thrust within ``guard_thrust`` (relative): past stall a station can have
+    two fixed points and another start may select the other one (thrust
+    percent apart, where starts on the same branch drift apart by a few 1e-4
+    over a run at tol 1e-6). A case that stopped at ``maxiter`` under the
+    reference has no fixed point to compare against and is not compared. If
+    no candidate passes, the network falls back to the previous-step base
+    with alpha = 0 (the reference's start). Sets
     ``m.shrink`` (and ``m.base``); ``m.validation`` lists (alpha, iterations,
     largest difference) per candidate."""
     shift, scale, _ = m.scaling()
@@ -239,12 +242,15 @@ def choose_shrink(m, points, run_steps, skip=4, alphas=(0.0, 0.25, 0.5, 0.75, 1.
     maxiter = kw.get("maxiter", 200)
     ref = run(points, run_steps, **kw)
 
+    fixed = np.asarray(ref["iters"][-1]) < maxiter  # cases at a fixed point at the last step
+
     def largest_difference(r):
-        return max(float(np.abs(np.asarray(x) - np.asarray(y)).max() / (np.abs(np.asarray(y)).max() + 1.0))
-                   for x, y in zip(r["bounds"][-1], ref["bounds"][-1]))
+        return max((float(np.abs(np.asarray(x) - np.asarray(y)).max() / (np.abs(np.asarray(y)).max() + 1.0))
+                    for x, y, f in zip(r["bounds"][-1], ref["bounds"][-1], fixed) if f), default=0.0)
 
     def thrust_difference(r):
-        return float(np.max(np.abs(r["thrust"][-1] - ref["thrust"][-1]) / np.abs(ref["thrust"][-1])))
+        d = np.abs(r["thrust"][-1] - ref["thrust"][-1]) / np.abs(ref["thrust"][-1])
+        return float(d[fixed].max()) if fixed.any() else 0.0
 
     its, valid, diffs = [], [], []
     for a in alphas:
@@ -252,10 +258,12 @@ def choose_shrink(m, points, run_steps, skip=4, alphas=(0.0, 0.25, 0.5, 0.75, 1.
         r = run(points, run_steps, mlp=m, **kw)
         its.append(r["iters"])
         diffs.append(largest_difference(r))
-        valid.append(diffs[-1] <= guard and thrust_difference(r) <= guard_thrust)
-    ok = ref["iters"] < maxiter
-    for it in its:
-        ok &= it < maxiter
+        keeps = bool(np.all(np.asarray(r["iters"][-1])[fixed] < maxiter))
+        valid.append(keeps and diffs[-1] <= guard and thrust_difference(r) <= guard_thrust)
+    ok = ref["iters"] < maxiter  # (step, case) pairs converged under the reference and every valid candidate
+    for it, v in zip(its, valid):
+        if v:
+            ok &= it < maxiter
     ok[:skip] = False
     tot = [int(it[ok].sum()) if v else np.iinfo(np.int64).max for it, v in zip(its, valid)]
     m.validation = [(float(a), int(it[ok].sum()), d) for a, it, d in zip(alphas, its, diffs)]
