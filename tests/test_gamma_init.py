@@ -136,27 +136,21 @@ def test_fit_start_value_keeps_the_base_that_saves_more(monkeypatch):
                                                                    ("extrapolated", 0.2)]
 
 
-def test_choose_shrink_compares_fixed_points_only(monkeypatch):
-    """A case that stops at maxiter under the reference start (no fixed point)
-    is not compared; a candidate that leaves a converged case at maxiter is
-    rejected."""
+def test_choose_shrink_keeps_convergence(monkeypatch):
+    """A candidate that leaves a case the reference start converged at
+    maxiter is rejected, and the iterations are compared over the pairs that
+    converged under the reference and every valid candidate."""
     gi = importlib.import_module("winds-master_b200.gamma_init")
 
     def run(points, steps, mlp=None, **kw):
         key = None if mlp is None else round(mlp.out / mlp.full_out_scale, 2)
-        its = [[9, 9]] * 5 + [[40, 200]]
-        bounds = [10.0, 20.0], [5.0, 7.0]
-        thrust = [1.0, 1.0]
-        if key == 0.25:  # fastest, but case 0 no longer converges
-            its = [[9, 9]] * 5 + [[200, 200]]
-        elif key is not None:
-            its = [[9, 9]] * 5 + [[{0.0: 30, 0.5: 25, 0.75: 35, 1.0: 50}[key], 200]]
-            bounds = [10.0, 20.0], [9.0, 3.0]  # the stalled case ends elsewhere
-            thrust = [1.0, 1.3]
-        return {"iters": np.array(its), "bounds": [[np.array(b) for b in bounds]],
-                "thrust": np.array([thrust])}
+        last = {None: [40, 40], 0.0: [30, 40], 0.25: [200, 20], 0.5: [25, 40], 0.75: [35, 40],
+                1.0: [50, 40]}[key]
+        return {"iters": np.array([[9, 9]] * 5 + [last]), "bounds": [[np.array([10.0, 20.0])] * 2],
+                "thrust": np.array([[1.0, 1.0]])}
 
     monkeypatch.setattr(gi, "run", run)
     m = FakeMlp()
+    # 0.25 is fastest on case 1 but leaves case 0 at maxiter: the next best valid is 0.5
     assert gi.choose_shrink(m, [], 6, skip=4) == 0.5
-    assert m.base == "extrapolated"
+    assert [v[1] for v in m.validation][2] == 18 + 25 + 40

@@ -226,13 +226,14 @@ def choose_shrink(m, points, run_steps, skip=4, alphas=(0.0, 0.25, 0.5, 0.75, 1.
 
     A candidate counts only if, at the last step, every case that reached
     its fixed point under the reference's previous-step start reaches one
-    under the candidate too, within ``guard`` (relative to its largest
-    |Gamma| + 1) of the reference's bound circulation and with its rotor
-    thrust within ``guard_thrust`` (relative): past stall a station can have
-    two fixed points and another start may select the other one (thrust
-    percent apart, where starts on the same branch drift apart by a few 1e-4
-    over a run at tol 1e-6). A case that stopped at ``maxiter`` under the
-    reference has no fixed point to compare against and is not compared. If
+    under the candidate too, and every case ends within ``guard`` (relative
+    to its largest |Gamma| + 1) of the reference's bound circulation with
+    its rotor thrust within ``guard_thrust`` (relative): past stall a station
+    can have two fixed points and another start may select the other one
+    (thrust percent apart, where starts on the same branch drift apart by a
+    few 1e-4 over a run at tol 1e-6). Cases that stop at ``maxiter`` are
+    compared too: comparing only the converged ones let a start through
+    that moved a converged case of a later run to the other fixed point. If
     no candidate passes, the network falls back to the previous-step base
     with alpha = 0 (the reference's start). Sets
     ``m.shrink`` (and ``m.base``); ``m.validation`` lists (alpha, iterations,
@@ -245,12 +246,11 @@ def choose_shrink(m, points, run_steps, skip=4, alphas=(0.0, 0.25, 0.5, 0.75, 1.
     fixed = np.asarray(ref["iters"][-1]) < maxiter  # cases at a fixed point at the last step
 
     def largest_difference(r):
-        return max((float(np.abs(np.asarray(x) - np.asarray(y)).max() / (np.abs(np.asarray(y)).max() + 1.0))
-                    for x, y, f in zip(r["bounds"][-1], ref["bounds"][-1], fixed) if f), default=0.0)
+        return max(float(np.abs(np.asarray(x) - np.asarray(y)).max() / (np.abs(np.asarray(y)).max() + 1.0))
+                   for x, y in zip(r["bounds"][-1], ref["bounds"][-1]))
 
     def thrust_difference(r):
-        d = np.abs(r["thrust"][-1] - ref["thrust"][-1]) / np.abs(ref["thrust"][-1])
-        return float(d[fixed].max()) if fixed.any() else 0.0
+        return float(np.max(np.abs(r["thrust"][-1] - ref["thrust"][-1]) / np.abs(ref["thrust"][-1])))
 
     its, valid, diffs = [], [], []
     for a in alphas:
