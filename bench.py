@@ -660,6 +660,7 @@ def ours(args):
         main_ms.append(m)
         launches += n
         near_pairs = near
+        free_pairs = wb.last_core_free()
     torch.cuda.synchronize()
     clk = clocks.stop()
     wb.sync(sp)
@@ -769,6 +770,8 @@ def ours(args):
             "speedup_vs_plain_fp64": (value / world / fp64) if fp64 else None,
             "rel_err_max_vs_fp64": rel_err,
             "near_pairs_per_step": near_pairs,
+            "core_free_pairs_per_step": free_pairs,
+            "core_free_fraction": free_pairs / interactions,
             "tiling": dict(zip(("targets_per_thread", "filaments_per_tile", "waves"),
                                wb.get_tuning(core, nt, nf))),
             "wake_batch": wake_line,

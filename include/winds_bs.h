@@ -137,6 +137,14 @@ int winds_bs_length_device(const double *F1, const double *F2, const long long d
  * the FP64 path). */
 int winds_bs_last_stats(double *main_ms, int *launches, long long *near_pairs);
 
+/* How many pairs of the last winds_bs_eval_host / winds_bs_eval_device call's
+ * FP32c Vatistas direct sum took the core-free form: pairs whose target lies
+ * at least 64 core radii from the filament's line (the screen of 32 filaments
+ * against a warp's 128 targets decides), where the core factor
+ * 1/sqrt(1 + (rc/h)^4) is within 3e-8 of 1 and the kernel leaves it out.
+ * 0 for the cut-off core and the FP64 path. */
+int winds_bs_last_core_free(long long *pairs);
+
 /* Synchronises `stream` (NULL: the library's stream) and reports a device-side
  * error (WINDS_BS_ERR_TIMEOUT for a bounded wait that ran out) recorded by an
  * earlier asynchronous call; the error word is cleared. */

@@ -252,3 +252,37 @@ def test_fp32_peak_probe(wb):
     t = C.c_double()
     assert wb.lib().winds_bs_fp32_peak(C.byref(t)) == 0
     assert 20.0 < t.value < 200.0
+
+
+def test_core_free_form(wb, oracle):
+    """Targets far from every filament line (more than 64 core radii, the
+    warp's ball included) take the core-free form for every pair, and match
+    the FP64 oracle; targets inside the cores take none of it. The counter
+    reports exactly the pairs that took the form."""
+    rng = np.random.default_rng(21)
+    nf = 256
+    a = np.linspace(0.0, 2 * np.pi, nf + 1)
+    ring = np.stack([10.0 * np.cos(a), 10.0 * np.sin(a), 0.2 * np.sin(5 * a)], 1)
+    F1 = np.asfortranarray(ring[:-1].reshape(nf, 3, 1, 1))
+    F2 = np.asfortranarray(ring[1:].reshape(nf, 3, 1, 1))
+    g = np.asfortranarray(rng.uniform(5.0, 15.0, (nf, 1, 1, 1)))
+    rc = np.full((nf, 1, 1, 1), 0.01, order="F")  # squared core: rc = 0.1 m
+    fams = [(F1, F2, g, rc)]
+    # far: a small cloud 300 m above the ring (the lines lie in the ring's plane)
+    Pf = np.asfortranarray((rng.uniform(-1.0, 1.0, (512, 3)) + [0.0, 0.0, 300.0]).reshape(512, 3, 1, 1))
+    u = wb.eval_host(fams, Pf, wb.bs.CORE_VATISTAS, 2.0, 1000.0, "f32c")
+    assert wb.last_core_free() == nf * 512
+    uo = oracle.c_eval(F1, F2, Pf, g, rc, "visc2", 1000.0)
+    # a closed ring seen from 30 radii away: its terms cancel to ~1/30 of
+    # their size, which scales the FP32 rounding (the omitted core factor
+    # differs from 1 by (0.1/300)^4 / 2 here)
+    assert per_target_rel(u, uo) < F32C_TOL
+    # near: targets on the ring, inside the cores of the nearby filaments
+    Pn = np.asfortranarray((ring[:-1] + rng.normal(0.0, 0.05, (nf, 3))).reshape(nf, 3, 1, 1))
+    u = wb.eval_host(fams, Pn, wb.bs.CORE_VATISTAS, 2.0, 1000.0, "f32c")
+    uo = oracle.c_eval(F1, F2, Pn, g, rc, "visc2", 1000.0)
+    assert per_target_rel(u, uo) < F32C_TOL
+    assert wb.last_core_free() < nf * nf
+    # the cut-off core has no such form
+    wb.eval_host(fams, Pf, wb.bs.CORE_CUTOFF, 1e-4, 1000.0, "f32c")
+    assert wb.last_core_free() == 0

@@ -26,6 +26,7 @@ from .bs import (  # noqa: F401
     eval_device,
     eval_host,
     last_stats,
+    last_core_free,
     lib,
     set_tuning,
     get_tuning,

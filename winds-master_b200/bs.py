@@ -69,6 +69,7 @@ def lib():
                                              C.c_void_p, C.c_void_p]
         L.winds_bs_last_stats.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_int),
                                           C.POINTER(C.c_longlong)]
+        L.winds_bs_last_core_free.argtypes = [C.POINTER(C.c_longlong)]
         L.winds_bs_sync.argtypes = [C.c_void_p]
         L.winds_bs_set_tuning.argtypes = [C.c_int, C.c_longlong, C.c_longlong, C.c_int, C.c_int,
                                           C.c_double]
@@ -175,6 +176,14 @@ def last_stats():
     ms, n, near = C.c_double(), C.c_int(), C.c_longlong()
     _check(lib().winds_bs_last_stats(C.byref(ms), C.byref(n), C.byref(near)))
     return ms.value, n.value, near.value
+
+
+def last_core_free():
+    """Pairs of the last evaluation that took the core-free form (Vatistas
+    FP32c: targets at least 64 core radii from the filament's line)."""
+    n = C.c_longlong()
+    _check(lib().winds_bs_last_core_free(C.byref(n)))
+    return n.value
 
 
 def set_autotune(on: bool):

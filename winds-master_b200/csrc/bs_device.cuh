@@ -215,7 +215,9 @@ __device__ __forceinline__ void filament_fields(double x1, double y1, double z1,
   v[4] = (float)(x1 - (double)hx), v[5] = (float)(y1 - (double)hy);
   v[6] = (float)(z1 - (double)hz), v[7] = (float)Rn2;
   v[8] = (float)Lx, v[9] = (float)Ly, v[10] = (float)Lz, v[11] = (float)D;
-  v[12] = (float)(K * Lx), v[13] = (float)(K * Ly), v[14] = (float)(K * Lz), v[15] = 0.f;
+  v[12] = (float)(K * Lx), v[13] = (float)(K * Ly), v[14] = (float)(K * Lz);
+  // the core radius, for the kernel's screen of pairs whose core factor is 1
+  v[15] = model == kCoreVatistas && K != 0.0 ? (float)sqrt(fmax(r, 0.0)) : 0.f;
 }
 
 // Fields of an inert filament (far away, zero length, zero circulation) for padding.

@@ -248,6 +248,13 @@ __device__ __forceinline__ void load_pair(const float4 *r, float2 ncx, float2 nc
   f.Mz = lo2(m1);
 }
 
+// Internal form code of interact2: the Vatistas pair term with its core
+// factor taken as 1 (pairs the warp screen places at least kCoreFreeRatio
+// core radii from the filament's line, where the factor
+// 1/sqrt(1 + (rc/h)^4) is within 3e-8 of 1, below FP32 resolution).
+constexpr int kCoreFree = 2;
+constexpr float kCoreFreeRatio = 64.f;
+
 // One target against one filament pair, accumulated into the packed sums
 // (ax, ay, az) (one lane per filament of the pair). (npx, npy, npz) = -(P - c)
 // broadcast to both lanes. With NEAR it also tests r1.r2 < Rn^2 per lane: such
@@ -287,6 +294,9 @@ __device__ __forceinline__ void interact2(float2 npx, float2 npy, float2 npz, co
     const float2 q = __ffma2_rn(c2, c2, f.D);
     const float2 w = __fmul2_rn(__fmul2_rn(__fadd2_rn(i1, i2), gg), c2);
     ub = __fmul2_rn(w, rsqrt2(__fmul2_rn(__fmul2_rn(e, e), q)));
+  } else if (MODEL == kCoreFree) {
+    // (r1+r2)/(r1r2(r1r2+r1.r2)) = (i1+i2) gg / e
+    ub = __fmul2_rn(__fmul2_rn(__fadd2_rn(i1, i2), gg), rcp2(e));
   } else {
     // (r1+r2)/(r1r2(r1r2+r1.r2) + d|L|^2) = (i1+i2) gg / (e + d|L|^2 gg^2)
     ub = __fmul2_rn(__fmul2_rn(__fadd2_rn(i1, i2), gg),
@@ -328,12 +338,15 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, uns
                                           unsigned &gt, float2 (&npx)[T], float2 (&npy)[T],
                                           float2 (&npz)[T], float2 ncx, float2 ncy, float2 ncz,
                                           float S2, const float *ws, unsigned &near_cnt,
+                                          unsigned long long &free_cnt,
                                           const Tile &tl) {
   constexpr int S = StageSmem<KF>::kStages;
   constexpr int kB = StageSmem<KF>::kBytes;
   const int lane = threadIdx.x & 31;
   const int ntiles = (it.f_end - it.f_begin) / KF;
   const float co2 = (float)(a.co * a.co);
+  const int nslots = tl.t_count - lane * T;  // this lane's targets in the tile
+  const unsigned live_slots = (unsigned)(nslots < 0 ? 0 : (nslots > T ? T : nslots));
   RefParams rp;
   rp.model = a.model;
   rp.d = a.d;
@@ -363,11 +376,13 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, uns
     // far from all of the warp's targets down the plain path; the others test
     // every pair and put their near-singular bits (bit 8*j + t: filament
     // 4*kk+j, target t) in shared memory as one word. `careful` has bit g for
-    // every such group g.
+    // every such group g. With the Vatistas core, a far group whose four
+    // lines all pass at least kCoreFreeRatio core radii from the warp's ball
+    // takes the core-free form (`mf` has a bit per such filament).
     unsigned careful = 0u;
 #pragma unroll 1
     for (int w = 0; w < KF / 32; ++w) {
-      unsigned m;
+      unsigned m, mf = 0u;
       if (CO) {
         m = 0xffffffffu;
       } else {
@@ -387,11 +402,35 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, uns
             1e-5f * (big + fabsf(Ax) + fabsf(Ay) + fabsf(Az)) + 1e-3f * (reach + wr);
         const float lim = wr + reach + slack;
         m = __ballot_sync(0xffffffffu, !(d2 > lim * lim));
+        if (MODEL == kCoreVatistas) {
+          // distance of the ball centre from the filament's line: |L x (x1 - c)| / |L|;
+          // every target of the warp is at least that less wr from it
+          const float Lx = f[16], Ly = f[18], Lz = f[20], rc = f[30];
+          const float dx = Ax - wcx, dy = Ay - wcy, dz = Az - wcz;
+          const float cx = Ly * dz - Lz * dy, cy = Lz * dx - Lx * dz, cz = Lx * dy - Ly * dx;
+          const float R = fmaf(kCoreFreeRatio, rc, wr + slack);
+          // zero length or zero K L: the pair term is zero on either form
+          const bool free_ = !(L2 > 0.f) || rc == 0.f || cx * cx + cy * cy + cz * cz >= R * R * L2;
+          mf = __ballot_sync(0xffffffffu, free_);
+        }
       }
 #pragma unroll 1
       for (int g = 0; g < 8; ++g) {
         const int kk = 32 * w + 4 * g;
-        if (((m >> (4 * g)) & 0xfu) == 0u) {
+        if (MODEL == kCoreVatistas && ((m >> (4 * g)) & 0xfu) == 0u &&
+            ((mf >> (4 * g)) & 0xfu) == 0xfu) {
+          free_cnt += 4u * live_slots;
+#pragma unroll
+          for (int j = 0; j < 2; ++j) {
+            Fil2 f;
+            load_pair(sP + (kk / 2 + j) * 8, ncx, ncy, ncz, f);
+            unsigned unused = 0;
+#pragma unroll
+            for (int t = 0; t < T; ++t)
+              interact2<kCoreFree, false, false>(npx[t], npy[t], npz[t], f, f.Rn2, co2, ax[t],
+                                                 ay[t], az[t], unused, 0u, 0u);
+          }
+        } else if (((m >> (4 * g)) & 0xfu) == 0u) {
 #pragma unroll
           for (int j = 0; j < 2; ++j) {
             Fil2 f;
@@ -550,6 +589,7 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<T>::value) bs_f32c(const F
   const bool co_on = co_can_trigger(a.bbox, a.co);
   unsigned gt = 0;
   unsigned near_cnt = 0;
+  unsigned long long free_cnt = 0;  // pairs of this lane that took the core-free form
   while (true) {
     int q = 0;
     if (lane == 0) q = (int)atomicAdd(a.work_ctr, 1u);
@@ -624,10 +664,10 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<T>::value) bs_f32c(const F
     bool ok;
     if (co_on)
       ok = f32c_item<T, KF, MODEL, true>(a, it, stages, full, s_k, s_nb, gt, npx, npy, npz, ncx,
-                                         ncy, ncz, S2, ws, near_cnt, tl);
+                                         ncy, ncz, S2, ws, near_cnt, free_cnt, tl);
     else
       ok = f32c_item<T, KF, MODEL, false>(a, it, stages, full, s_k, s_nb, gt, npx, npy, npz, ncx,
-                                          ncy, ncz, S2, ws, near_cnt, tl);
+                                          ncy, ncz, S2, ws, near_cnt, free_cnt, tl);
     if (!ok) break;
     double *part = a.part + (size_t)item_id * 3 * a.tile_cap;
 #pragma unroll
@@ -643,6 +683,7 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<T>::value) bs_f32c(const F
     __syncwarp();
   }
   if (a.near_ctr && near_cnt) atomicAdd(a.near_ctr, (unsigned long long)near_cnt);
+  if (a.near_ctr && free_cnt) atomicAdd(a.near_ctr + 1, free_cnt);
 }
 
 // ------------------------------------------------------- FP64 direct sum

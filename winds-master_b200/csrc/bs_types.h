@@ -7,7 +7,8 @@
 //     fields  0-3   x1_hi.x, x1_hi.y, x1_hi.z, |L|^2
 //             4-7   x1_lo.x, x1_lo.y, x1_lo.z, Rn^2   (x1 = hi + lo to ~2^-48)
 //             8-11  L.x, L.y, L.z, D                  (L = x2 - x1)
-//            12-15  K L.x, K L.y, K L.z, 0            (K = gamma/4pi)
+//            12-15  K L.x, K L.y, K L.z, rc           (K = gamma/4pi; rc the core
+//                                                       radius, Vatistas with K != 0, else 0)
 //   with D = (K^2 rc^2 |L|^2)^2 (Vatistas: the core term scaled like |K L x r1|^4,
 //   so K cancels from the core factor and enters only through K L) or d |L|^2
 //   (cut-off)

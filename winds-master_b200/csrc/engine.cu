@@ -144,13 +144,13 @@ Context *get_context(int *rc) {
   if ((*rc = c->bbox.ensure(sizeof(BBox), c->stream)) ||
       (*rc = c->ctr.ensure(64 * sizeof(unsigned), c->stream)) ||
       (*rc = c->err.ensure(sizeof(unsigned), c->stream)) ||
-      (*rc = c->nearctr.ensure(sizeof(unsigned long long), c->stream)) ||
+      (*rc = c->nearctr.ensure(2 * sizeof(unsigned long long), c->stream)) ||
       (*rc = c->hstat.ensure(64))) {
     delete c;
     return nullptr;
   }
   cudaMemsetAsync(c->err.p, 0, sizeof(unsigned), c->stream);
-  cudaMemsetAsync(c->nearctr.p, 0, sizeof(unsigned long long), c->stream);
+  cudaMemsetAsync(c->nearctr.p, 0, 2 * sizeof(unsigned long long), c->stream);
   g_ctx[dev] = c;
   *rc = WINDS_BS_OK;
   return c;
@@ -475,7 +475,7 @@ int run_direct_sum(Context *c, const std::vector<GroupSpec> &gs, int model, doub
   a.wait_limit_ns = default_wait_limit_ns();
   cudaError_t e = cudaMemsetAsync(c->ctr.p, 0, sizeof(unsigned), s);
   // near-singular pairs are counted per evaluation
-  if (e == cudaSuccess) e = cudaMemsetAsync(c->nearctr.p, 0, sizeof(unsigned long long), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->nearctr.p, 0, 2 * sizeof(unsigned long long), s);
   if (e != cudaSuccess) return cuda_fail(e, "work counter reset");
   const int grid = (int)std::max<long long>(1, std::min<long long>(a.n_items, resident));
   if (time_main) cudaEventRecord(c->ev_main0, s);
@@ -806,6 +806,21 @@ int winds_bs_last_stats(double *main_ms, int *launches, long long *near_pairs) {
     cudaMemset(c->nearctr.p, 0, sizeof(v));
     *near_pairs = (long long)v;
   }
+  return WINDS_BS_OK;
+}
+
+int winds_bs_last_core_free(long long *pairs) {
+  int rc;
+  Context *c = get_context(&rc);
+  if (!c) return rc;
+  if (!pairs) return WINDS_BS_ERR_ARG;
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "stats sync");
+  unsigned long long v = 0;
+  e = cudaMemcpy(&v, (const unsigned long long *)c->nearctr.p + 1, sizeof(v),
+                 cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "stats read");
+  *pairs = (long long)v;
   return WINDS_BS_OK;
 }
 

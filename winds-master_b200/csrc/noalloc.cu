@@ -186,7 +186,7 @@ extern "C" int winds_bs_eval_device_noalloc(const winds_bs_family *fams, int nfa
   BBox *bbox = cv.take<BBox>(1);
   unsigned *ctr = cv.take<unsigned>(4);
   unsigned *err = cv.take<unsigned>(4);
-  unsigned long long *nearc = cv.take<unsigned long long>(1);
+  unsigned long long *nearc = cv.take<unsigned long long>(2);  // near, core-free pairs
   PackedFilaments pf{cv.take<float4>(nfp * 4), cv.take<double4>(nfp), cv.take<double4>(nfp)};
   double4 *tp = cv.take<double4>(nt);
   double4 *tp_raw = cv.take<double4>(nt);
@@ -207,7 +207,7 @@ extern "C" int winds_bs_eval_device_noalloc(const winds_bs_family *fams, int nfa
   // ---- state carried over from the previous call: clear what starts at zero
   if ((e = cudaMemsetAsync(ctr, 0, 4 * sizeof(unsigned), s)) != cudaSuccess ||
       (e = cudaMemsetAsync(err, 0, 4 * sizeof(unsigned), s)) != cudaSuccess ||
-      (e = cudaMemsetAsync(nearc, 0, sizeof(unsigned long long), s)) != cudaSuccess)
+      (e = cudaMemsetAsync(nearc, 0, 2 * sizeof(unsigned long long), s)) != cudaSuccess)
     return cuda_fail(e, "scratch reset");
 
   // ---- pack (the same kernels as winds_bs_eval_device)
