@@ -139,9 +139,10 @@ int winds_bs_last_stats(double *main_ms, int *launches, long long *near_pairs);
 
 /* How many pairs of the last winds_bs_eval_host / winds_bs_eval_device call's
  * FP32c Vatistas direct sum took the core-free form: pairs whose target lies
- * at least 64 core radii from the filament's line (the screen of 32 filaments
- * against a warp's 128 targets decides), where the core factor
- * 1/sqrt(1 + (rc/h)^4) is within 3e-8 of 1 and the kernel leaves it out.
+ * at least 54 core radii from the filament's line (the screen of 32 filaments
+ * against a warp's targets decides), where the core factor
+ * 1/sqrt(1 + (rc/h)^4) is within 5.9e-8 (below 2^-24) of 1 and the kernel
+ * leaves it out.
  * 0 for the cut-off core and the FP64 path. */
 int winds_bs_last_core_free(long long *pairs);
 

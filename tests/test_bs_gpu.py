@@ -255,7 +255,7 @@ def test_fp32_peak_probe(wb):
 
 
 def test_core_free_form(wb, oracle):
-    """Targets far from every filament line (more than 64 core radii, the
+    """Targets far from every filament line (more than 54 core radii, the
     warp's ball included) take the core-free form for every pair, and match
     the FP64 oracle; targets inside the cores take none of it. The counter
     reports exactly the pairs that took the form."""

@@ -180,7 +180,7 @@ def last_stats():
 
 def last_core_free():
     """Pairs of the last evaluation that took the core-free form (Vatistas
-    FP32c: targets at least 64 core radii from the filament's line)."""
+    FP32c: targets at least 54 core radii from the filament's line)."""
     n = C.c_longlong()
     _check(lib().winds_bs_last_core_free(C.byref(n)))
     return n.value

@@ -251,9 +251,10 @@ __device__ __forceinline__ void load_pair(const float4 *r, float2 ncx, float2 nc
 // Internal form code of interact2: the Vatistas pair term with its core
 // factor taken as 1 (pairs the warp screen places at least kCoreFreeRatio
 // core radii from the filament's line, where the factor
-// 1/sqrt(1 + (rc/h)^4) is within 3e-8 of 1, below FP32 resolution).
+// 1/sqrt(1 + (rc/h)^4) is within (1/54)^4 / 2 = 5.9e-8 of 1, below FP32's
+// unit roundoff 2^-24).
 constexpr int kCoreFree = 2;
-constexpr float kCoreFreeRatio = 64.f;
+constexpr float kCoreFreeRatio = 54.f;
 
 // One target against one filament pair, accumulated into the packed sums
 // (ax, ay, az) (one lane per filament of the pair). (npx, npy, npz) = -(P - c)
@@ -413,6 +414,21 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, uns
           const bool free_ = !(L2 > 0.f) || rc == 0.f || cx * cx + cy * cy + cz * cz >= R * R * L2;
           mf = __ballot_sync(0xffffffffu, free_);
         }
+      }
+      if (MODEL == kCoreVatistas && m == 0u && mf == 0xffffffffu) {
+        // the whole word far and core-free: one loop over its 16 pairs
+        free_cnt += 32u * live_slots;
+#pragma unroll 2
+        for (int j = 0; j < 16; ++j) {
+          Fil2 f;
+          load_pair(sP + (16 * w + j) * 8, ncx, ncy, ncz, f);
+          unsigned unused = 0;
+#pragma unroll
+          for (int t = 0; t < T; ++t)
+            interact2<kCoreFree, false, false>(npx[t], npy[t], npz[t], f, f.Rn2, co2, ax[t],
+                                               ay[t], az[t], unused, 0u, 0u);
+        }
+        continue;
       }
 #pragma unroll 1
       for (int g = 0; g < 8; ++g) {
