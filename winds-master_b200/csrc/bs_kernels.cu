@@ -649,14 +649,28 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<T>::value) bs_f32c(const F
     }
     const float2 ncx = make_float2(-cx, -cx), ncy = make_float2(-cy, -cy),
                  ncz = make_float2(-cz, -cz);
-    // The warp's targets lie in the ball (wc, wr) around lane 0's centre. As
-    // r1.r2 = |P - m|^2 - |L|^2/4 (m the filament midpoint), a filament whose
-    // midpoint is farther than wr + sqrt(|L|^2/4 + Rn^2) from wc has
-    // r1.r2 >= Rn^2 for every target of the warp; rn_floor is the warp's
-    // largest per-thread threshold S2.
-    const float wcx = __shfl_sync(0xffffffffu, cx, 0);
-    const float wcy = __shfl_sync(0xffffffffu, cy, 0);
-    const float wcz = __shfl_sync(0xffffffffu, cz, 0);
+    // The warp's targets lie in the ball (wc, wr) around the centre of their
+    // bounding box. As r1.r2 = |P - m|^2 - |L|^2/4 (m the filament midpoint),
+    // a filament whose midpoint is farther than wr + sqrt(|L|^2/4 + Rn^2)
+    // from wc has r1.r2 >= Rn^2 for every target of the warp; rn_floor is
+    // the warp's largest per-thread threshold S2.
+    float blo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, bhi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+#pragma unroll
+    for (int t = 0; t < T; ++t) {
+      const float q[3] = {cx + px[t], cy + py[t], cz + pz[t]};
+#pragma unroll
+      for (int c = 0; c < 3; ++c) blo[c] = fminf(blo[c], q[c]), bhi[c] = fmaxf(bhi[c], q[c]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        blo[c] = fminf(blo[c], __shfl_xor_sync(0xffffffffu, blo[c], o));
+        bhi[c] = fmaxf(bhi[c], __shfl_xor_sync(0xffffffffu, bhi[c], o));
+      }
+    const float wcx = 0.5f * (blo[0] + bhi[0]);
+    const float wcy = 0.5f * (blo[1] + bhi[1]);
+    const float wcz = 0.5f * (blo[2] + bhi[2]);
     float wr2 = 0.f;
 #pragma unroll
     for (int t = 0; t < T; ++t) {
