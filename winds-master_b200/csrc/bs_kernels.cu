@@ -410,8 +410,10 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, uns
           const float dx = Ax - wcx, dy = Ay - wcy, dz = Az - wcz;
           const float cx = Ly * dz - Lz * dy, cy = Lz * dx - Lx * dz, cz = Lx * dy - Ly * dx;
           const float R = fmaf(kCoreFreeRatio, rc, wr + slack);
-          // zero length or zero K L: the pair term is zero on either form
-          const bool free_ = !(L2 > 0.f) || rc == 0.f || cx * cx + cy * cy + cz * cz >= R * R * L2;
+          // zero length: the pair term is zero on either form; rc = 0 (no core,
+          // or K = 0 and a zero term): the factor is 1
+          const bool free_ =
+              !(L2 > 0.f) || rc == 0.f || cx * cx + cy * cy + cz * cz >= R * R * L2;
           mf = __ballot_sync(0xffffffffu, free_);
         }
       }
