@@ -695,6 +695,39 @@ def ours(args):
         b = np.stack([b64[:, c].ravel(order="F") for c in range(3)], 1)
         rel_err = float(np.max(np.linalg.norm(a - b, axis=1) / np.linalg.norm(b, axis=1)))
 
+    # the same workload with the reference's default core (cut-off, d = 1e-4)
+    cutoff_line = None
+    if not args.quick:
+        core_c = wb.bs.CORE_CUTOFF
+        outc = torch.zeros_like(out)
+        for _ in range(3):  # the first call tunes this core's bucket
+            wb.eval_device(dfams, dP, core_c, 1e-4, 1000.0, outc, "f32c", stream=sp)
+        tc = []
+        for _ in range(5):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            wb.eval_device(dfams, dP, core_c, 1e-4, 1000.0, outc, "f32c", stream=sp)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            tc.append(e0.elapsed_time(e1))
+        free_c = wb.last_core_free()
+        out64c = torch.zeros_like(out)
+        wb.eval_device(dfams, dP, core_c, 1e-4, 1000.0, out64c, "f64", stream=sp)
+        torch.cuda.synchronize()
+        a = outc.cpu().numpy().reshape(P.shape, order="F")
+        b = out64c.cpu().numpy().reshape(P.shape, order="F")
+        a = np.stack([a[:, c].ravel(order="F") for c in range(3)], 1)
+        b = np.stack([b[:, c].ravel(order="F") for c in range(3)], 1)
+        cutoff_line = {"core": "cut-off, d = 1e-4", "timed_steps": 5,
+                       "gint_per_s": interactions / (statistics.median(tc) * 1e-3) / 1e9,
+                       "core_free_fraction": free_c / interactions,
+                       "rel_err_max_vs_fp64": float(np.max(np.linalg.norm(a - b, axis=1) /
+                                                           np.linalg.norm(b, axis=1))),
+                       "tiling": dict(zip(("targets_per_thread", "filaments_per_tile", "waves"),
+                                          wb.get_tuning(core_c, nt, nf)))}
+
     # end to end through the public host API: pinned host inputs, H2D + eval + D2H per step
     e2e_line = None
     if not args.quick:
@@ -774,6 +807,7 @@ def ours(args):
             "core_free_fraction": free_pairs / interactions,
             "tiling": dict(zip(("targets_per_thread", "filaments_per_tile", "waves"),
                                wb.get_tuning(core, nt, nf))),
+            "cutoff_core": cutoff_line,
             "wake_batch": wake_line,
             "wake_batch_sharded": sharded_line,
             "kj_start_value": mlp_line,

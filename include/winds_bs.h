@@ -138,12 +138,12 @@ int winds_bs_length_device(const double *F1, const double *F2, const long long d
 int winds_bs_last_stats(double *main_ms, int *launches, long long *near_pairs);
 
 /* How many pairs of the last winds_bs_eval_host / winds_bs_eval_device call's
- * FP32c Vatistas direct sum took the core-free form: pairs whose target lies
- * at least 54 core radii from the filament's line (the screen of 32 filaments
- * against a warp's targets decides), where the core factor
- * 1/sqrt(1 + (rc/h)^4) is within 5.9e-8 (below 2^-24) of 1 and the kernel
- * leaves it out.
- * 0 for the cut-off core and the FP64 path. */
+ * FP32c direct sum took the core-free form, where leaving the core out
+ * changes the pair term by less than FP32's unit roundoff 2^-24 (one-sided):
+ * Vatistas, targets at least 54 core radii from the filament's line (the
+ * factor 1/sqrt(1 + (rc/h)^4) is within 5.9e-8 of 1); cut-off, targets at
+ * least r from the segment with r^4 >= 2^24 d |L|^2. A screen of 32
+ * filaments against a warp's targets decides. 0 for the FP64 path. */
 int winds_bs_last_core_free(long long *pairs);
 
 /* Synchronises `stream` (NULL: the library's stream) and reports a device-side

@@ -257,8 +257,9 @@ def test_fp32_peak_probe(wb):
 def test_core_free_form(wb, oracle):
     """Targets far from every filament line (more than 54 core radii, the
     warp's ball included) take the core-free form for every pair, and match
-    the FP64 oracle; targets inside the cores take none of it. The counter
-    reports exactly the pairs that took the form."""
+    the FP64 oracle; targets inside the cores take it only for the far side
+    of the ring. The same with the cut-off core. The counter reports exactly
+    the pairs that took the form."""
     rng = np.random.default_rng(21)
     nf = 256
     a = np.linspace(0.0, 2 * np.pi, nf + 1)
@@ -283,6 +284,13 @@ def test_core_free_form(wb, oracle):
     uo = oracle.c_eval(F1, F2, Pn, g, rc, "visc2", 1000.0)
     assert per_target_rel(u, uo) < F32C_TOL
     assert wb.last_core_free() < nf * nf
-    # the cut-off core has no such form
-    wb.eval_host(fams, Pf, wb.bs.CORE_CUTOFF, 1e-4, 1000.0, "f32c")
-    assert wb.last_core_free() == 0
+    # cut-off: 300 m from 0.25 m segments with d = 1e-4, d |L|^2 is far below
+    # FP32 resolution against r^4
+    u = wb.eval_host(fams, Pf, wb.bs.CORE_CUTOFF, 1e-4, 1000.0, "f32c")
+    assert wb.last_core_free() == nf * 512
+    uo = oracle.c_eval(F1, F2, Pf, g, rc, 1e-4, 1000.0)
+    assert per_target_rel(u, uo) < F32C_TOL
+    u = wb.eval_host(fams, Pn, wb.bs.CORE_CUTOFF, 1e-4, 1000.0, "f32c")
+    assert wb.last_core_free() < nf * nf
+    uo = oracle.c_eval(F1, F2, Pn, g, rc, 1e-4, 1000.0)
+    assert per_target_rel(u, uo) < F32C_TOL

@@ -179,8 +179,9 @@ def last_stats():
 
 
 def last_core_free():
-    """Pairs of the last evaluation that took the core-free form (Vatistas
-    FP32c: targets at least 54 core radii from the filament's line)."""
+    """Pairs of the last FP32c evaluation that took the core-free form
+    (Vatistas: targets at least 54 core radii from the filament's line;
+    cut-off: targets far enough that d |L|^2 is below FP32 resolution)."""
     n = C.c_longlong()
     _check(lib().winds_bs_last_core_free(C.byref(n)))
     return n.value

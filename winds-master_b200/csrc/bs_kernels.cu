@@ -248,13 +248,17 @@ __device__ __forceinline__ void load_pair(const float4 *r, float2 ncx, float2 nc
   f.Mz = lo2(m1);
 }
 
-// Internal form code of interact2: the Vatistas pair term with its core
-// factor taken as 1 (pairs the warp screen places at least kCoreFreeRatio
-// core radii from the filament's line, where the factor
-// 1/sqrt(1 + (rc/h)^4) is within (1/54)^4 / 2 = 5.9e-8 of 1, below FP32's
-// unit roundoff 2^-24).
+// Internal form code of interact2: the pair term with its core left out,
+// (i1 + i2) i1 i2 / e, for pairs where the core changes it by less than
+// FP32's unit roundoff 2^-24. Vatistas: the warp screen places the targets
+// at least kCoreFreeRatio core radii from the filament's line, where the
+// factor 1/sqrt(1 + (rc/h)^4) is within (1/54)^4 / 2 = 5.9e-8 of 1.
+// Cut-off: the targets are at least r from the segment with
+// r^4 >= 2^24 d |L|^2, so the denominator's d |L|^2 gg^2 <= 2^-24 <= 2^-24 e
+// (e >= 1 on the far path, where r1.r2 > 0).
 constexpr int kCoreFree = 2;
 constexpr float kCoreFreeRatio = 54.f;
+constexpr float kCutoffFreeSq = 4096.f;  // r^2 >= 4096 sqrt(d |L|^2) is r^4 >= 2^24 d |L|^2
 
 // One target against one filament pair, accumulated into the packed sums
 // (ax, ay, az) (one lane per filament of the pair). (npx, npy, npz) = -(P - c)
@@ -377,9 +381,11 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, uns
     // far from all of the warp's targets down the plain path; the others test
     // every pair and put their near-singular bits (bit 8*j + t: filament
     // 4*kk+j, target t) in shared memory as one word. `careful` has bit g for
-    // every such group g. With the Vatistas core, a far group whose four
-    // lines all pass at least kCoreFreeRatio core radii from the warp's ball
-    // takes the core-free form (`mf` has a bit per such filament).
+    // every such group g. A far group whose four filaments all leave every
+    // target of the warp outside their core's reach (Vatistas: lines at least
+    // kCoreFreeRatio core radii away; cut-off: segments far enough that the
+    // d |L|^2 term is below FP32 resolution) takes the core-free form (`mf`
+    // has a bit per such filament).
     unsigned careful = 0u;
 #pragma unroll 1
     for (int w = 0; w < KF / 32; ++w) {
@@ -415,9 +421,15 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, uns
           const bool free_ =
               !(L2 > 0.f) || rc == 0.f || cx * cx + cy * cy + cz * cz >= R * R * L2;
           mf = __ballot_sync(0xffffffffu, free_);
+        } else {
+          // nearest approach of a warp target to the segment: its midpoint
+          // distance less wr and |L|/2; D = d |L|^2 (record field 11)
+          const float rmin = sqrtf(d2) - wr - 0.5f * sqrtf(L2) - slack;
+          const bool free_ = rmin > 0.f && rmin * rmin >= kCutoffFreeSq * sqrtf(f[22]);
+          mf = __ballot_sync(0xffffffffu, free_);
         }
       }
-      if (MODEL == kCoreVatistas && m == 0u && mf == 0xffffffffu) {
+      if (m == 0u && mf == 0xffffffffu) {
         // the whole word far and core-free: one loop over its 16 pairs
         free_cnt += 32u * live_slots;
 #pragma unroll 2
@@ -435,8 +447,7 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, uns
 #pragma unroll 1
       for (int g = 0; g < 8; ++g) {
         const int kk = 32 * w + 4 * g;
-        if (MODEL == kCoreVatistas && ((m >> (4 * g)) & 0xfu) == 0u &&
-            ((mf >> (4 * g)) & 0xfu) == 0xfu) {
+        if (((m >> (4 * g)) & 0xfu) == 0u && ((mf >> (4 * g)) & 0xfu) == 0xfu) {
           free_cnt += 4u * live_slots;
 #pragma unroll
           for (int j = 0; j < 2; ++j) {
