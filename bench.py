@@ -13,7 +13,10 @@ per second), whole job over all ranks.
   formula (the C restatement of core/BiotSavart.m, all host threads) on a
   bounded sample of the same workload.
 For N > 1 (torchrun) each rank evaluates its own wake (seed + rank): weak
-scaling, no data-path collective; the time is the max over ranks.
+scaling, no data-path collective; the time is the max over ranks. Beside that
+line, at N > 1: the 64-case batch split by case (``wake_batch_sharded``) and
+one wake's evaluation split by target with an NCCL all-gather of the
+velocities (``target_sharded``, strong scaling).
 """
 from __future__ import annotations
 
@@ -338,6 +341,67 @@ def sharded_wake_bench(args, rank, world, seed=2, ncases=64):
             "steps_per_s": 1000.0 * args.wake_steps / float(t.item()),
             "cases_per_rank": [len(p) for p in parts], "imbalance": sh.imbalance(costs, parts),
             "timing": "CUDA events around each rank's steps, max over ranks"}
+
+
+def target_sharded_bench(args, rank, world, stream, flush):
+    """The headline evaluation of ONE wake (seed 1 on every rank) split over
+    the ranks by target (sharding.TargetShardedEval): each rank evaluates its
+    run of targets against all filaments, and one NCCL all-gather of the
+    velocities (24 bytes per target) gives every rank the whole field. Strong
+    scaling: one evaluation per step whatever the number of ranks. CUDA events
+    around each step on the stream the ranks launch on, max over ranks; rank
+    0 checks the gathered field against its own evaluation of all targets."""
+    import torch
+    import torch.distributed as dist
+    wb = importlib.import_module("winds-master_b200")
+    sh = importlib.import_module("winds-master_b200.sharding")
+    _, fams, P, nf, nt = workload(1, args.workload)
+
+    def dev(a):
+        return torch.from_numpy(np.asarray(a).ravel(order="F").copy()).cuda()
+
+    dfams = [(dev(F1), dev(F2), dev(g), dev(rc), F1.shape) for F1, F2, g, rc in fams]
+    dP = dev(P)
+    sp = stream.cuda_stream
+    core = wb.bs.CORE_VATISTAS
+    ev = sh.device_evaluator(dfams, core, 2.0, 1000.0, "f32c", stream=sp)
+    te = sh.TargetShardedEval(P.shape, rank=rank, world=world)
+    out = torch.zeros(P.size, dtype=torch.float64, device="cuda")
+    for _ in range(3):  # warm-up (the first call tunes the run's size bucket)
+        te(dP, out, ev)
+    torch.cuda.synchronize()
+    dist.barrier()
+    ms = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        te(dP, out, ev)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
+    t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    err = None
+    if rank == 0:
+        full = torch.zeros_like(out)
+        wb.eval_device(dfams, (dP, P.shape), core, 2.0, 1000.0, full, "f32c", stream=sp)
+        wb.sync(sp)
+        a = out.cpu().numpy().reshape(P.shape, order="F")
+        b = full.cpu().numpy().reshape(P.shape, order="F")
+        a = np.stack([a[:, c].ravel(order="F") for c in range(3)], 1)
+        b = np.stack([b[:, c].ravel(order="F") for c in range(3)], 1)
+        err = float(np.max(np.linalg.norm(a - b, axis=1) / np.linalg.norm(b, axis=1)))
+    return {"parallelism": "target-sharded", "ranks": world, "scaling": "strong",
+            "targets": nt, "filaments": nf, "timed_steps": args.steps,
+            "targets_per_rank": [t1 - t0 for t0, t1 in te.slices],
+            "gint_per_s": nf * nt * args.steps / (ms * 1e-3) / 1e9,
+            "ms_per_step": ms / args.steps,
+            "exchange_bytes_per_rank": 3 * 8 * te.n_max * world,
+            "rel_diff_max_vs_one_rank": err,
+            "timing": "CUDA events around each step (own run + all-gather), max over ranks"}
 
 
 def batch_start_value(seed=12, n_train=48, n_val=8, steps=10, relax=0.3, tol=1e-6, maxiter=200):
@@ -775,9 +839,11 @@ def ours(args):
         wake_line = wake_bench(args, mlp=net)
         if net is not None:
             net.close()
-    sharded_line = None
+    sharded_line = target_line = None
     if world > 1 and args.wake_steps > 0 and not args.quick:
         sharded_line = sharded_wake_bench(args, rank, world)
+    if world > 1 and not args.quick:
+        target_line = target_sharded_bench(args, rank, world, stream, flush)
     mlp_line = e2e_line_run = None
     if rank == 0 and world == 1 and not (args.quick or args.no_studies):
         mlp_line = kj_mlp_bench()
@@ -810,6 +876,7 @@ def ours(args):
             "cutoff_core": cutoff_line,
             "wake_batch": wake_line,
             "wake_batch_sharded": sharded_line,
+            "target_sharded": target_line,
             "kj_start_value": mlp_line,
             "e2e_run": e2e_line_run,
         }
