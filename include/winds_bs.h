@@ -146,6 +146,17 @@ int winds_bs_last_stats(double *main_ms, int *launches, long long *near_pairs);
  * filaments against a warp's targets decides. 0 for the FP64 path. */
 int winds_bs_last_core_free(long long *pairs);
 
+/* 1 when the last winds_bs_eval_host / winds_bs_eval_device call's FP32c
+ * direct sum ran on the chained filament stream, else 0. The chained stream
+ * lays each line of connected filaments (the shed call's along the span, the
+ * trailing call's along the wake age: BiotSavart calls of WInDS.m:150,153)
+ * along one lane of consecutive pair records, so that each interaction takes
+ * its second endpoint's inverse distance from the previous filament's first
+ * one (one rsqrt fewer); the autotuner picks it or the input order per size
+ * bucket together with the tiling (no reference counterpart: the reference's
+ * kernel evaluates every filament on its own, BiotSavartMex.cu:131-193). */
+int winds_bs_last_chained(int *chained);
+
 /* Synchronises `stream` (NULL: the library's stream) and reports a device-side
  * error (WINDS_BS_ERR_TIMEOUT for a bounded wait that ran out) recorded by an
  * earlier asynchronous call; the error word is cleared. */
@@ -162,6 +173,10 @@ int winds_bs_set_tuning(int core_model, long long n_targets, long long n_filamen
                         double waves);
 int winds_bs_get_tuning(int core_model, long long n_targets, long long n_filaments, int *T,
                         int *KF, double *waves);
+/* Sets the FP32c evaluations' stream layout of a bucket (1: chained, 0: input
+ * order; see winds_bs_last_chained), keeping its tiling (the untuned default
+ * when the bucket has none); set_tuning resets the bucket to input order. */
+int winds_bs_set_layout(int core_model, long long n_targets, long long n_filaments, int chained);
 
 /* Measured FP32 FMA throughput of this GPU in TFLOP/s (a ~0.1 s probe of
  * independent FFMA chains): the roofline denominator of the direct sum. */

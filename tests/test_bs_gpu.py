@@ -100,19 +100,27 @@ def test_large_case_subset_vs_oracle(wb, synth, oracle, large):
 
 def test_large_case_full_f32c_vs_f64(wb, large):
     """All 88,803 targets: FP32-compensated against the FP64 GPU path (itself
-    pinned to the oracle above), plus exact linearity in the circulation."""
+    pinned to the oracle above), plus exact linearity in the circulation, on
+    the input-order and the chained filament stream."""
     w, fams, _ = large
     P = w["dom"]
+    nt = P.shape[0] * P.shape[2] * P.shape[3]
+    nf = sum(f[0].shape[0] * f[0].shape[2] * f[0].shape[3] for f in fams)
     u64 = wb.eval_host(fams, P, wb.bs.CORE_VATISTAS, 2.0, 1000.0, "f64")
-    u32 = wb.eval_host(fams, P, wb.bs.CORE_VATISTAS, 2.0, 1000.0, "f32c")
-    assert per_target_rel(u32, u64) < F32C_TOL
     fams2 = [(F1, F2, 2.0 * g, rc) for F1, F2, g, rc in fams]
-    u32x2 = wb.eval_host(fams2, P, wb.bs.CORE_VATISTAS, 2.0, 1000.0, "f32c")
-    np.testing.assert_array_equal(u32x2, 2.0 * u32)
+    for chained in (False, True):
+        wb.set_tuning(wb.bs.CORE_VATISTAS, nt, nf, 4, 64, 32.0)
+        wb.set_layout(wb.bs.CORE_VATISTAS, nt, nf, chained)
+        u32 = wb.eval_host(fams, P, wb.bs.CORE_VATISTAS, 2.0, 1000.0, "f32c")
+        assert wb.last_chained() == chained
+        assert per_target_rel(u32, u64) < F32C_TOL, chained
+        u32x2 = wb.eval_host(fams2, P, wb.bs.CORE_VATISTAS, 2.0, 1000.0, "f32c")
+        np.testing.assert_array_equal(u32x2, 2.0 * u32)
 
 
 def test_every_tiling_agrees(wb, synth, oracle):
-    """Each compiled (T, KF) tiling of the FP32 kernel gives the oracle's answer."""
+    """Each compiled (T, KF) tiling of the FP32 kernel gives the oracle's
+    answer, on the input-order and the chained filament stream."""
     w = synth.make_wake(synth.RotorCase(nst=21, nsteps=90, dpsi_deg=4.0, seed=5))
     fams = [synth.shed_filaments(w["dom"]) + (w["gamma_shed"], w["rc_shed"]),
             synth.trail_filaments(w["dom"]) + (w["gamma_trail"], w["rc_trail"])]
@@ -120,23 +128,27 @@ def test_every_tiling_agrees(wb, synth, oracle):
     nt = P.shape[0] * P.shape[2] * P.shape[3]
     nf = sum(f[0].shape[0] * f[0].shape[2] * f[0].shape[3] for f in fams)
     uo = sum(oracle.c_eval(F1, F2, P, g, rc, "visc2", 1000.0) for F1, F2, g, rc in fams)
+    uc = sum(oracle.c_eval(F1, F2, P, g, rc, 1e-4, 1000.0) for F1, F2, g, rc in fams)
     for T in (2, 3, 4, 8):
         for KF in (32, 64, 128):
             for waves in (1.0, 16.0):
-                wb.set_tuning(wb.bs.CORE_VATISTAS, nt, nf, T, KF, waves)
-                u = wb.eval_host(fams, P, wb.bs.CORE_VATISTAS, 2.0, 1000.0, "f32c")
-                assert per_target_rel(u, uo) < F32C_TOL, (T, KF, waves)
-                wb.set_tuning(wb.bs.CORE_CUTOFF, nt, nf, T, KF, waves)
-                u = wb.eval_host(fams, P, wb.bs.CORE_CUTOFF, 1e-4, 1000.0, "f32c")
-                uc = sum(oracle.c_eval(F1, F2, P, g, rc, 1e-4, 1000.0) for F1, F2, g, rc in fams)
-                assert per_target_rel(u, uc) < F32C_TOL, (T, KF, waves)
+                for chained in (False, True):
+                    wb.set_tuning(wb.bs.CORE_VATISTAS, nt, nf, T, KF, waves)
+                    wb.set_layout(wb.bs.CORE_VATISTAS, nt, nf, chained)
+                    u = wb.eval_host(fams, P, wb.bs.CORE_VATISTAS, 2.0, 1000.0, "f32c")
+                    assert wb.last_chained() == chained
+                    assert per_target_rel(u, uo) < F32C_TOL, (T, KF, waves, chained)
+                    wb.set_tuning(wb.bs.CORE_CUTOFF, nt, nf, T, KF, waves)
+                    wb.set_layout(wb.bs.CORE_CUTOFF, nt, nf, chained)
+                    u = wb.eval_host(fams, P, wb.bs.CORE_CUTOFF, 1e-4, 1000.0, "f32c")
+                    assert per_target_rel(u, uc) < F32C_TOL, (T, KF, waves, chained)
 
 
 def test_tiles_full_of_near_pairs(wb, oracle):
     """A compact ring of 64 short filaments with a 1 m core inside a cloud of
     1024 targets: every pair is near-singular, so each tile lists far more
     FP64 pairs than one pass of its list holds. All of them are counted and
-    the sums match the FP64 oracle for every tiling."""
+    the sums match the FP64 oracle for every tiling and both stream layouts."""
     rng = np.random.default_rng(11)
     nf, nt = 64, 1024
     a = np.linspace(0.0, 2 * np.pi, nf + 1)
@@ -150,10 +162,12 @@ def test_tiles_full_of_near_pairs(wb, oracle):
     uo = oracle.c_eval(F1, F2, P, g, rc, "visc2", 1000.0)
     for T in (2, 4, 8):
         for KF in (32, 64):
-            wb.set_tuning(wb.bs.CORE_VATISTAS, nt, nf, T, KF, 4.0)
-            u = wb.eval_host(fams, P, wb.bs.CORE_VATISTAS, 2.0, 1000.0, "f32c")
-            assert wb.last_stats()[2] == nf * nt, (T, KF)
-            assert per_target_rel(u, uo) < 1e-6, (T, KF)
+            for chained in (False, True):
+                wb.set_tuning(wb.bs.CORE_VATISTAS, nt, nf, T, KF, 4.0)
+                wb.set_layout(wb.bs.CORE_VATISTAS, nt, nf, chained)
+                u = wb.eval_host(fams, P, wb.bs.CORE_VATISTAS, 2.0, 1000.0, "f32c")
+                assert wb.last_stats()[2] == nf * nt, (T, KF, chained)
+                assert per_target_rel(u, uo) < 1e-6, (T, KF, chained)
 
 
 def test_edge_cases_gpu(wb):

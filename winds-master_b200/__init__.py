@@ -27,8 +27,10 @@ from .bs import (  # noqa: F401
     eval_host,
     last_stats,
     last_core_free,
+    last_chained,
     lib,
     set_tuning,
+    set_layout,
     get_tuning,
     set_autotune,
     sync,

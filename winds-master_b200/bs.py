@@ -70,6 +70,7 @@ def lib():
         L.winds_bs_last_stats.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_int),
                                           C.POINTER(C.c_longlong)]
         L.winds_bs_last_core_free.argtypes = [C.POINTER(C.c_longlong)]
+        L.winds_bs_last_chained.argtypes = [C.POINTER(C.c_int)]
         L.winds_bs_sync.argtypes = [C.c_void_p]
         L.winds_bs_set_tuning.argtypes = [C.c_int, C.c_longlong, C.c_longlong, C.c_int, C.c_int,
                                           C.c_double]
@@ -187,12 +188,27 @@ def last_core_free():
     return n.value
 
 
+def last_chained():
+    """True when the last FP32c evaluation ran on the chained filament stream
+    (the autotuner's layout choice for its size bucket)."""
+    n = C.c_int()
+    _check(lib().winds_bs_last_chained(C.byref(n)))
+    return bool(n.value)
+
+
 def set_autotune(on: bool):
     _check(lib().winds_bs_set_autotune(1 if on else 0))
 
 
 def set_tuning(core, n_targets, n_filaments, T, KF, waves=8.0):
     _check(lib().winds_bs_set_tuning(core, n_targets, n_filaments, T, KF, waves))
+
+
+def set_layout(core, n_targets, n_filaments, chained):
+    """Stream layout of a bucket's FP32c evaluations (chained or input order)."""
+    L = lib()
+    L.winds_bs_set_layout.argtypes = [C.c_int, C.c_longlong, C.c_longlong, C.c_int]
+    _check(L.winds_bs_set_layout(core, n_targets, n_filaments, 1 if chained else 0))
 
 
 def get_tuning(core, n_targets, n_filaments):

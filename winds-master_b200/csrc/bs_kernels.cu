@@ -6,13 +6,19 @@
 //   bs_pack_filaments  MATLAB-layout F1/F2/gamma/rc -> packed SoA float4 tiles
 //                      (+ FP64 copies), the device-side replacement of the host
 //                      crunch_f / crunch_rg packing (BiotSavartMex.cu:316-357)
+//   bs_chain_count,    the same records laid out along the wake's lines of
+//   bs_pack_chains     filaments (each lane of a record continuing the lane of
+//                      the record before: x2 = previous x1), with a head bit per
+//                      record where a line starts or the input has no link
 //   bs_pack_targets    MATLAB-layout P -> double4 targets (crunch_p, :361-379)
 //   bs_f32c            persistent FP32 direct sum on independent warp workers:
 //                      each warp stages its filament tiles into its own shared
 //                      memory by bulk copies (cp.async.bulk + mbarrier), keeps
 //                      T register-resident targets per lane, Kahan-compensates
 //                      the per-target sums, and recomputes the near-singular
-//                      pairs in FP64 with all 32 lanes
+//                      pairs in FP64 with all 32 lanes; on a chained stream
+//                      (CHAIN) each interaction reuses the previous record's
+//                      endpoint rsqrt
 //   bs_f64             plain FP64 direct sum (the comparison GPU path)
 //   bs_reduce          deterministic sum of the per-chunk partials, written in
 //                      MATLAB layout (reassem_uind, :383-401)
@@ -63,6 +69,121 @@ __global__ void bs_pad_filaments(long long from, long long to, float4 *pk, doubl
   const long long f = from + (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= to) return;
   pack_inert(f, pk, ra, rb);
+}
+
+// ------------------------------------------------------- chained packing
+// WInDS's filaments meet at the wake's nodes: the shed call's F2(i) is its
+// F1(i+1) (WInDS.m:150, along the first index) and the trailing call's
+// F2(:,:,j) is its F1(:,:,j-1) (WInDS.m:153, along the third). Laid out so that
+// each lane of a pair record follows one such line -- x2 of record r equal to
+// x1 of record r - 1 -- the FP32 kernel reuses the previous record's endpoint
+// term (interact_chain). bs_chain_count counts, per family, the filaments
+// whose end is bitwise the start of their neighbour along each index;
+// bs_pack_chains lays the family out along the index with more such links,
+// lines paired in the two lanes of the records, and flags every record where
+// either lane does not continue its predecessor (a head). Any layout of the
+// input is evaluated correctly: a filament that does not continue a chain is
+// a head, which the kernel evaluates from its own L.
+__device__ __forceinline__ bool same_point(const double *__restrict__ F2, long long b2,
+                                           const double *__restrict__ F1, long long b1,
+                                           long long d0) {
+  return F2[b2] == F1[b1] && F2[b2 + d0] == F1[b1 + d0] && F2[b2 + 2 * d0] == F1[b1 + 2 * d0];
+}
+
+__global__ void bs_chain_count(const double *__restrict__ F1, const double *__restrict__ F2,
+                               long long d0, long long d2, long long nf,
+                               unsigned long long *cnt) {
+  const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  bool s = false, t = false;
+  if (f < nf) {
+    const long long jb = f / d0, i = f - jb * d0, j = jb % d2;
+    const long long b = i + d0 * 3 * jb;
+    if (i + 1 < d0) s = same_point(F2, b, F1, b + 1, d0);   // F2(i) == F1(i+1)
+    if (j >= 1) t = same_point(F2, b, F1, b - 3 * d0, d0);  // F2(:,:,j) == F1(:,:,j-1)
+  }
+  const unsigned ns = __popc(__ballot_sync(0xffffffffu, s));
+  const unsigned nt = __popc(__ballot_sync(0xffffffffu, t));
+  if ((threadIdx.x & 31) == 0) {
+    if (ns) atomicAdd(cnt, (unsigned long long)ns);
+    if (nt) atomicAdd(cnt + 1, (unsigned long long)nt);
+  }
+}
+
+// Records of nl lines of len filaments: pairs of lines side by side, and an
+// odd last line split in two halves side by side.
+__host__ __device__ __forceinline__ long long chain_layout_records(long long nl, long long len) {
+  return nl / 2 * len + (nl & 1) * ((len + 1) / 2);
+}
+
+// One thread per lane slot of the family's nrec records from record rec_off:
+// slot 2 r + h is lane h of record r. Order along the third index when cnt[1]
+// > cnt[0] (lines (i, b), position k = j), else along the first (lines (j, b),
+// position k = d0 - 1 - i). Line 2 m + h fills lane h of the m-th run of `len`
+// records; an odd last line fills lane 0 with its first (len + 1) / 2
+// positions and lane 1 with the rest. Slots past the lines are inert heads.
+__global__ void bs_pack_chains(const double *__restrict__ F1, const double *__restrict__ F2,
+                               const double *__restrict__ gam, const double *__restrict__ rc,
+                               long long d0, long long d2, long long d3, long long rec_off,
+                               long long nrec, const unsigned long long *__restrict__ cnt,
+                               int model, double dcut, float4 *pk, double4 *ra, double4 *rb,
+                               unsigned *heads, BBox *bb) {
+  const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+  if (slot < 2 * nrec) {
+    const bool along3 = cnt[1] > cnt[0];
+    const long long nl = along3 ? d0 * d3 : d2 * d3;
+    const long long len = along3 ? d2 : d0;
+    const long long r = slot >> 1;
+    const long long h = slot & 1;
+    const long long f = 2 * rec_off + slot;  // packed filament index
+    long long k = 0, run = 0, line = -1;      // position in the line, in this lane's run
+    const long long full = nl / 2 * len, half = (len + 1) / 2;
+    if (r < full) {
+      const long long m = r / len;
+      run = k = r - m * len;
+      line = 2 * m + h;
+    } else if ((nl & 1) && r < full + half) {
+      run = r - full;
+      k = run + h * half;
+      if (k < len) line = nl - 1;
+    }
+    bool head;
+    if (line >= 0 && line < nl) {
+      long long i, jb;
+      if (along3) {
+        const long long bl = line / d0;
+        i = line - bl * d0;
+        jb = k + d2 * bl;
+      } else {
+        i = d0 - 1 - k;
+        jb = line;
+      }
+      const long long b = i + d0 * 3 * jb;
+      const double x1 = F1[b], y1 = F1[b + d0], z1 = F1[b + 2 * d0];
+      const double x2 = F2[b], y2 = F2[b + d0], z2 = F2[b + 2 * d0];
+      const long long src = i + d0 * jb;
+      pack_filament(f, x1, y1, z1, x2, y2, z2, gam[src], rc[src], model, dcut, pk, ra, rb);
+      lo[0] = (float)fmin(x1, x2), lo[1] = (float)fmin(y1, y2), lo[2] = (float)fmin(z1, z2);
+      hi[0] = (float)fmax(x1, x2), hi[1] = (float)fmax(y1, y2), hi[2] = (float)fmax(z1, z2);
+      // the predecessor in the line is (i, j-1) along the third index, (i+1, j) along the first
+      head = run == 0 || !(along3 ? same_point(F2, b, F1, b - 3 * d0, d0)
+                                  : same_point(F2, b, F1, b + 1, d0));
+    } else {
+      pack_inert(f, pk, ra, rb);
+      head = true;  // never continues a real lane (its x2 would not be its own)
+    }
+    if (head) atomicOr(heads + (f >> 6), 1u << ((f >> 1) & 31));
+  }
+  bbox_accumulate(lo, hi, bb->fmin, bb->fmax);
+}
+
+// Inert filaments filling [from, to) of a chained stream, their records heads.
+__global__ void bs_pad_chains(long long from, long long to, float4 *pk, double4 *ra, double4 *rb,
+                              unsigned *heads) {
+  const long long f = from + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= to) return;
+  pack_inert(f, pk, ra, rb);
+  atomicOr(heads + (f >> 6), 1u << ((f >> 1) & 31));
 }
 
 __global__ void bs_pack_targets(const double *__restrict__ P, long long ns, long long np,
@@ -326,6 +447,122 @@ __device__ __forceinline__ void interact2(float2 npx, float2 npy, float2 npz, co
   az = __ffma2_rn(ub, cz, az);
 }
 
+// interact2 on chained pair records. In a chained stream the second endpoint
+// of each filament (per lane of the record) is the first endpoint of the same
+// lane's filament in the previous record -- the wake's filaments meet at its
+// nodes -- so 1/|x2 - P| is the previous record's 1/|x1 - P|, carried in `ti`,
+// and x2 - P is the previous record's re-centred x1 (qp, shared by the lane's
+// targets) plus -(P - c): every interaction needs one rsqrt fewer, for the
+// same FP32 operations. A record that starts a chain (HEAD) forms r2 from L
+// as interact2 does. Either way 1/|x1 - P| is left in `ti` for the next record.
+template <int MODEL, bool CO, bool NEAR, bool HEAD>
+__device__ __forceinline__ void interact_chain(float2 npx, float2 npy, float2 npz, const Fil2 &f,
+                                               float2 qpx, float2 qpy, float2 qpz, float2 Rn2,
+                                               float co2, float2 &ax, float2 &ay, float2 &az,
+                                               unsigned &bits, unsigned bit0, unsigned bit1,
+                                               float2 &ti) {
+  const float2 nx = __fadd2_rn(f.qx, npx);  // x1 - P = -r1
+  const float2 ny = __fadd2_rn(f.qy, npy);
+  const float2 nz = __fadd2_rn(f.qz, npz);
+  float2 r1s = __fmul2_rn(nx, nx);
+  r1s = __ffma2_rn(ny, ny, r1s);
+  r1s = __ffma2_rn(nz, nz, r1s);
+  float2 dot, i2, r2s;
+  if (HEAD) {
+    float2 ld = __fmul2_rn(f.Lx, nx);  // -L.r1
+    ld = __ffma2_rn(f.Ly, ny, ld);
+    ld = __ffma2_rn(f.Lz, nz, ld);
+    dot = __fadd2_rn(r1s, ld);                   // r1 . r2
+    r2s = __fadd2_rn(dot, __fadd2_rn(f.L2, ld));  // |r1 - L|^2
+    i2 = rsqrt2(r2s);
+  } else {
+    const float2 mx = __fadd2_rn(qpx, npx);  // x2 - P = -r2
+    const float2 my = __fadd2_rn(qpy, npy);
+    const float2 mz = __fadd2_rn(qpz, npz);
+    dot = __fmul2_rn(nx, mx);  // r1 . r2
+    dot = __ffma2_rn(ny, my, dot);
+    dot = __ffma2_rn(nz, mz, dot);
+    i2 = ti;
+    if (CO) {
+      r2s = __fmul2_rn(mx, mx);
+      r2s = __ffma2_rn(my, my, r2s);
+      r2s = __ffma2_rn(mz, mz, r2s);
+    }
+  }
+  const float2 i1 = rsqrt2(r1s);
+  const float2 gg = __fmul2_rn(i1, i2);
+  const float2 e = __ffma2_rn(dot, gg, make_float2(1.f, 1.f));  // 1 + cos(theta)
+  const float2 cx = __ffma2_rn(ny, f.Mz, __fmul2_rn(nz, neg2(f.My)));
+  const float2 cy = __ffma2_rn(nz, f.Mx, __fmul2_rn(nx, neg2(f.Mz)));
+  const float2 cz = __ffma2_rn(nx, f.My, __fmul2_rn(ny, neg2(f.Mx)));
+  float2 ub;
+  if (MODEL == kCoreVatistas) {
+    float2 c2 = __fmul2_rn(cx, cx);
+    c2 = __ffma2_rn(cy, cy, c2);
+    c2 = __ffma2_rn(cz, cz, c2);
+    const float2 q = __ffma2_rn(c2, c2, f.D);
+    const float2 w = __fmul2_rn(__fmul2_rn(__fadd2_rn(i1, i2), gg), c2);
+    ub = __fmul2_rn(w, rsqrt2(__fmul2_rn(__fmul2_rn(e, e), q)));
+  } else if (MODEL == kCoreFree) {
+    ub = __fmul2_rn(__fmul2_rn(__fadd2_rn(i1, i2), gg), rcp2(e));
+  } else {
+    ub = __fmul2_rn(__fmul2_rn(__fadd2_rn(i1, i2), gg),
+                    rcp2(__ffma2_rn(f.D, __fmul2_rn(gg, gg), e)));
+  }
+  if (NEAR) {
+    if (dot.x < Rn2.x) {
+      bits |= bit0;
+      ub.x = 0.f;
+    }
+    if (dot.y < Rn2.y) {
+      bits |= bit1;
+      ub.y = 0.f;
+    }
+  }
+  if (CO) {
+    if (fminf(r1s.x, r2s.x) > co2) ub.x = 0.f;
+    if (fminf(r1s.y, r2s.y) > co2) ub.y = 0.f;
+  }
+  ax = __ffma2_rn(ub, cx, ax);
+  ay = __ffma2_rn(ub, cy, ay);
+  az = __ffma2_rn(ub, cz, az);
+  ti = i1;
+}
+
+// One chained pair record against the lane's T targets, in form FORM
+// (kCoreFree, or the kernel's model), the record starting a chain or not;
+// (qx, qy, qz) hold the previous record's re-centred x1 and receive this one's.
+template <int T, int FORM, bool CO, bool NEAR>
+__device__ __forceinline__ void chain_record(const float4 *rec, bool head, float2 ncx, float2 ncy,
+                                             float2 ncz, const float2 (&npx)[T],
+                                             const float2 (&npy)[T], const float2 (&npz)[T],
+                                             float S2, float co2, float2 (&ax)[T],
+                                             float2 (&ay)[T], float2 (&az)[T], float2 &qx,
+                                             float2 &qy, float2 &qz, float2 (&ti)[T],
+                                             unsigned &nbits, int j) {
+  Fil2 f;
+  load_pair(rec, ncx, ncy, ncz, f);
+  // near-singular threshold, raised for threads whose targets spread far
+  // from their centre (as in the unchained careful path)
+  const float2 Rn2 = NEAR ? make_float2(fmaxf(f.Rn2.x, S2), fmaxf(f.Rn2.y, S2)) : f.Rn2;
+  if (head) {
+#pragma unroll
+    for (int t = 0; t < T; ++t)
+      interact_chain<FORM, CO, NEAR, true>(npx[t], npy[t], npz[t], f, qx, qy, qz, Rn2, co2,
+                                           ax[t], ay[t], az[t], nbits, 1u << (8 * (2 * j) + t),
+                                           1u << (8 * (2 * j + 1) + t), ti[t]);
+  } else {
+#pragma unroll
+    for (int t = 0; t < T; ++t)
+      interact_chain<FORM, CO, NEAR, false>(npx[t], npy[t], npz[t], f, qx, qy, qz, Rn2, co2,
+                                            ax[t], ay[t], az[t], nbits, 1u << (8 * (2 * j) + t),
+                                            1u << (8 * (2 * j + 1) + t), ti[t]);
+  }
+  qx = f.qx;
+  qy = f.qy;
+  qz = f.qz;
+}
+
 // A near-singular pair of a tile, listed in the tile's consumed stage: the
 // FP64 reference term `u` of filament `fidx` at the owner's target `slot`.
 struct NearEntry {
@@ -337,7 +574,7 @@ struct NearEntry {
 // streamed through the warp's S stages (tile g of the warp in stage g % S).
 // Returns false, for the whole warp, when a bounded wait ran out (the item is
 // abandoned after the copies in flight have landed).
-template <int T, int KF, int MODEL, bool CO>
+template <int T, int KF, int MODEL, bool CO, bool CHAIN>
 __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, unsigned char *stages,
                                           uint64_t *full, float *s_k, unsigned *s_nb,
                                           unsigned &gt, float2 (&npx)[T], float2 (&npy)[T],
@@ -428,6 +665,53 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, uns
           const bool free_ = rmin > 0.f && rmin * rmin >= kCutoffFreeSq * sqrtf(f[22]);
           mf = __ballot_sync(0xffffffffu, free_);
         }
+      }
+      if constexpr (CHAIN) {
+        // Chained records: bit j of hm is set when record j of the word starts
+        // a chain (the word's first record always does: no carry crosses a
+        // word). The carry holds the previous record's x1 - P and 1/|x1 - P|.
+        const unsigned r0 = (unsigned)((it.f_begin + i * KF + 32 * w) >> 1);
+        const unsigned hm = ((__ldg(a.heads + (r0 >> 5)) >> (r0 & 31u)) & 0xffffu) | 1u;
+        float2 qx, qy, qz, ti[T];
+        unsigned unused = 0;
+        if (m == 0u && mf == 0xffffffffu) {
+          free_cnt += 32u * live_slots;
+#pragma unroll 2
+          for (int j = 0; j < 16; ++j)
+            chain_record<T, kCoreFree, false, false>(sP + (16 * w + j) * 8, (hm >> j) & 1u, ncx,
+                                                     ncy, ncz, npx, npy, npz, S2, co2, ax, ay, az,
+                                                     qx, qy, qz, ti, unused, 0);
+          continue;
+        }
+#pragma unroll 1
+        for (int g = 0; g < 8; ++g) {
+          const int kk = 32 * w + 4 * g;
+          const unsigned hg = hm >> (2 * g);
+          if (((m >> (4 * g)) & 0xfu) == 0u && ((mf >> (4 * g)) & 0xfu) == 0xfu) {
+            free_cnt += 4u * live_slots;
+#pragma unroll
+            for (int j = 0; j < 2; ++j)
+              chain_record<T, kCoreFree, false, false>(sP + (kk / 2 + j) * 8, (hg >> j) & 1u, ncx,
+                                                       ncy, ncz, npx, npy, npz, S2, co2, ax, ay,
+                                                       az, qx, qy, qz, ti, unused, j);
+          } else if (((m >> (4 * g)) & 0xfu) == 0u) {
+#pragma unroll
+            for (int j = 0; j < 2; ++j)
+              chain_record<T, MODEL, false, false>(sP + (kk / 2 + j) * 8, (hg >> j) & 1u, ncx,
+                                                   ncy, ncz, npx, npy, npz, S2, co2, ax, ay, az,
+                                                   qx, qy, qz, ti, unused, j);
+          } else {
+            careful |= 1u << (8 * w + g);
+            unsigned nbits = 0;
+#pragma unroll
+            for (int j = 0; j < 2; ++j)
+              chain_record<T, MODEL, CO, true>(sP + (kk / 2 + j) * 8, (hg >> j) & 1u, ncx, ncy,
+                                               ncz, npx, npy, npz, S2, co2, ax, ay, az, qx, qy,
+                                               qz, ti, nbits, j);
+            s_nb[(kk / 4) * 32 + lane] = nbits;
+          }
+        }
+        continue;
       }
       if (m == 0u && mf == 0xffffffffu) {
         // the whole word far and core-free: one loop over its 16 pairs
@@ -594,13 +878,14 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, uns
 // (80 registers), 5 for T = 3 (96), 4 for T = 4 (128), 2 for T = 8 (255). The
 // packed loop keeps each target as broadcast pairs and its sums as pairs (12
 // registers a target).
-template <int T>
+template <int T, bool CHAIN>
 struct MinBlocks {
-  static constexpr int value = T <= 2 ? 6 : (T == 3 ? 5 : (T <= 4 ? 4 : 2));
+  static constexpr int value = CHAIN ? (T <= 2 ? 5 : (T == 3 ? 4 : (T <= 4 ? 3 : 2)))
+                                     : (T <= 2 ? 6 : (T == 3 ? 5 : (T <= 4 ? 4 : 2)));
 };
 
-template <int T, int KF, int MODEL>
-__global__ void __launch_bounds__(kThreads, MinBlocks<T>::value) bs_f32c(const F32cArgs a) {
+template <int T, int KF, int MODEL, bool CHAIN>
+__global__ void __launch_bounds__(kThreads, MinBlocks<T, CHAIN>::value) bs_f32c(const F32cArgs a) {
   static_assert(KF % 32 == 0 && KF / 4 <= 32, "one screen word per 32 filaments, one bit per group");
   constexpr int S = StageSmem<KF>::kStages;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -706,11 +991,12 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<T>::value) bs_f32c(const F
     __syncwarp();
     bool ok;
     if (co_on)
-      ok = f32c_item<T, KF, MODEL, true>(a, it, stages, full, s_k, s_nb, gt, npx, npy, npz, ncx,
-                                         ncy, ncz, S2, ws, near_cnt, free_cnt, tl);
+      ok = f32c_item<T, KF, MODEL, true, CHAIN>(a, it, stages, full, s_k, s_nb, gt, npx, npy, npz,
+                                                ncx, ncy, ncz, S2, ws, near_cnt, free_cnt, tl);
     else
-      ok = f32c_item<T, KF, MODEL, false>(a, it, stages, full, s_k, s_nb, gt, npx, npy, npz, ncx,
-                                          ncy, ncz, S2, ws, near_cnt, free_cnt, tl);
+      ok = f32c_item<T, KF, MODEL, false, CHAIN>(a, it, stages, full, s_k, s_nb, gt, npx, npy,
+                                                 npz, ncx, ncy, ncz, S2, ws, near_cnt, free_cnt,
+                                                 tl);
     if (!ok) break;
     double *part = a.part + (size_t)item_id * 3 * a.tile_cap;
 #pragma unroll
@@ -877,43 +1163,43 @@ __global__ void bs_wait_selftest(unsigned *err, unsigned long long limit_ns) {
 
 // ============================================================ host launchers
 namespace {
-template <int T, int KF, int MODEL>
+template <int T, int KF, int MODEL, bool CH>
 cudaError_t launch_f32c_t(const F32cArgs &a, int grid, cudaStream_t s) {
   const size_t smem = f32c_smem_bytes_t<T, KF>();
   static unsigned attr_set = 0;  // one bit per device: the attribute is per context
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev >= 32 || !(attr_set & (1u << dev))) {
-    cudaError_t e = cudaFuncSetAttribute(bs_f32c<T, KF, MODEL>,
+    cudaError_t e = cudaFuncSetAttribute(bs_f32c<T, KF, MODEL, CH>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(bs_f32c<T, KF, MODEL>,
+    e = cudaFuncSetAttribute(bs_f32c<T, KF, MODEL, CH>,
                              cudaFuncAttributePreferredSharedMemoryCarveout,
                              (int)cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
     if (dev < 32) attr_set |= (1u << dev);
   }
   // `grid` counts workers (warps); kWarps of them per CTA
-  bs_f32c<T, KF, MODEL><<<(grid + kWarps - 1) / kWarps, kThreads, smem, s>>>(a);
+  bs_f32c<T, KF, MODEL, CH><<<(grid + kWarps - 1) / kWarps, kThreads, smem, s>>>(a);
   return cudaGetLastError();
 }
 
-template <int T, int KF, int MODEL>
+template <int T, int KF, int MODEL, bool CH>
 int occupancy_t() {
   const size_t smem = f32c_smem_bytes_t<T, KF>();
-  cudaFuncSetAttribute(bs_f32c<T, KF, MODEL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaFuncSetAttribute(bs_f32c<T, KF, MODEL, CH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)smem);
-  cudaFuncSetAttribute(bs_f32c<T, KF, MODEL>, cudaFuncAttributePreferredSharedMemoryCarveout,
+  cudaFuncSetAttribute(bs_f32c<T, KF, MODEL, CH>, cudaFuncAttributePreferredSharedMemoryCarveout,
                        (int)cudaSharedmemCarveoutMaxShared);
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bs_f32c<T, KF, MODEL>, kThreads, smem) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bs_f32c<T, KF, MODEL, CH>, kThreads, smem) !=
       cudaSuccess)
     return kWarps;
   return (n > 0 ? n : 1) * kWarps;  // resident workers per SM
 }
 
 #define WINDS_F32C_CASE(FN, M, TT, KK, ...) \
-  case M * 1000 + TT * 100 + KK / 32: return FN<TT, KK, M>(__VA_ARGS__);
+  case M * 1000 + TT * 100 + KK / 32: return FN<TT, KK, M, CH>(__VA_ARGS__);
 #define WINDS_F32C_DISPATCH(FN, ...)                                                    \
   switch (model * 1000 + T * 100 + KF / 32) {                                          \
     WINDS_F32C_CASE(FN, 0, 2, 32, __VA_ARGS__) WINDS_F32C_CASE(FN, 0, 2, 64, __VA_ARGS__) \
@@ -941,14 +1227,28 @@ int f32c_threads() { return 32; }  // lanes of one worker: a tile holds 32 x T t
 int f64_threads() { return kF64Threads; }
 int f64_tile() { return kF64Tile; }
 
-cudaError_t launch_f32c(const F32cArgs &a, int model, int T, int KF, int grid, cudaStream_t s) {
+namespace {
+template <bool CH>
+cudaError_t launch_f32c_ch(const F32cArgs &a, int model, int T, int KF, int grid, cudaStream_t s) {
   WINDS_F32C_DISPATCH(launch_f32c_t, a, grid, s)
   return cudaErrorInvalidValue;
 }
 
-int f32c_occupancy(int model, int T, int KF) {
+template <bool CH>
+int f32c_occupancy_ch(int model, int T, int KF) {
   WINDS_F32C_DISPATCH(occupancy_t)
   return 1;
+}
+}  // namespace
+
+// a.heads set: the filament stream is chained (bs_pack_chains)
+cudaError_t launch_f32c(const F32cArgs &a, int model, int T, int KF, int grid, cudaStream_t s) {
+  return a.heads ? launch_f32c_ch<true>(a, model, T, KF, grid, s)
+                 : launch_f32c_ch<false>(a, model, T, KF, grid, s);
+}
+
+int f32c_occupancy(int model, int T, int KF, bool chain) {
+  return chain ? f32c_occupancy_ch<true>(model, T, KF) : f32c_occupancy_ch<false>(model, T, KF);
 }
 
 int f64_occupancy() {
@@ -986,6 +1286,42 @@ cudaError_t launch_pad_filaments(long long from, long long to, const PackedFilam
   const int bs = 256;
   const long long grid = (to - from + bs - 1) / bs;
   bs_pad_filaments<<<(unsigned)grid, bs, 0, s>>>(from, to, pf.pk, pf.ra, pf.rb);
+  return cudaGetLastError();
+}
+
+// Records of a [d0,3,d2,d3] family in a chained stream: room for the layout
+// along either index (the device picks one; the rest of the room is inert).
+long long chain_records(long long d0, long long d2, long long d3) {
+  if (d0 <= 0 || d2 <= 0 || d3 <= 0) return 0;
+  const long long a = chain_layout_records(d2 * d3, d0), b = chain_layout_records(d0 * d3, d2);
+  return a > b ? a : b;
+}
+
+cudaError_t launch_pack_chains(const double *F1, const double *F2, const double *gam,
+                               const double *rc, const long long d[4], long long rec_off,
+                               unsigned long long *cnt, int model, double dcut,
+                               const PackedFilaments &pf, unsigned *heads, BBox *bb,
+                               cudaStream_t s) {
+  const long long nf = d[0] * d[2] * d[3];
+  const long long nrec = chain_records(d[0], d[2], d[3]);
+  if (nf <= 0 || nrec <= 0) return cudaSuccess;
+  const int bs = 256;
+  cudaError_t e = cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return e;
+  bs_chain_count<<<(unsigned)((nf + bs - 1) / bs), bs, 0, s>>>(F1, F2, d[0], d[2], nf, cnt);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  bs_pack_chains<<<(unsigned)((2 * nrec + bs - 1) / bs), bs, 0, s>>>(
+      F1, F2, gam, rc, d[0], d[2], d[3], rec_off, nrec, cnt, model, dcut, pf.pk, pf.ra, pf.rb,
+      heads, bb);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pad_chains(long long from, long long to, const PackedFilaments &pf,
+                              unsigned *heads, cudaStream_t s) {
+  if (to <= from) return cudaSuccess;
+  const int bs = 256;
+  bs_pad_chains<<<(unsigned)((to - from + bs - 1) / bs), bs, 0, s>>>(from, to, pf.pk, pf.ra, pf.rb,
+                                                                     heads);
   return cudaGetLastError();
 }
 

@@ -23,7 +23,7 @@ bool f32c_config_supported(int T, int KF);
 int f32c_threads();
 int f64_threads();
 int f64_tile();
-int f32c_occupancy(int model, int T, int KF);
+int f32c_occupancy(int model, int T, int KF, bool chain = false);
 int f64_occupancy();
 unsigned long long default_wait_limit_ns();
 
@@ -34,6 +34,17 @@ cudaError_t launch_pack_filaments(const double *F1, const double *F2, const doub
                                   cudaStream_t s);
 cudaError_t launch_pad_filaments(long long from, long long to, const PackedFilaments &pf,
                                  cudaStream_t s);
+// Chained filament stream (the FP32c path): records per [d0,3,d2,d3] family,
+// and the packing of one family from record rec_off (cnt: 2 device words of
+// scratch per family; heads zeroed beforehand, one bit per record).
+long long chain_records(long long d0, long long d2, long long d3);
+cudaError_t launch_pack_chains(const double *F1, const double *F2, const double *gam,
+                               const double *rc, const long long d[4], long long rec_off,
+                               unsigned long long *cnt, int model, double dcut,
+                               const PackedFilaments &pf, unsigned *heads, BBox *bb,
+                               cudaStream_t s);
+cudaError_t launch_pad_chains(long long from, long long to, const PackedFilaments &pf,
+                              unsigned *heads, cudaStream_t s);
 cudaError_t launch_pack_targets(const double *P, long long ns, long long np, long long off,
                                 int group, double4 *tp, int *tgroup, BBox *bb, cudaStream_t s);
 cudaError_t launch_target_keys(const double4 *tp, const int *tgroup, long long n, const BBox *bb,

@@ -12,6 +12,11 @@
 //   with D = (K^2 rc^2 |L|^2)^2 (Vatistas: the core term scaled like |K L x r1|^4,
 //   so K cancels from the core factor and enters only through K L) or d |L|^2
 //   (cut-off)
+//   For the FP32c evaluations the records form a chained stream: the lines of
+//   filaments of each family (the shed call's along the span, the trailing
+//   call's along the wake age) fill the two lanes of consecutive records so
+//   that x2 of a lane is x1 of the same lane one record earlier, except at the
+//   records flagged in a head bit array (F32cArgs::heads).
 //   raw FP64 filaments for near-singular terms and the FP64 path
 //     ra[f] = (x1, y1, z1, gamma)  rb[f] = (x2, y2, z2, rc^2)   double4
 //   targets  tp[t] = (x, y, z, 0) double4, sorted by (group, Morton code of the
@@ -82,6 +87,10 @@ struct F32cArgs {
   const Item *items;
   const int *order;  // work queue: queue position -> item (nullptr: identity)
   const GroupLive *live = nullptr;  // per group (nullptr: every tile and item is live)
+  // Chained stream (nullptr: unchained): bit (r & 31) of heads[r >> 5] is set
+  // when pair record r starts a chain, i.e. when either of its filaments does
+  // not end where the same lane's filament of record r - 1 begins.
+  const unsigned *heads = nullptr;
   int n_items;
   int tile_cap;
   double *part;

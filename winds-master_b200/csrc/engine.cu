@@ -292,15 +292,19 @@ int upload_plan(Context *c, const Plan &pl, cudaStream_t s) {
 }
 
 // ------------------------------------------------------------- packing
+// chain: lay the filaments out as a chained stream (the FP32c kernel's
+// faster form; bs_pack_chains), else in input order.
 int pack_inputs(Context *c, const winds_bs_family *fams, int nfam,
                 const std::vector<TargetSpec> &tsets, int model, double dcut, cudaStream_t s,
-                long long *nf_real, long long *nf_pad, long long *nt_total) {
-  long long nf = 0;
+                long long *nf_real, long long *nf_pad, long long *nt_total, bool chain) {
+  long long nf = 0, nrec = 0;
   for (int k = 0; k < nfam; ++k) {
     const long long *d = fams[k].dims;
     nf += d[0] * d[2] * d[3];
+    nrec += chain_records(d[0], d[2], d[3]);
   }
-  const long long nfp = std::max<long long>(round_up(nf, kFilamentPad), kFilamentPad);
+  const long long nfp =
+      std::max<long long>(round_up(chain ? 2 * nrec : nf, kFilamentPad), kFilamentPad);
   long long nt = 0;
   for (const TargetSpec &t : tsets) nt += t.count;
   int rc;
@@ -314,6 +318,9 @@ int pack_inputs(Context *c, const winds_bs_family *fams, int nfam,
       (rc = c->vals.ensure(std::max<long long>(nt, 1) * sizeof(int), s)) ||
       (rc = c->perm.ensure(std::max<long long>(nt, 1) * sizeof(int), s)))
     return rc;
+  if (chain && ((rc = c->heads.ensure((nfp / 64 + 1) * sizeof(unsigned), s)) ||
+                (rc = c->chaincnt.ensure(std::max(nfam, 1) * 2 * sizeof(unsigned long long), s))))
+    return rc;
   size_t sort_bytes = 0;
   if (sort_target_keys(nullptr, &sort_bytes, nullptr, nullptr, nullptr, nullptr, nt, s) !=
       cudaSuccess)
@@ -322,18 +329,37 @@ int pack_inputs(Context *c, const winds_bs_family *fams, int nfam,
   PackedFilaments pf{(float4 *)c->pk.p, (double4 *)c->ra.p, (double4 *)c->rb.p};
   cudaError_t e = launch_bbox_init((BBox *)c->bbox.p, s);
   c->launches += 1;
-  long long off = 0;
-  for (int k = 0; k < nfam && e == cudaSuccess; ++k) {
-    const long long *d = fams[k].dims;
-    const long long n = d[0] * d[2] * d[3];
-    e = launch_pack_filaments(fams[k].F1, fams[k].F2, fams[k].gamma, fams[k].rc, d[0], n, off,
-                              model, dcut, pf, (BBox *)c->bbox.p, s);
-    c->launches += n > 0;
-    off += n;
-  }
-  if (e == cudaSuccess) {
-    e = launch_pad_filaments(nf, nfp, pf, s);
-    c->launches += nfp > nf;
+  c->chained = chain;
+  if (chain) {
+    unsigned *heads = (unsigned *)c->heads.p;
+    if (e == cudaSuccess) e = cudaMemsetAsync(heads, 0, (nfp / 64 + 1) * sizeof(unsigned), s);
+    long long roff = 0;
+    for (int k = 0; k < nfam && e == cudaSuccess; ++k) {
+      const long long *d = fams[k].dims;
+      e = launch_pack_chains(fams[k].F1, fams[k].F2, fams[k].gamma, fams[k].rc, d,
+                             roff, (unsigned long long *)c->chaincnt.p + 2 * k, model, dcut, pf,
+                             heads, (BBox *)c->bbox.p, s);
+      c->launches += d[0] * d[2] * d[3] > 0 ? 2 : 0;
+      roff += chain_records(d[0], d[2], d[3]);
+    }
+    if (e == cudaSuccess) {
+      e = launch_pad_chains(2 * nrec, nfp, pf, heads, s);
+      c->launches += nfp > 2 * nrec;
+    }
+  } else {
+    long long off = 0;
+    for (int k = 0; k < nfam && e == cudaSuccess; ++k) {
+      const long long *d = fams[k].dims;
+      const long long n = d[0] * d[2] * d[3];
+      e = launch_pack_filaments(fams[k].F1, fams[k].F2, fams[k].gamma, fams[k].rc, d[0], n, off,
+                                model, dcut, pf, (BBox *)c->bbox.p, s);
+      c->launches += n > 0;
+      off += n;
+    }
+    if (e == cudaSuccess) {
+      e = launch_pad_filaments(nf, nfp, pf, s);
+      c->launches += nfp > nf;
+    }
   }
   long long toff = 0;
   int gid = 0;
@@ -367,8 +393,9 @@ int pack_inputs(Context *c, const winds_bs_family *fams, int nfam,
 struct TuneKey {
   int model;
   int tb, fb;  // log2 buckets of targets and filaments
+  bool eval;   // the evaluation entry points (layout included in the choice)
   bool operator<(const TuneKey &o) const {
-    return std::tie(model, tb, fb) < std::tie(o.model, o.tb, o.fb);
+    return std::tie(model, tb, fb, eval) < std::tie(o.model, o.tb, o.fb, o.eval);
   }
 };
 static std::mutex g_tune_mu;
@@ -394,17 +421,17 @@ TuneChoice default_choice(long long nt) {
   return ch;
 }
 
-bool lookup_tune(int model, long long nt, long long nf, TuneChoice *out) {
+bool lookup_tune(int model, long long nt, long long nf, TuneChoice *out, bool eval) {
   std::lock_guard<std::mutex> g(g_tune_mu);
-  auto it = g_tune.find(TuneKey{model, log2_bucket(nt), log2_bucket(nf)});
+  auto it = g_tune.find(TuneKey{model, log2_bucket(nt), log2_bucket(nf), eval});
   if (it == g_tune.end()) return false;
   *out = it->second;
   return true;
 }
 
-void store_tune(int model, long long nt, long long nf, const TuneChoice &ch) {
+void store_tune(int model, long long nt, long long nf, const TuneChoice &ch, bool eval) {
   std::lock_guard<std::mutex> g(g_tune_mu);
-  g_tune[TuneKey{model, log2_bucket(nt), log2_bucket(nf)}] = ch;
+  g_tune[TuneKey{model, log2_bucket(nt), log2_bucket(nf), eval}] = ch;
 }
 
 // ------------------------------------------------------------- evaluation
@@ -420,7 +447,7 @@ int run_direct_sum(Context *c, const std::vector<GroupSpec> &gs, int model, doub
   } else {
     if (!f32c_config_supported(ch.T, ch.KF)) return fail(WINDS_BS_ERR_ARG, "bad tile choice");
     tile_cap = f32c_threads() * ch.T;
-    resident = f32c_occupancy(model, ch.T, ch.KF) * c->num_sms;
+    resident = f32c_occupancy(model, ch.T, ch.KF, c->chained) * c->num_sms;
     quantum = kFilamentPad;
   }
   // sequential: one chunk per tile, so every target sums its filaments in order
@@ -473,6 +500,7 @@ int run_direct_sum(Context *c, const std::vector<GroupSpec> &gs, int model, doub
   a.n = n;
   a.co = co;
   a.wait_limit_ns = default_wait_limit_ns();
+  a.heads = precision == WINDS_PREC_F32C && c->chained ? (const unsigned *)c->heads.p : nullptr;
   cudaError_t e = cudaMemsetAsync(c->ctr.p, 0, sizeof(unsigned), s);
   // near-singular pairs are counted per evaluation
   if (e == cudaSuccess) e = cudaMemsetAsync(c->nearctr.p, 0, 2 * sizeof(unsigned long long), s);
@@ -534,19 +562,15 @@ int resolve_model(const winds_bs_params *prm, int *model, double *dcut, double *
   return WINDS_BS_OK;
 }
 
-int eval_device(Context *c, const winds_bs_family *fams, int nfam,
-                const std::vector<TargetSpec> &tsets, const winds_bs_params *prm,
-                cudaStream_t s, bool sequential) {
-  int model, prec, rc;
-  double dcut, n;
-  if ((rc = resolve_model(prm, &model, &dcut, &n, &prec))) return rc;
-  for (int k = 0; k < nfam; ++k)
-    if ((rc = validate_family(fams[k]))) return rc;
-  c->launches = 0;
-  long long nf, nfp, nt;
-  if ((rc = pack_inputs(c, fams, nfam, tsets, model, dcut, s, &nf, &nfp, &nt))) return rc;
-  if (nt == 0) return WINDS_BS_OK;
-  std::vector<GroupSpec> gs;
+// Packs the inputs in one layout and describes one group per target set.
+static int pack_groups(Context *c, const winds_bs_family *fams, int nfam,
+                       const std::vector<TargetSpec> &tsets, int model, double dcut,
+                       cudaStream_t s, bool chain, std::vector<GroupSpec> *gs, long long *nf,
+                       long long *nt) {
+  long long nfp;
+  int rc;
+  if ((rc = pack_inputs(c, fams, nfam, tsets, model, dcut, s, nf, &nfp, nt, chain))) return rc;
+  gs->clear();
   long long toff = 0;
   for (const TargetSpec &t : tsets) {
     GroupSpec g;
@@ -557,34 +581,59 @@ int eval_device(Context *c, const winds_bs_family *fams, int nfam,
     g.f_begin = 0;
     g.f_end = (int)nfp;
     g.accumulate = t.accumulate;
-    gs.push_back(g);
+    gs->push_back(g);
     toff += t.count;
   }
-  TuneChoice ch;
-  if (prec == WINDS_PREC_F32C && !sequential) {
-    if (!lookup_tune(model, nt, nf, &ch)) {
-      if (c->autotune && s == c->stream) {
-        if ((rc = autotune(c, gs, model, dcut, n, prm->co, nt, nf, &ch))) return rc;
-      } else {
-        ch = default_choice(nt);
-      }
+  return WINDS_BS_OK;
+}
+
+int eval_device(Context *c, const winds_bs_family *fams, int nfam,
+                const std::vector<TargetSpec> &tsets, const winds_bs_params *prm,
+                cudaStream_t s, bool sequential) {
+  int model, prec, rc;
+  double dcut, n;
+  if ((rc = resolve_model(prm, &model, &dcut, &n, &prec))) return rc;
+  for (int k = 0; k < nfam; ++k)
+    if ((rc = validate_family(fams[k]))) return rc;
+  c->launches = 0;
+  long long nf = 0, nt = 0;
+  for (int k = 0; k < nfam; ++k) nf += fams[k].dims[0] * fams[k].dims[2] * fams[k].dims[3];
+  for (const TargetSpec &t : tsets) nt += t.count;
+  // The FP64 path (and the sequential mode that reproduces the reference's
+  // order) runs on the input order. FP32c runs on the layout its tuned choice
+  // names; the autotuner times both layouts, each with every tiling.
+  const bool fast = prec == WINDS_PREC_F32C && !sequential;
+  TuneChoice ch = default_choice(nt);
+  std::vector<GroupSpec> gs;
+  if (fast && nt > 0 && !lookup_tune(model, nt, nf, &ch, true) && c->autotune && s == c->stream) {
+    float best_ms = 1e30f;
+    for (int layout = 0; layout < 2; ++layout) {
+      TuneChoice tc;
+      float ms = 1e30f;
+      if ((rc = pack_groups(c, fams, nfam, tsets, model, dcut, s, layout == 1, &gs, &nf, &nt)) ||
+          (rc = autotune(c, gs, model, dcut, n, prm->co, &tc, &ms)))
+        return rc;
+      tc.chain = layout == 1;
+      if (ms < best_ms) best_ms = ms, ch = tc;
     }
-  } else {
-    ch = default_choice(nt);
+    store_tune(model, nt, nf, ch, true);
   }
+  if ((rc = pack_groups(c, fams, nfam, tsets, model, dcut, s, fast && ch.chain, &gs, &nf, &nt)))
+    return rc;
+  if (nt == 0) return WINDS_BS_OK;
   return run_direct_sum(c, gs, model, dcut, n, prm->co, prec, sequential, ch, s, true);
 }
 
-// Times each candidate (T, KF, waves) twice after a warm-up and keeps the
-// fastest for this (model, log2 targets, log2 filaments) bucket.
+// Times each candidate (T, KF, waves) twice after a warm-up on the inputs as
+// packed and returns the fastest with its time.
 int autotune(Context *c, const std::vector<GroupSpec> &gs, int model, double dcut, double n,
-             double co, long long nt, long long nf, TuneChoice *best) {
+             double co, TuneChoice *best, float *best_ms_out) {
   // T = 8 (supported, settable) is left out: its unrolled paths run slower
   const int Ts[3] = {2, 3, 4};
   const int KFs[3] = {32, 64, 128};
   const double Ws[3] = {16.0, 32.0, 64.0};
   float best_ms = 1e30f;
-  TuneChoice bc = default_choice(nt);
+  TuneChoice bc;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -619,8 +668,8 @@ int autotune(Context *c, const std::vector<GroupSpec> &gs, int model, double dcu
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  store_tune(model, nt, nf, bc);
   *best = bc;
+  *best_ms_out = best_ms;
   return WINDS_BS_OK;
 }
 
@@ -813,6 +862,15 @@ int winds_bs_last_stats(double *main_ms, int *launches, long long *near_pairs) {
   return WINDS_BS_OK;
 }
 
+int winds_bs_last_chained(int *chained) {
+  int rc;
+  Context *c = get_context(&rc);
+  if (!c) return rc;
+  if (!chained) return WINDS_BS_ERR_ARG;
+  *chained = c->chained ? 1 : 0;
+  return WINDS_BS_OK;
+}
+
 int winds_bs_last_core_free(long long *pairs) {
   int rc;
   Context *c = get_context(&rc);
@@ -844,16 +902,29 @@ int winds_bs_set_tuning(int core_model, long long n_targets, long long n_filamen
   ch.T = T;
   ch.KF = KF;
   ch.waves = waves;
-  store_tune(core_model == WINDS_CORE_CUTOFF ? kCoreCutoff : kCoreVatistas, n_targets, n_filaments,
-             ch);
+  // for every FP32c path of the bucket: the evaluations' chained stream and
+  // the unchained ones
+  const int model = core_model == WINDS_CORE_CUTOFF ? kCoreCutoff : kCoreVatistas;
+  store_tune(model, n_targets, n_filaments, ch, true);
+  store_tune(model, n_targets, n_filaments, ch, false);
+  return WINDS_BS_OK;
+}
+
+int winds_bs_set_layout(int core_model, long long n_targets, long long n_filaments, int chained) {
+  const int model = core_model == WINDS_CORE_CUTOFF ? kCoreCutoff : kCoreVatistas;
+  TuneChoice ch;
+  if (!lookup_tune(model, n_targets, n_filaments, &ch, true)) ch = default_choice(n_targets);
+  ch.chain = chained != 0;
+  store_tune(model, n_targets, n_filaments, ch, true);
   return WINDS_BS_OK;
 }
 
 int winds_bs_get_tuning(int core_model, long long n_targets, long long n_filaments, int *T, int *KF,
                         double *waves) {
   TuneChoice ch;
-  if (!lookup_tune(core_model == WINDS_CORE_CUTOFF ? kCoreCutoff : kCoreVatistas, n_targets,
-                   n_filaments, &ch))
+  const int model = core_model == WINDS_CORE_CUTOFF ? kCoreCutoff : kCoreVatistas;
+  if (!lookup_tune(model, n_targets, n_filaments, &ch, true) &&
+      !lookup_tune(model, n_targets, n_filaments, &ch, false))
     ch = default_choice(n_targets);
   if (T) *T = ch.T;
   if (KF) *KF = ch.KF;

@@ -51,6 +51,7 @@ struct TuneChoice {
   int T = 4;
   int KF = 64;
   double waves = 8.0;
+  bool chain = false;  // FP32c on the chained filament stream (evaluation entry points)
 };
 
 struct Context {
@@ -65,6 +66,10 @@ struct Context {
   DevBuf groups, tiles, items, order, part;
   // small words
   DevBuf bbox, ctr, err, nearctr;
+  // chained filament stream (FP32c path): head bit per pair record, and the
+  // per-family link counts that choose each family's layout
+  DevBuf heads, chaincnt;
+  bool chained = false;  // the packed filaments are a chained stream
   // device copies of host inputs/outputs (host API)
   DevBuf in_P, in_F, out_u;
   HostBuf htab, hstat;
@@ -85,15 +90,18 @@ void build_plan(Plan &pl, const std::vector<GroupSpec> &gs, int tile_cap, int re
 int resolve_model(const winds_bs_params *prm, int *model, double *dcut, double *n, int *prec);
 int validate_family(const winds_bs_family &f);
 TuneChoice default_choice(long long nt);
-bool lookup_tune(int model, long long nt, long long nf, TuneChoice *out);
-void store_tune(int model, long long nt, long long nf, const TuneChoice &ch);
+// Tuned tilings per (model, log2 targets, log2 filaments) bucket, apart for
+// the evaluation entry points (eval = true: their choice includes the stream
+// layout) and the callers that pack their own unchained stream.
+bool lookup_tune(int model, long long nt, long long nf, TuneChoice *out, bool eval = false);
+void store_tune(int model, long long nt, long long nf, const TuneChoice &ch, bool eval = false);
 int cuda_fail(cudaError_t e, const char *what);
 Context *get_context(int *rc);
 int eval_device(Context *c, const winds_bs_family *fams, int nfam,
                 const std::vector<TargetSpec> &tsets, const winds_bs_params *prm, cudaStream_t s,
                 bool sequential);
 int autotune(Context *c, const std::vector<GroupSpec> &gs, int model, double dcut, double n,
-             double co, long long nt, long long nf, TuneChoice *best);
+             double co, TuneChoice *best, float *best_ms);
 int check_device_error(Context *c, cudaStream_t s);
 
 }  // namespace winds
