@@ -40,6 +40,9 @@ sys.path.insert(0, ROOT)
 # denominator (3), numerator (2), L.r1 and h^2 (8), the Vatistas factor (3),
 # scale (1), accumulate (6); rsqrt/rcp are counted apart (3 per interaction)
 FLOP_PER_INTERACTION = 52
+# the cut-off core's count: the d |L|^2 denominator term in place of h^2 and
+# the Vatistas factor
+FLOP_PER_INTERACTION_CUTOFF = 44
 METRIC = "biot_savart_gint_per_s"
 UNIT = "Gint/s"
 
@@ -55,6 +58,11 @@ def parse():
                     help="large: 3x41x720 (the metric's case); medium: 3x41x180 for profiling")
     ap.add_argument("--tiling", default=None,
                     help="force the FP32 tiling 'T,KF,waves' instead of the autotuner's choice")
+    ap.add_argument("--layout", default=None, choices=["input", "chained"],
+                    help="with --tiling: the filament stream layout (default: input order)")
+    ap.add_argument("--core", default="vatistas", choices=["vatistas", "cutoff"],
+                    help="profiling aid: the timed loop's core (cutoff: d = 1e-4); the metric's "
+                         "case is vatistas")
     ap.add_argument("--wake-steps", type=int, default=10,
                     help="timed pcc steps of the 64-case batched wake (0: skip)")
     ap.add_argument("--quick", action="store_true",
@@ -682,22 +690,25 @@ def ours(args):
     dP = (dev(P), P.shape)
     out = torch.zeros(P.size, dtype=torch.float64, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    core = wb.bs.CORE_VATISTAS
+    core, dval = ((wb.bs.CORE_CUTOFF, 1e-4) if args.core == "cutoff"
+                  else (wb.bs.CORE_VATISTAS, 2.0))
 
     torch.cuda.synchronize()
     if args.tiling:
         T, KF, waves = args.tiling.split(",")
-        wb.set_tuning(wb.bs.CORE_VATISTAS, nt, nf, int(T), int(KF), float(waves))
+        wb.set_tuning(core, nt, nf, int(T), int(KF), float(waves))
+        if args.layout:
+            wb.set_layout(core, nt, nf, args.layout == "chained")
     # warm-up on the library's own stream (the first call autotunes the tiling)
     for _ in range(max(1, args.warmup)):
-        wb.eval_device(dfams, dP, core, 2.0, 1000.0, out, "f32c")
+        wb.eval_device(dfams, dP, core, dval, 1000.0, out, "f32c")
     wb.sync()
     # timed work runs on a dedicated (non-default) stream shared with the events
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     sp = stream.cuda_stream
     for _ in range(2):
-        wb.eval_device(dfams, dP, core, 2.0, 1000.0, out, "f32c", stream=sp)
+        wb.eval_device(dfams, dP, core, dval, 1000.0, out, "f32c", stream=sp)
     peak = C.c_double()
     lib.winds_bs_fp32_peak(C.byref(peak))
 
@@ -716,7 +727,7 @@ def ours(args):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        wb.eval_device(dfams, dP, core, 2.0, 1000.0, out, "f32c", stream=sp)
+        wb.eval_device(dfams, dP, core, dval, 1000.0, out, "f32c", stream=sp)
         e1.record(stream)
         torch.cuda.synchronize()
         step_ms.append(e0.elapsed_time(e1))
@@ -742,7 +753,7 @@ def ours(args):
     rel_err = None
     if not (args.no_fp64 or args.quick):
         out64 = torch.zeros_like(out)
-        wb.eval_device(dfams, dP, core, 2.0, 1000.0, out64, "f64", stream=sp)
+        wb.eval_device(dfams, dP, core, dval, 1000.0, out64, "f64", stream=sp)
         torch.cuda.synchronize()
         t64 = []
         for _ in range(2):
@@ -750,7 +761,7 @@ def ours(args):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            wb.eval_device(dfams, dP, core, 2.0, 1000.0, out64, "f64", stream=sp)
+            wb.eval_device(dfams, dP, core, dval, 1000.0, out64, "f64", stream=sp)
             e1.record(stream)
             torch.cuda.synchronize()
             t64.append(e0.elapsed_time(e1))
@@ -813,19 +824,20 @@ def ours(args):
         hout = pin(np.zeros(P.shape, order="F"))
         h2d = sum(sum(x.nbytes for x in f) for f in hfams) + hP.nbytes
         d2h = hout.nbytes
-        wb.eval_host(hfams, hP, core, 2.0, 1000.0, "f32c", out=hout)
+        wb.eval_host(hfams, hP, core, dval, 1000.0, "f32c", out=hout)
         e2e_t = []
         for _ in range(max(1, min(args.steps, 5))):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            wb.eval_host(hfams, hP, core, 2.0, 1000.0, "f32c", out=hout)
+            wb.eval_host(hfams, hP, core, dval, 1000.0, "f32c", out=hout)
             e2e_t.append(time.perf_counter() - t0)
         e2e = world * interactions / statistics.median(e2e_t) / 1e9
         e2e_line = {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "timing": "wall clock around the synchronous host-API call"}
 
     mean_main = statistics.mean(main_ms)
-    achieved = FLOP_PER_INTERACTION * interactions / (mean_main * 1e-3) / 1e12
+    flop = FLOP_PER_INTERACTION if args.core == "vatistas" else FLOP_PER_INTERACTION_CUTOFF
+    achieved = flop * interactions / (mean_main * 1e-3) / 1e12
     traffic = profiled_traffic(interactions)
 
     cpu = None
@@ -865,7 +877,7 @@ def ours(args):
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                          "frac": achieved / peak.value if peak.value else None, "traffic": traffic,
                          "peak_source": "FFMA probe measured in this run (winds_bs_fp32_peak)",
-                         "kernel": "bs_f32c", "flop_per_interaction": FLOP_PER_INTERACTION,
+                         "kernel": "bs_f32c", "flop_per_interaction": flop,
                          "kernel_ms": mean_main},
             "cpu_baseline": cpu,
             "e2e": e2e_line,
