@@ -163,11 +163,13 @@ def bench_config(kind, nt, nf, world):
             "parallelism": f"replicated wakes x{world}" if world > 1 else "single GPU"}
 
 
-def profiled_traffic(interactions):
-    """DRAM bytes per launch of bs_f32c from the committed ncu summary
-    (dram__bytes_read.sum + dram__bytes_write.sum of one captured launch),
-    scaled to this launch by interactions; None without a summary."""
-    path = os.path.join(ROOT, "profiles", "bs_f32c_large.md")
+def profiled_traffic(interactions, chained=False):
+    """DRAM bytes per launch of bs_f32c from the committed ncu summary of its
+    stream layout (dram__bytes_read.sum + dram__bytes_write.sum of one
+    captured launch), scaled to this launch by interactions; None without a
+    summary."""
+    path = os.path.join(ROOT, "profiles",
+                        "bs_f32c_large_chained.md" if chained else "bs_f32c_large.md")
     if not os.path.exists(path):
         return None
     for line in open(path):
@@ -838,7 +840,7 @@ def ours(args):
     mean_main = statistics.mean(main_ms)
     flop = FLOP_PER_INTERACTION if args.core == "vatistas" else FLOP_PER_INTERACTION_CUTOFF
     achieved = flop * interactions / (mean_main * 1e-3) / 1e12
-    traffic = profiled_traffic(interactions)
+    traffic = profiled_traffic(interactions, chained)
 
     cpu = None
     if rank == 0 and world == 1 and not args.quick:

@@ -450,45 +450,32 @@ __device__ __forceinline__ void interact2(float2 npx, float2 npy, float2 npz, co
 // interact2 on chained pair records. In a chained stream the second endpoint
 // of each filament (per lane of the record) is the first endpoint of the same
 // lane's filament in the previous record -- the wake's filaments meet at its
-// nodes -- so 1/|x2 - P| is the previous record's 1/|x1 - P|, carried in `ti`,
-// and x2 - P is the previous record's re-centred x1 (qp, shared by the lane's
-// targets) plus -(P - c): every interaction needs one rsqrt fewer, for the
-// same FP32 operations. A record that starts a chain (HEAD) forms r2 from L
-// as interact2 does. Either way 1/|x1 - P| is left in `ti` for the next record.
+// nodes -- so 1/|x2 - P| is the previous record's 1/|x1 - P|, carried in `ti`:
+// a chained record needs neither |r2|^2 nor its rsqrt (two FP32 operations and
+// one MUFU result fewer per interaction). A record that starts a chain (HEAD)
+// forms them from L as interact2 does. Either way 1/|x1 - P| is left in `ti`
+// for the next record.
 template <int MODEL, bool CO, bool NEAR, bool HEAD>
 __device__ __forceinline__ void interact_chain(float2 npx, float2 npy, float2 npz, const Fil2 &f,
-                                               float2 qpx, float2 qpy, float2 qpz, float2 Rn2,
-                                               float co2, float2 &ax, float2 &ay, float2 &az,
-                                               unsigned &bits, unsigned bit0, unsigned bit1,
-                                               float2 &ti) {
+                                               float2 Rn2, float co2, float2 &ax, float2 &ay,
+                                               float2 &az, unsigned &bits, unsigned bit0,
+                                               unsigned bit1, float2 &ti) {
   const float2 nx = __fadd2_rn(f.qx, npx);  // x1 - P = -r1
   const float2 ny = __fadd2_rn(f.qy, npy);
   const float2 nz = __fadd2_rn(f.qz, npz);
   float2 r1s = __fmul2_rn(nx, nx);
   r1s = __ffma2_rn(ny, ny, r1s);
   r1s = __ffma2_rn(nz, nz, r1s);
-  float2 dot, i2, r2s;
-  if (HEAD) {
-    float2 ld = __fmul2_rn(f.Lx, nx);  // -L.r1
-    ld = __ffma2_rn(f.Ly, ny, ld);
-    ld = __ffma2_rn(f.Lz, nz, ld);
-    dot = __fadd2_rn(r1s, ld);                   // r1 . r2
-    r2s = __fadd2_rn(dot, __fadd2_rn(f.L2, ld));  // |r1 - L|^2
+  float2 ld = __fmul2_rn(f.Lx, nx);  // -L.r1
+  ld = __ffma2_rn(f.Ly, ny, ld);
+  ld = __ffma2_rn(f.Lz, nz, ld);
+  const float2 dot = __fadd2_rn(r1s, ld);  // r1 . r2
+  float2 r2s, i2;
+  if (HEAD || CO) r2s = __fadd2_rn(dot, __fadd2_rn(f.L2, ld));  // |r1 - L|^2
+  if (HEAD)
     i2 = rsqrt2(r2s);
-  } else {
-    const float2 mx = __fadd2_rn(qpx, npx);  // x2 - P = -r2
-    const float2 my = __fadd2_rn(qpy, npy);
-    const float2 mz = __fadd2_rn(qpz, npz);
-    dot = __fmul2_rn(nx, mx);  // r1 . r2
-    dot = __ffma2_rn(ny, my, dot);
-    dot = __ffma2_rn(nz, mz, dot);
+  else
     i2 = ti;
-    if (CO) {
-      r2s = __fmul2_rn(mx, mx);
-      r2s = __ffma2_rn(my, my, r2s);
-      r2s = __ffma2_rn(mz, mz, r2s);
-    }
-  }
   const float2 i1 = rsqrt2(r1s);
   const float2 gg = __fmul2_rn(i1, i2);
   const float2 e = __ffma2_rn(dot, gg, make_float2(1.f, 1.f));  // 1 + cos(theta)
@@ -530,15 +517,13 @@ __device__ __forceinline__ void interact_chain(float2 npx, float2 npy, float2 np
 }
 
 // One chained pair record against the lane's T targets, in form FORM
-// (kCoreFree, or the kernel's model), the record starting a chain or not;
-// (qx, qy, qz) hold the previous record's re-centred x1 and receive this one's.
+// (kCoreFree, or the kernel's model), the record starting a chain or not.
 template <int T, int FORM, bool CO, bool NEAR>
 __device__ __forceinline__ void chain_record(const float4 *rec, bool head, float2 ncx, float2 ncy,
                                              float2 ncz, const float2 (&npx)[T],
                                              const float2 (&npy)[T], const float2 (&npz)[T],
                                              float S2, float co2, float2 (&ax)[T],
-                                             float2 (&ay)[T], float2 (&az)[T], float2 &qx,
-                                             float2 &qy, float2 &qz, float2 (&ti)[T],
+                                             float2 (&ay)[T], float2 (&az)[T], float2 (&ti)[T],
                                              unsigned &nbits, int j) {
   Fil2 f;
   load_pair(rec, ncx, ncy, ncz, f);
@@ -548,19 +533,16 @@ __device__ __forceinline__ void chain_record(const float4 *rec, bool head, float
   if (head) {
 #pragma unroll
     for (int t = 0; t < T; ++t)
-      interact_chain<FORM, CO, NEAR, true>(npx[t], npy[t], npz[t], f, qx, qy, qz, Rn2, co2,
-                                           ax[t], ay[t], az[t], nbits, 1u << (8 * (2 * j) + t),
+      interact_chain<FORM, CO, NEAR, true>(npx[t], npy[t], npz[t], f, Rn2, co2, ax[t], ay[t],
+                                           az[t], nbits, 1u << (8 * (2 * j) + t),
                                            1u << (8 * (2 * j + 1) + t), ti[t]);
   } else {
 #pragma unroll
     for (int t = 0; t < T; ++t)
-      interact_chain<FORM, CO, NEAR, false>(npx[t], npy[t], npz[t], f, qx, qy, qz, Rn2, co2,
-                                            ax[t], ay[t], az[t], nbits, 1u << (8 * (2 * j) + t),
+      interact_chain<FORM, CO, NEAR, false>(npx[t], npy[t], npz[t], f, Rn2, co2, ax[t], ay[t],
+                                            az[t], nbits, 1u << (8 * (2 * j) + t),
                                             1u << (8 * (2 * j + 1) + t), ti[t]);
   }
-  qx = f.qx;
-  qy = f.qy;
-  qz = f.qz;
 }
 
 // A near-singular pair of a tile, listed in the tile's consumed stage: the
@@ -672,7 +654,7 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, uns
         // word). The carry holds the previous record's x1 - P and 1/|x1 - P|.
         const unsigned r0 = (unsigned)((it.f_begin + i * KF + 32 * w) >> 1);
         const unsigned hm = ((__ldg(a.heads + (r0 >> 5)) >> (r0 & 31u)) & 0xffffu) | 1u;
-        float2 qx, qy, qz, ti[T];
+        float2 ti[T];
         unsigned unused = 0;
         if (m == 0u && mf == 0xffffffffu) {
           free_cnt += 32u * live_slots;
@@ -680,7 +662,7 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, uns
           for (int j = 0; j < 16; ++j)
             chain_record<T, kCoreFree, false, false>(sP + (16 * w + j) * 8, (hm >> j) & 1u, ncx,
                                                      ncy, ncz, npx, npy, npz, S2, co2, ax, ay, az,
-                                                     qx, qy, qz, ti, unused, 0);
+                                                     ti, unused, 0);
           continue;
         }
 #pragma unroll 1
@@ -693,21 +675,21 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, uns
             for (int j = 0; j < 2; ++j)
               chain_record<T, kCoreFree, false, false>(sP + (kk / 2 + j) * 8, (hg >> j) & 1u, ncx,
                                                        ncy, ncz, npx, npy, npz, S2, co2, ax, ay,
-                                                       az, qx, qy, qz, ti, unused, j);
+                                                       az, ti, unused, j);
           } else if (((m >> (4 * g)) & 0xfu) == 0u) {
 #pragma unroll
             for (int j = 0; j < 2; ++j)
               chain_record<T, MODEL, false, false>(sP + (kk / 2 + j) * 8, (hg >> j) & 1u, ncx,
                                                    ncy, ncz, npx, npy, npz, S2, co2, ax, ay, az,
-                                                   qx, qy, qz, ti, unused, j);
+                                                   ti, unused, j);
           } else {
             careful |= 1u << (8 * w + g);
             unsigned nbits = 0;
 #pragma unroll
             for (int j = 0; j < 2; ++j)
               chain_record<T, MODEL, CO, true>(sP + (kk / 2 + j) * 8, (hg >> j) & 1u, ncx, ncy,
-                                               ncz, npx, npy, npz, S2, co2, ax, ay, az, qx, qy,
-                                               qz, ti, nbits, j);
+                                               ncz, npx, npy, npz, S2, co2, ax, ay, az, ti,
+                                               nbits, j);
             s_nb[(kk / 4) * 32 + lane] = nbits;
           }
         }
@@ -877,10 +859,13 @@ __device__ __forceinline__ bool f32c_item(const F32cArgs &a, const Item &it, uns
 // Resident CTAs per SM the register allocation is capped for: 6 for T = 2
 // (80 registers), 5 for T = 3 (96), 4 for T = 4 (128), 2 for T = 8 (255). The
 // packed loop keeps each target as broadcast pairs and its sums as pairs (12
-// registers a target).
+// registers a target). The chained kernel carries one more pair a target: 5
+// for T = 2 (96), 4 for T = 3 and T = 4 (128; T = 4 then spills ~100 bytes,
+// and measured faster so than at 3 CTAs with 168 registers on the cut-off
+// core, slower on the Vatistas core, where T = 3 wins).
 template <int T, bool CHAIN>
 struct MinBlocks {
-  static constexpr int value = CHAIN ? (T <= 2 ? 5 : (T == 3 ? 4 : (T <= 4 ? 3 : 2)))
+  static constexpr int value = CHAIN ? (T <= 2 ? 5 : (T <= 4 ? 4 : 2))
                                      : (T <= 2 ? 6 : (T == 3 ? 5 : (T <= 4 ? 4 : 2)));
 };
 
