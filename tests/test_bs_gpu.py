@@ -188,6 +188,50 @@ def test_edge_cases_gpu(wb):
                 assert np.all(u[3] == 0.0)
 
 
+def _count(shape):
+    d = list(shape) + [1] * (4 - len(shape))
+    return d[0] * d[2] * d[3]
+
+
+def test_chained_stream_on_unlinked_and_edge_inputs(wb, synth, oracle):
+    """The chained filament stream evaluates any input correctly, linked or
+    not: the edge cases above (zero-length filament, NaN circulation, targets
+    on a filament and its extension), and a wake whose trailing family has
+    its ages shuffled (so only a few of its filaments still continue their
+    neighbour), each forced onto the chained and the input-order layout and
+    checked against the FP64 oracle."""
+    g = load_golden("bs_edge.npz")
+    fams = [(g["F1"], g["F2"], g["g"], g["rc"])]
+    nt, nf = _count(g["P"].shape), _count(g["F1"].shape)
+    for d in (1e-4, "visc2"):
+        core, dv = wb.bs.parse_core(d)
+        uo = g[f"u_oracle_{d if isinstance(d, str) else '0.0001'}_1000.0"]
+        scale = np.abs(uo).max()
+        for chained in (True, False):
+            wb.set_tuning(core, nt, nf, 4, 64, 8.0)
+            wb.set_layout(core, nt, nf, chained)
+            u = wb.eval_host(fams, g["P"], core, dv, 1000.0, "f32c")
+            assert wb.last_chained() == chained
+            assert np.all(np.isfinite(u))
+            assert np.abs(u - uo).max() <= F32C_TOL * scale, (d, chained)
+    w = synth.make_wake(synth.RotorCase(nst=13, nsteps=40, dpsi_deg=6.0, seed=17))
+    F1, F2 = synth.trail_filaments(w["dom"])
+    perm = np.random.default_rng(3).permutation(F1.shape[2])  # shuffles the wake ages
+    fams = [synth.shed_filaments(w["dom"]) + (w["gamma_shed"], w["rc_shed"]),
+            (np.asfortranarray(F1[:, :, perm]), np.asfortranarray(F2[:, :, perm]),
+             np.asfortranarray(w["gamma_trail"][:, :, perm]),
+             np.asfortranarray(w["rc_trail"][:, :, perm]))]
+    P = w["dom"]
+    nt, nf = _count(P.shape), sum(_count(f[0].shape) for f in fams)
+    uo = sum(oracle.c_eval(F1_, F2_, P, g_, rc_, "visc2", 1000.0) for F1_, F2_, g_, rc_ in fams)
+    for chained in (True, False):
+        wb.set_tuning(wb.bs.CORE_VATISTAS, nt, nf, 3, 64, 16.0)
+        wb.set_layout(wb.bs.CORE_VATISTAS, nt, nf, chained)
+        u = wb.eval_host(fams, P, wb.bs.CORE_VATISTAS, 2.0, 1000.0, "f32c")
+        assert wb.last_chained() == chained
+        assert per_target_rel(u, uo) < F32C_TOL, chained
+
+
 def test_empty_inputs(wb, synth):
     w = synth.make_wake(synth.RotorCase(nst=5, nsteps=4))
     F1, F2 = synth.shed_filaments(w["dom"])
