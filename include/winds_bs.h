@@ -165,9 +165,12 @@ int winds_bs_sync(void *stream);
 /* Autotuner control. The first FP32 evaluation of a (core model, log2 targets,
  * log2 filaments) bucket on the library's own stream times the candidate
  * tilings (targets per thread T in {2,3,4}, filaments per tile KF in {32,64,128},
- * work-queue depth: items per resident warp) and caches the fastest (T = 8 is
- * settable); set_tuning / get_tuning read and
- * write that cache directly (e.g. to restore a saved choice). */
+ * work-queue depth: items per resident warp) on both filament stream layouts
+ * (input order and chained) and caches the fastest tiling and layout (T = 8
+ * is settable). Evaluations on another stream, or with the autotuner off, use
+ * the cached choice or the untuned default (T = 4, KF = 64, input order).
+ * set_tuning / get_tuning read and write that cache directly (e.g. to restore
+ * a saved choice). */
 int winds_bs_set_autotune(int on);
 int winds_bs_set_tuning(int core_model, long long n_targets, long long n_filaments, int T, int KF,
                         double waves);
