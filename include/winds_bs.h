@@ -168,7 +168,8 @@ int winds_bs_sync(void *stream);
  * work-queue depth: items per resident warp) on both filament stream layouts
  * (input order and chained) and caches the fastest tiling and layout (T = 8
  * is settable). Evaluations on another stream, or with the autotuner off, use
- * the cached choice or the untuned default (T = 4, KF = 64, input order).
+ * the cached choice or the untuned default (T = 4, or 2 below 2048 targets;
+ * KF = 64; input order).
  * set_tuning / get_tuning read and write that cache directly (e.g. to restore
  * a saved choice). */
 int winds_bs_set_autotune(int on);
