@@ -38,11 +38,13 @@ def test_reference_arm_prints_one_contract_line():
 
 
 def test_traffic_from_committed_profile():
+    """Both stream layouts have a committed capture to scale from."""
     b = _bench()
     n = 15547629240
-    t = b.profiled_traffic(n)
-    assert t is not None and 1e7 < t < 1e10
-    assert abs(b.profiled_traffic(2 * n) - 2 * t) < 1e-6 * t
+    for chained in (False, True):
+        t = b.profiled_traffic(n, chained)
+        assert t is not None and 1e7 < t < 1e10, chained
+        assert abs(b.profiled_traffic(2 * n, chained) - 2 * t) < 1e-6 * t
 
 
 def test_workload_sizes_match_the_metric_case():
